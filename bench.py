@@ -1,0 +1,321 @@
+#!/usr/bin/env python
+"""Benchmark of the relaxation loop: node-iterations per second.
+
+Workload (default): 256^3 volume, six nested noisy ellipsoidal shells (semi-axes
+60..120 voxels, 4-octave seeded noise of amplitude 6 voxels), h in [1.5, 6]
+voxels graded by the distance to the nearest interface, ~1M seeded nodes, 500
+FP32 FIRE iterations (dptol 0: no early stop), the reference's Verlet rebuild
+trigger. One step = one whole relaxation from the seeds (first list build +
+500 iterations), inputs resident in HBM.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+
+N > 1 runs under torchrun, one process per GPU: a single volume does not
+shard, so each rank relaxes its own replica (weak scaling, no collective on the
+data path); the step time is the max over ranks (all_reduce MAX over NCCL).
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "relax node-iters/s at 1M nodes"
+UNIT = "node-iters/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--workload", default="shells256")
+    ap.add_argument("--iters", type=int, default=None)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--ref-iters", type=int, default=10, help="iterations per reference-arm / CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(name, seed=0):
+    from trussnet_b200 import synth
+    if name == "shells256":
+        g, nd = synth.shells(seed=seed)
+        prm = synth.params_for("shells256")
+        desc = ("shells256: 256^3, 6 nested noisy ellipsoidal shells (semi-axes 60-120 vox, noise amp 6 vox, "
+                "4 octaves), h in [1.5,6] vox graded by interface distance, FIRE, reference Verlet trigger")
+    elif name == "sphere64":
+        g, nd = synth.sphere(seed=seed)
+        prm = synth.params_for("sphere64")
+        desc = "sphere64: 64^3 sphere r=24, h=2, 2-voxel lattice + jitter, dt=0.2"
+    elif name == "tpm182":
+        g, nd = synth.tpm(seed=seed)
+        prm = synth.params_for("tpm182")
+        desc = "tpm182: 182x218x182 argmax of 6 smoothed noise fields (sigma 4), h=1.3"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return g, nd, prm, desc
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel: str, workload_name: str):
+    """dram bytes per launch of `kernel` from the committed ncu summary
+    (profiles/<kernel>_<workload>.txt, line 'traffic_bytes_per_launch: X')."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload_name}.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(g, nd, prm, iters):
+    """The reference's relax_cpu (oracle/_ref, the compiled reference) on a bounded
+    sample: the same grid and seeds, `iters` iterations."""
+    from oracle.ref import RefLib, available
+    from trussnet_b200.types import RelaxParams
+    p = RelaxParams(**{**prm.__dict__, "max_iters": iters})
+    if not available():
+        return None
+    lib = RefLib()
+    a = nd.copy()
+    t0 = time.perf_counter()
+    lib.relax_cpu(g, p, a)
+    dt = time.perf_counter() - t0
+    cores = os.cpu_count() or 1
+    if os.environ.get("OMP_NUM_THREADS"):
+        cores = int(os.environ["OMP_NUM_THREADS"])
+    else:
+        cap = int(os.environ.get("V2M_OMP_MAX_THREADS", "64"))
+        cores = min(cores, cap) if cap > 0 else cores
+    return {"value": nd.size() * iters / dt, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"relax_cpu on the same grid and seeds, {iters} iterations (first list build included), "
+                      f"{dt:.2f} s"}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return
+    g, nd, prm, desc = workload(args.workload)
+    from oracle.ref import available
+    if not available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libv2m_ref.so is not built"}))
+        return
+    for _ in range(args.warmup):
+        cpu_baseline(g, nd, prm, args.ref_iters)
+    vals = []
+    cb = None
+    for _ in range(args.steps):
+        cb = cpu_baseline(g, nd, prm, args.ref_iters)
+        vals.append(cb["value"])
+    v = statistics.mean(vals)
+    ms = nd.size() * args.ref_iters / v * 1e3
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": desc, "nodes": nd.size(), "iters_per_step": args.ref_iters,
+                       "parallelism": "replicas"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cb["cores"], "kind": "reference",
+                             "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def pinned_copy(a: np.ndarray) -> np.ndarray:
+    import torch
+    t = torch.empty(a.shape, dtype={np.dtype(np.float32): torch.float32, np.dtype(np.uint16): torch.int16,
+                                    np.dtype(np.int32): torch.int32, np.dtype(np.uint8): torch.uint8}[a.dtype],
+                    pin_memory=True)
+    out = t.numpy().view(a.dtype)
+    out[...] = a
+    out._keep = t  # noqa: the tensor owns the pinned pages
+    return out
+
+
+def run_cuda(args):
+    import torch
+    world, rank, local = dist_setup(args)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from trussnet_b200 import Session, relax_cl
+    from trussnet_b200.types import Grid, Nodes
+    g, nd, prm, desc = workload(args.workload)
+    if args.iters:
+        prm.max_iters = args.iters
+    iters = prm.max_iters
+    n = nd.size()
+    sess = Session(g, prm, nd, device=local)
+    sess.timed_runs(args.warmup, graph=True)
+    sess.clear_counters()
+
+    def barrier():
+        torch.cuda.synchronize(local)
+        if world > 1:
+            torch.distributed.barrier()
+
+    barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    ms = sess.timed_runs(args.steps, graph=True, time_force=True)
+    clocks = clk.stop()
+    barrier()
+    cnt = sess.counters()
+    step_ms = ms / args.steps
+    if world > 1:
+        t = torch.tensor([step_ms], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        step_ms = float(t.item())
+    value = world * n * iters / (step_ms / 1e3)
+    # force kernel roofline: algorithmic bytes per launch / mean event-timed launch
+    nnb = sess.read("nnb").astype(np.int64)
+    force_bytes = 37 * n + 4 * int(nnb.sum())
+    force_avg_ms = cnt["force_ms"] / max(1, cnt["force_launches"])
+    peak, peak_kind = peaks()
+    achieved = force_bytes / (force_avg_ms / 1e3) / 1e9 if force_avg_ms > 0 else None
+    roofline = {"kernel": "k_force", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None, "peak_source": peak_kind,
+                "traffic": profiled_traffic("k_force", args.workload),
+                "bytes_per_launch": force_bytes, "mean_nnb": float(nnb.mean()) if n else 0.0,
+                "force_ms_per_launch": force_avg_ms, "force_share_of_step": cnt["force_ms"] / ms if ms else None}
+    st = sess.stats()
+    sess.close()
+    # end to end through the public call (tn::relax_cl's C ABI) with pinned host buffers
+    gp = Grid(nx=g.nx, ny=g.ny, nz=g.nz, vs=g.vs, L=pinned_copy(g.L), bl_cnt=pinned_copy(g.bl_cnt),
+              bl_lab=pinned_copy(g.bl_lab), bl_slot=pinned_copy(g.bl_slot), phi=pinned_copy(g.phi),
+              h=pinned_copy(g.h), hmin=g.hmin, hmax=g.hmax)
+    npin = Nodes(P=pinned_copy(nd.P), lab=pinned_copy(nd.lab), typ=pinned_copy(nd.typ), part=pinned_copy(nd.part))
+    e2e_times = []
+    for k in range(args.e2e_steps + 1):
+        npin.P[...] = nd.P
+        npin.typ[...] = nd.typ
+        npin.part[...] = nd.part
+        barrier()
+        t0 = time.perf_counter()
+        relax_cl(gp, prm, npin, device=local)
+        torch.cuda.synchronize(local)
+        t1 = time.perf_counter()
+        if k > 0:   # the first call loads the module and warms the allocator
+            e2e_times.append(t1 - t0)
+    e2e_s = statistics.mean(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = g.nbytes() + nd.nbytes()
+    d2h = nd.P.nbytes + nd.typ.nbytes + nd.part.nbytes
+    e2e = {"value": world * n * iters / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "s_per_step": e2e_s}
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(g, nd, prm, args.ref_iters)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": desc, "nodes": n, "iters_per_step": iters, "parallelism": f"replicas x{world}",
+                           "l2": "inputs larger than L2 (grid %.0f MB + nodes %.0f MB per replica)" %
+                                 (g.nbytes() / 1e6, nd.nbytes() / 1e6),
+                           "rebuilds_per_step": st.rebuilds, "final_types": [st.n_interior, st.n_interface,
+                                                                             st.n_junction, st.n_corner]},
+                "clocks": clocks, "e2e": e2e, "gpu_launches": int(cnt["launches"]), "roofline": roofline,
+                "cpu_baseline": cb}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_cuda(args)
+
+
+if __name__ == "__main__":
+    main()

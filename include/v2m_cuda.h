@@ -1,0 +1,215 @@
+/*
+ * v2m_cuda.h -- C ABI of the B200 (sm_100a) relaxation library libv2m_cuda.so.
+ *
+ * The library replaces v2mesh's OpenCL relaxation, tn::relax_cl
+ * (src/v2m_gpu.h:16-18 in fangq/trussnet), behind plain C: POD views of the
+ * reference's Grid / RelaxParams / Nodes / RelaxStats, host pointers and sizes,
+ * an int status (0 = ok, < 0 = error) and a thread-local error text. The C++
+ * shim libv2m_relax_cl.so builds tn::relax_cl with the reference's exact
+ * signature on top of these entry points, so the reference's v2m_core links
+ * against it unchanged (the pipeline's CPU fallback still catches its
+ * std::runtime_error).
+ *
+ * Nothing here falls back to the CPU: without a usable CUDA device every entry
+ * point returns V2M_ERR_CUDA.
+ */
+#ifndef V2M_CUDA_H
+#define V2M_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define V2M_CUDA_ABI_VERSION 1
+
+/* status codes */
+#define V2M_OK 0
+#define V2M_ERR_ARG (-1)      /* invalid argument (sizes, null pointers, limits) */
+#define V2M_ERR_CUDA (-2)     /* a CUDA runtime call failed (no device, out of memory, launch) */
+#define V2M_ERR_KERNEL (-3)   /* a kernel raised its error flag (index out of range, bounded wait) */
+#define V2M_ERR_STATE (-4)    /* call out of order (e.g. force before the first rebuild) */
+
+/* node types (src/opencl/v2m_seed_body.cl:15-19) */
+#define V2M_INTERIOR 0
+#define V2M_INTERFACE 1
+#define V2M_JUNCTION 2
+#define V2M_CORNER 3
+#define V2M_NOLAB 0xFFFF
+
+#define V2M_K 24        /* truss neighbours per node (src/opencl/v2m_particle_body.cl:18) */
+#define V2M_MAXLEV 8    /* hash levels (src/opencl/v2m_particle_body.cl:19) */
+#define V2M_BS 8        /* brick side (src/opencl/v2m_grid_body.cl:20) */
+#define V2M_SLOT 512    /* phi values per (brick, label) slot (src/opencl/v2m_grid_body.cl:21) */
+#define V2M_BL 16       /* labels per brick (src/opencl/v2m_grid_body.cl:22) */
+
+/*
+ * The read-only fields the relaxation samples: tn::Grid (src/v2m_grid.h:45-81),
+ * the members relax_cl reads. Every array is caller-owned host memory, x-fastest
+ * (index i + nx*(j + ny*k)); bricks are 8^3 voxels, nb = nbx*nby*nbz.
+ */
+typedef struct {
+    int32_t nx, ny, nz;          /* voxels */
+    int32_t nbx, nby, nbz;       /* bricks: ceil(n / 8) per axis */
+    float vs[3];                 /* voxel size (mm) */
+    const uint16_t* L;           /* labels, nx*ny*nz */
+    const int32_t* bl_cnt;       /* nb: labels within R of each brick (V2M_BL+1 = overflow) */
+    const uint16_t* bl_lab;      /* V2M_BL*nb: those labels, ascending, 0xFFFF padded */
+    const int32_t* bl_slot;      /* nb: first slot of each mixed brick, -1 = uniform */
+    const float* phi;            /* V2M_SLOT*nslots smoothed indicators */
+    int64_t nslots;
+    const float* h;              /* nx*ny*nz target size (mm) */
+    float hmin, hmax;            /* range of h (mm): the hash geometry */
+    const float* gI;             /* gray-scale intensity nx*ny*nz (gm > 0), else NULL */
+    const float* gTW;            /* gray-scale [t_0..t_{m-1}, W_0..W_{m-1}] (gm > 0), else NULL */
+    int32_t gm;                  /* number of gray thresholds; 0 = label volume; < 0 (analytic shapes) is rejected */
+} v2m_grid_view;
+
+/*
+ * tn::RelaxParams (src/v2m_particles.h:21-41), same names and meaning, plus
+ * three extensions (0 keeps the reference's behaviour).
+ */
+typedef struct {
+    int32_t nseed;
+    float t, skin, fscale, fsurf, dt, maxstep, snap;
+    int32_t max_iters;
+    float dptol, jseed;
+    int32_t corners, voxel_trap;
+    float thin;
+    int32_t fire;
+    float fire_dtmax;
+    int32_t verbose;
+    /* extensions */
+    int32_t h_mode;          /* 0: h at the nearest voxel (reference); 1: trilinear h */
+    int32_t rebuild_div;     /* Verlet trigger divisor; 0: V2M_REBUILD_DIV or 300 (src/v2m_gpu.cpp:119) */
+    int32_t rebuild_policy;  /* 0: reference Verlet trigger; 1: rebuild when max |dp| since the build > 0.1 h */
+} v2m_relax_params;
+
+/* tn::Nodes (src/v2m_particles.h:78-87): the node arrays, caller-owned host memory. */
+typedef struct {
+    int64_t n;
+    float* P;              /* 3n positions (grid mm), in/out */
+    const uint16_t* lab;   /* n own labels */
+    uint8_t* typ;          /* n types, in/out */
+    uint16_t* part;        /* 2n partner labels, in/out */
+} v2m_nodes_view;
+
+/* tn::RelaxStats (src/v2m_particles.h:89-96). */
+typedef struct {
+    int32_t iters, rebuilds;
+    float last_move, last_p99;
+    int32_t fire_resets;
+    float fire_dt;
+    int64_t n_interior, n_interface, n_junction, n_corner;
+    double ms_seed, ms_hash, ms_force, ms_move;
+} v2m_relax_stats;
+
+/* The reference's RelaxParams defaults (src/v2m_particles.h:22-40). */
+void v2m_relax_params_default(v2m_relax_params* p);
+
+/* Text of the last error on this thread ("" if none). */
+const char* v2m_cuda_last_error(void);
+
+/* Number of CUDA devices (0 when none or the driver is missing). */
+int v2m_cuda_device_count(void);
+
+/*
+ * Relax the nodes on CUDA device `device` (-1 = device 0). Same contract as
+ * tn::relax_cl (src/v2m_gpu.cpp:116-553) and tn::relax_cpu
+ * (src/v2m_particles.cpp:728-976): positions, types and partner labels are
+ * updated in place, the node count and order are unchanged. Host buffers in,
+ * host buffers out; the grid is uploaded on every call.
+ */
+int v2m_relax_cuda(const v2m_grid_view* g, const v2m_relax_params* prm, v2m_nodes_view* nd, v2m_relax_stats* st,
+                   int device);
+
+/*
+ * Many independent volumes in one set of launches (one per stage for all of
+ * them), the iteration loop captured in a CUDA graph. Each volume keeps its own
+ * hash, lists, FIRE state and stop / rebuild decisions, so volume v's result is
+ * the one v2m_relax_cuda gives for it alone. No counterpart in the reference,
+ * which relaxes one volume per call (src/v2m_pipeline.cpp:492-536).
+ */
+int v2m_relax_cuda_batch(int nvol, const v2m_grid_view* g, const v2m_relax_params* prm, v2m_nodes_view* nd,
+                         v2m_relax_stats* st, int device);
+
+/*
+ * Sessions: the relaxation state kept on the device between calls, for step-wise
+ * use (the stages of relax_cl one at a time), repeated runs from the same seeds,
+ * and batches. A session owns device copies of the grids and of the seeds.
+ */
+typedef struct v2m_session v2m_session;
+
+int v2m_session_create(int nvol, const v2m_grid_view* g, const v2m_relax_params* prm, const v2m_nodes_view* nd,
+                       int device, v2m_session** out);
+int v2m_session_destroy(v2m_session* s);
+/* Back to the seeds: positions, types, partners, velocities, FIRE state, counters. */
+int v2m_session_reset(v2m_session* s);
+/* relax_cl's rebuild (src/v2m_gpu.cpp:259-277): keys, stable counting sort, bin-order gather, K-nearest lists. */
+int v2m_session_rebuild(v2m_session* s);
+/* k_force (src/opencl/v2m_kernels.cl:159-169) for every node. */
+int v2m_session_force(v2m_session* s);
+/*
+ * The rest of one iteration (src/v2m_particles.cpp:838-946): move, FIRE update,
+ * histogram / p99, stop test, Verlet self-refresh and rebuild trigger (the
+ * rebuild itself included when it fires).
+ */
+int v2m_session_step_tail(v2m_session* s);
+/* Up to `iters` whole iterations (force + tail); graph != 0 replays a captured CUDA graph. */
+int v2m_session_iterate(v2m_session* s, int iters, int graph);
+/* A whole relaxation from the current state: first rebuild, then the loop to max_iters or convergence. */
+int v2m_session_run(v2m_session* s, int graph);
+int v2m_session_synchronize(v2m_session* s);
+/* Write the current nodes (P, typ, part) of volume `vol` into nd (host). */
+int v2m_session_read_nodes(v2m_session* s, int vol, v2m_nodes_view* nd);
+int v2m_session_stats(v2m_session* s, int vol, v2m_relax_stats* st);
+
+/* Internal arrays of volume `vol` copied to host memory, for parity checks. */
+#define V2M_ARR_KEY 1        /* int32 [n]   bin key of each node (level offset + bin) */
+#define V2M_ARR_SORTED 2     /* int32 [n]   node ids in (key, id) order */
+#define V2M_ARR_CSTART 3     /* int32 [nkeys+1] bin starts */
+#define V2M_ARR_PS 4         /* float [4n]  positions + h in bin order */
+#define V2M_ARR_NBR 5        /* int32 [K*n] truss lists, row-major nbr[i*K+k] as the reference */
+#define V2M_ARR_NNB 6        /* int32 [n]   list lengths */
+#define V2M_ARR_F 7          /* float [4n]  force + active bars */
+#define V2M_ARR_HN 8         /* float [n]   h at each node */
+#define V2M_ARR_MV 9         /* float [n]   |dp| / h of the last move */
+#define V2M_ARR_V 10         /* float [3n]  FIRE velocities */
+#define V2M_ARR_PW 11        /* float [n]   FIRE power a.v of the last move */
+#define V2M_ARR_P0 12        /* float [3n]  positions at the last list build */
+#define V2M_ARR_HIST 13      /* int32 [34]  log2 histogram, max |dp|/h bits, half-skin count */
+int v2m_session_read_array(v2m_session* s, int vol, int what, void* host, int64_t bytes);
+/* Overwrite an internal array of volume `vol` from host memory (P, typ, part, nbr, nnb, V, hn). */
+int v2m_session_write_array(v2m_session* s, int vol, int what, const void* host, int64_t bytes);
+/* Overwrite the truss lists of volume `vol` (row-major nbr[i*K+k], local ids, and nnb). */
+int v2m_session_write_lists(v2m_session* s, int vol, const int32_t* nbr, const int32_t* nnb);
+#define V2M_ARR_P 20         /* float [3n]  positions */
+#define V2M_ARR_TYP 21       /* uint8 [n]   types */
+#define V2M_ARR_PART 22      /* uint16 [2n] partner labels */
+
+/* Sizes of volume `vol`: n nodes, nkeys bins, hash levels. */
+int v2m_session_info(v2m_session* s, int vol, int64_t* n, int64_t* nkeys, int32_t* nlev);
+
+/*
+ * Kernel launches issued so far by the session (all kernels of this library),
+ * and the device time of the force kernel's launches (CUDA events), for the
+ * roofline figures of the benchmark.
+ */
+int v2m_session_counters(v2m_session* s, int64_t* launches, int64_t* force_launches, double* force_ms);
+
+/*
+ * Benchmark helper: `runs` whole relaxations from the seeds (reset, first
+ * rebuild, loop), bracketed by CUDA events on the session's stream; the elapsed
+ * device time in *ms. time_force != 0 also records events around every force
+ * launch (read back with v2m_session_counters).
+ */
+int v2m_session_timed_runs(v2m_session* s, int runs, int graph, int time_force, float* ms);
+int v2m_session_clear_counters(v2m_session* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* V2M_CUDA_H */

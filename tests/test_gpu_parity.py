@@ -1,0 +1,215 @@
+"""GPU parity: the CUDA relaxation (through the C ABI) against the reference's
+own CPU path (oracle/_ref, relax_cpu and its stages) on identical inputs.
+
+The bar is bit-exact: bin keys, sorted order, bin starts, truss lists, forces,
+positions, types and partner labels. Kernels compute in FP32 without FMA
+contraction and with IEEE division and square root, in the reference's
+operation order, so there is no tolerance to state for these stages.
+"""
+import numpy as np
+import pytest
+
+import cases
+from cases import first_diff, same_bits
+from trussnet_b200 import Session, relax_cl, relax_cl_batch
+from trussnet_b200.types import V2M_CORNER, V2M_K, RelaxParams
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["sphere_small", "shells_small", "tpm_small", "ref_phantom"]
+
+
+def load_case(name, ref):
+    if name == "ref_phantom":
+        return cases.ref_phantom(ref)
+    return getattr(cases, name)()
+
+
+def rowmajor_lists(nbr, nnb, n):
+    """Truss lists with unused slots zeroed (both sides compared this way)."""
+    nbr = nbr.reshape(n, V2M_K).copy()
+    k = np.arange(V2M_K)[None, :]
+    nbr[k >= nnb[:, None]] = 0
+    return nbr
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_rebuild_bit_exact(name, ref, cuda_lib):
+    g, nd = load_case(name, ref)
+    prm = cases.params(10)
+    rs = ref.state(g, prm, nd.copy())
+    rs.rebuild()
+    with Session(g, prm, nd.copy()) as s:
+        s.rebuild()
+        assert s.nkeys[0] == rs.nkeys
+        for a in ("key", "sorted", "cstart", "nnb"):
+            d = first_diff(s.read(a), rs.read(a))
+            assert d is None, f"{a}: {d}"
+        ps_ref = rs.read("Ps").reshape(-1, 4)
+        assert same_bits(s.read("Ps").reshape(-1, 4), ps_ref)
+        n = nd.size()
+        nnb = rs.read("nnb")
+        d = first_diff(rowmajor_lists(s.read("nbr"), nnb, n), rowmajor_lists(rs.read("nbr"), nnb, n))
+        assert d is None, f"nbr: {d}"
+        assert same_bits(s.read("P0"), rs.read("P0"))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_force_bit_exact(name, ref, cuda_lib):
+    g, nd = load_case(name, ref)
+    prm = cases.params(10)
+    rs = ref.state(g, prm, nd.copy())
+    rs.rebuild()
+    rs.force()
+    with Session(g, prm, nd.copy()) as s:
+        s.rebuild()
+        s.force()
+        d = first_diff(s.read("F"), rs.read("F"))
+        assert d is None, f"F: {d}"
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("fire", [True, False])
+def test_one_iteration_bit_exact(name, fire, ref, cuda_lib):
+    g, nd = load_case(name, ref)
+    prm = cases.params(10, fire=fire)
+    rs = ref.state(g, prm, nd.copy())
+    rs.rebuild()
+    with Session(g, prm, nd.copy()) as s:
+        s.rebuild()
+        for it in range(3):
+            rs.force()
+            rs.tail()
+            s.force()
+            s.step_tail()
+            for a in ("P", "typ", "part", "mv", "hn"):
+                d = first_diff(s.read(a), rs.read(a))
+                assert d is None, f"iteration {it}, {a}: {d}"
+            if fire:
+                for a in ("V", "pw"):
+                    d = first_diff(s.read(a), rs.read(a))
+                    assert d is None, f"iteration {it}, {a}: {d}"
+            st = s.stats()
+            c = rs.counts()
+            assert st.rebuilds == c["rebuilds"], it
+            assert st.last_move == c["mmax"]
+            assert st.last_p99 == c["p99"]
+            assert st.fire_resets == c["fire_resets"]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_full_relax_bit_exact_serial_power(name, ref, cuda_lib, monkeypatch):
+    """Whole loop, FIRE power summed in the CPU's serial order: identical to relax_cpu."""
+    monkeypatch.setenv("V2M_CUDA_SERIAL_POWER", "1")
+    g, nd = load_case(name, ref)
+    prm = cases.params(60)
+    a = nd.copy()
+    st_ref = ref.relax_cpu(g, prm, a)
+    b = nd.copy()
+    st = relax_cl(g, prm, b)
+    assert st.iters == st_ref.iters and st.rebuilds == st_ref.rebuilds
+    for f in ("P", "typ", "part"):
+        d = first_diff(getattr(b, f), getattr(a, f))
+        assert d is None, f"{f}: {d}"
+    assert st.fire_resets == st_ref.fire_resets and st.fire_dt == st_ref.fire_dt
+    assert (st.n_interior, st.n_interface, st.n_junction, st.n_corner) == \
+        (st_ref.n_interior, st_ref.n_interface, st_ref.n_junction, st_ref.n_corner)
+
+
+@pytest.mark.parametrize("name", ["sphere64", "shells_small", "ref_phantom"])
+def test_full_relax_tree_power(name, ref, cuda_lib):
+    """Production FIRE sum (fixed-shape double tree): same trajectory as the
+    CPU unless the power's sign differs from the serial sum's; the graph and the
+    plain launches agree bit for bit, and two runs are identical."""
+    g, nd = load_case(name, ref)
+    prm = RelaxParams(max_iters=200, dt=0.2, dptol=0.0) if name == "sphere64" else cases.params(80)
+    a = nd.copy()
+    st_ref = ref.relax_cpu(g, prm, a)
+    with Session(g, prm, nd.copy()) as s:
+        s.run(graph=True)
+        b = s.read_nodes(nd.copy())
+        st = s.stats()
+        s.reset()
+        s.run(graph=False)
+        c = s.read_nodes(nd.copy())
+    for f in ("P", "typ", "part"):
+        assert same_bits(getattr(b, f), getattr(c, f)), f"graph vs plain launches differ in {f}"
+    assert st.iters == st_ref.iters
+    d = first_diff(b.P, a.P)
+    assert d is None, f"P vs relax_cpu: {d}"
+
+
+def test_relax_cl_deterministic(cuda_lib):
+    g, nd = cases.shells_small()
+    prm = cases.params(50)
+    a, b = nd.copy(), nd.copy()
+    relax_cl(g, prm, a)
+    relax_cl(g, prm, b)
+    assert same_bits(a.P, b.P) and same_bits(a.typ, b.typ) and same_bits(a.part, b.part)
+
+
+def test_voxel_trap_mode(ref, cuda_lib):
+    g, nd = cases.shells_small()
+    prm = cases.params(20, voxel_trap=True)
+    a = nd.copy()
+    ref.relax_cpu(g, prm, a)
+    b = nd.copy()
+    relax_cl(g, prm, b)
+    for f in ("P", "typ", "part"):
+        d = first_diff(getattr(b, f), getattr(a, f))
+        assert d is None, f"{f}: {d}"
+
+
+def test_corners_stay(ref, cuda_lib):
+    g, nd = cases.tpm_small()
+    nd = nd.copy()
+    rng = np.random.default_rng(5)
+    idx = rng.choice(nd.size(), 50, replace=False)
+    nd.typ[idx] = V2M_CORNER
+    prm = cases.params(20)
+    a = nd.copy()
+    ref.relax_cpu(g, prm, a)
+    b = nd.copy()
+    relax_cl(g, prm, b)
+    assert same_bits(b.P[idx], nd.P[idx])
+    assert same_bits(b.P, a.P) and same_bits(b.typ, a.typ)
+
+
+def test_batch_equals_single(cuda_lib, monkeypatch):
+    monkeypatch.setenv("V2M_CUDA_SERIAL_POWER", "1")
+    vols = [cases.sphere_small(), cases.shells_small(), cases.tpm_small()]
+    prms = [cases.params(40), cases.params(25), cases.params(30)]
+    singles = []
+    for (g, nd), p in zip(vols, prms):
+        x = nd.copy()
+        relax_cl(g, p, x)
+        singles.append(x)
+    outs = [nd.copy() for _, nd in vols]
+    relax_cl_batch([g for g, _ in vols], prms, outs)
+    for x, y in zip(singles, outs):
+        assert same_bits(x.P, y.P) and same_bits(x.typ, y.typ) and same_bits(x.part, y.part)
+
+
+def test_edge_cases(ref, cuda_lib):
+    g, nd = cases.sphere_small()
+    prm = cases.params(5)
+    # no nodes
+    empty = nd.copy()
+    empty.P = empty.P[:0].copy()
+    empty.lab = empty.lab[:0].copy()
+    empty.typ = empty.typ[:0].copy()
+    empty.part = empty.part[:0].copy()
+    st = relax_cl(g, prm, empty)
+    st_ref = ref.relax_cpu(g, prm, empty.copy())
+    assert st.iters == st_ref.iters
+    # one node
+    one = nd.copy()
+    one.P, one.lab, one.typ, one.part = one.P[:1].copy(), one.lab[:1].copy(), one.typ[:1].copy(), one.part[:1].copy()
+    a = one.copy()
+    ref.relax_cpu(g, prm, a)
+    relax_cl(g, prm, one)
+    assert same_bits(one.P, a.P)
+    # zero iterations: nothing moves
+    z = nd.copy()
+    relax_cl(g, cases.params(0), z)
+    assert same_bits(z.P, nd.P)

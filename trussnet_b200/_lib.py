@@ -1,0 +1,79 @@
+"""Loading libv2m_cuda.so (built in-tree by trussnet_b200.build) and its C ABI.
+
+There is no fallback: if the library is missing or fails to load, every call
+raises. The library itself returns V2M_ERR_CUDA when no CUDA device is usable.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+from .types import GridView, NodesView, RelaxParamsC, RelaxStatsC
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libv2m_cuda.so")
+
+V2M_OK, V2M_ERR_ARG, V2M_ERR_CUDA, V2M_ERR_KERNEL, V2M_ERR_STATE = 0, -1, -2, -3, -4
+
+# every symbol include/v2m_cuda.h declares
+EXPORTS = [
+    "v2m_relax_params_default", "v2m_cuda_last_error", "v2m_cuda_device_count", "v2m_relax_cuda",
+    "v2m_relax_cuda_batch", "v2m_session_create", "v2m_session_destroy", "v2m_session_reset", "v2m_session_rebuild",
+    "v2m_session_force", "v2m_session_step_tail", "v2m_session_iterate", "v2m_session_run", "v2m_session_synchronize",
+    "v2m_session_read_nodes", "v2m_session_stats", "v2m_session_read_array", "v2m_session_write_array",
+    "v2m_session_write_lists", "v2m_session_info", "v2m_session_counters", "v2m_session_timed_runs",
+    "v2m_session_clear_counters",
+]
+
+_lock = threading.Lock()
+_lib = None
+
+
+class V2mError(RuntimeError):
+    """A failed library call (the reference's relax_cl throws std::runtime_error)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"v2m_cuda error {code}: {msg}")
+        self.code = code
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(path):
+            raise V2mError(V2M_ERR_CUDA, f"{path} is not built (python -m trussnet_b200.build)")
+        L = C.CDLL(path)
+        vp = C.c_void_p
+        P = C.POINTER
+        L.v2m_cuda_last_error.restype = C.c_char_p
+        L.v2m_relax_params_default.argtypes = [P(RelaxParamsC)]
+        L.v2m_relax_params_default.restype = None
+        L.v2m_relax_cuda.argtypes = [P(GridView), P(RelaxParamsC), P(NodesView), P(RelaxStatsC), C.c_int]
+        L.v2m_relax_cuda_batch.argtypes = [C.c_int, P(GridView), P(RelaxParamsC), P(NodesView), P(RelaxStatsC),
+                                           C.c_int]
+        L.v2m_session_create.argtypes = [C.c_int, P(GridView), P(RelaxParamsC), P(NodesView), C.c_int, P(vp)]
+        for f in ("v2m_session_destroy", "v2m_session_reset", "v2m_session_rebuild", "v2m_session_force",
+                  "v2m_session_step_tail", "v2m_session_synchronize"):
+            getattr(L, f).argtypes = [vp]
+        L.v2m_session_iterate.argtypes = [vp, C.c_int, C.c_int]
+        L.v2m_session_run.argtypes = [vp, C.c_int]
+        L.v2m_session_read_nodes.argtypes = [vp, C.c_int, P(NodesView)]
+        L.v2m_session_stats.argtypes = [vp, C.c_int, P(RelaxStatsC)]
+        L.v2m_session_read_array.argtypes = [vp, C.c_int, C.c_int, vp, C.c_int64]
+        L.v2m_session_write_array.argtypes = [vp, C.c_int, C.c_int, vp, C.c_int64]
+        L.v2m_session_write_lists.argtypes = [vp, C.c_int, vp, vp]
+        L.v2m_session_info.argtypes = [vp, C.c_int, P(C.c_int64), P(C.c_int64), P(C.c_int32)]
+        L.v2m_session_counters.argtypes = [vp, P(C.c_int64), P(C.c_int64), P(C.c_double)]
+        L.v2m_session_timed_runs.argtypes = [vp, C.c_int, C.c_int, C.c_int, P(C.c_float)]
+        L.v2m_session_clear_counters.argtypes = [vp]
+        _lib = L
+        return L
+
+
+def check(rc: int) -> None:
+    if rc != V2M_OK:
+        msg = load().v2m_cuda_last_error().decode(errors="replace")
+        raise V2mError(rc, msg)

@@ -1,0 +1,110 @@
+"""Build the native libraries in-tree (they travel with the repository).
+
+  trussnet_b200/libv2m_cuda.so     the CUDA relaxation (csrc/*.cu), sm_100a, C ABI of
+                                   include/v2m_cuda.h
+  trussnet_b200/libv2m_relax_cl.so the C++ shim tn::relax_cl (csrc/relax_cl_shim.cpp),
+                                   built only where the reference headers are present
+
+Parity needs IEEE float arithmetic in the kernels: no FMA contraction
+(--fmad=false), correctly rounded division and square root (nvcc's defaults,
+kept explicit).
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libv2m_cuda.so")
+SHIM = os.path.join(HERE, "libv2m_relax_cl.so")
+REF = "/root/reference"
+
+NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "--fmad=false", "-prec-div=true",
+              "-prec-sqrt=true", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
+SOURCES = ["v2m_kernels.cu", "v2m_host.cu"]
+HEADERS = ["v2m_kernels.h", "v2m_types.cuh", "v2m_field.cuh"]
+
+
+def nvcc() -> str:
+    for c in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if c and os.path.exists(c):
+            return c
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(out: str, deps: list[str]) -> bool:
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build_cuda(force: bool = False, verbose: bool = False) -> str:
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "v2m_cuda.h"), __file__]
+    if not force and not _stale(LIB, deps):
+        return LIB
+    objs = []
+    logs = []
+    for src in SOURCES:
+        obj = os.path.join(CSRC, src.replace(".cu", ".o"))
+        cmd = [nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        logs.append(r.stdout + r.stderr)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src}:\n{r.stderr[-6000:]}")
+        objs.append(obj)
+    tmp = LIB + ".tmp"
+    cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp, *objs, "-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")
+    os.replace(tmp, LIB)
+    for o in objs:
+        os.remove(o)
+    with open(os.path.join(CSRC, "ptxas_info.txt"), "w") as f:
+        f.write("\n".join(line for log in logs for line in log.splitlines() if "ptxas" in line))
+    if verbose:
+        print("\n".join(logs))
+    return LIB
+
+
+def build_shim(force: bool = False) -> str | None:
+    """tn::relax_cl over the C ABI; compiled against the reference's headers
+    (src/v2m_particles.h, src/v2m_grid.h), so only where they exist."""
+    if not os.path.isdir(os.path.join(REF, "src")):
+        return SHIM if os.path.exists(SHIM) else None
+    src = os.path.join(CSRC, "relax_cl_shim.cpp")
+    if not os.path.exists(src):
+        return None
+    if not force and not _stale(SHIM, [src, LIB]):
+        return SHIM
+    cmd = ["/usr/bin/g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-I", os.path.join(REF, "src"), "-I",
+           os.path.join(ROOT, "include"), src, "-o", SHIM, "-L", HERE, "-lv2m_cuda", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"shim build failed:\n{r.stderr[-4000:]}")
+    return SHIM
+
+
+def build_oracle() -> None:
+    """The CPU checkers under oracle/ (test infrastructure)."""
+    env = dict(os.environ)
+    r = subprocess.run(["make", "-s", "-f", os.path.join(ROOT, "oracle", "Makefile"), "all"], capture_output=True,
+                       text=True, env=env)
+    if r.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{r.stdout[-3000:]}\n{r.stderr[-3000:]}")
+
+
+def build_all(force: bool = False) -> None:
+    build_cuda(force=force)
+    build_shim(force=force)
+    build_oracle()
+
+
+if __name__ == "__main__":
+    build_all(force="--force" in sys.argv)
+    print("built", LIB)

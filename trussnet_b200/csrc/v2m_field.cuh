@@ -1,0 +1,888 @@
+// v2m_field.cuh -- device-side point queries of the relaxation and the per-node
+// move, for sm_100a.
+//
+// These restate, for one CUDA thread per node, what the reference evaluates per
+// node in src/opencl/v2m_grid_body.cl:110-200 (brick-sparse phi lookups),
+// src/opencl/v2m_seed_body.cl:33-420 (labels near a point, owner label, psi and
+// its gradient, bracketed projections) and src/opencl/v2m_particle_body.cl
+// (crossing, glide, third label, valid branch, voxel trapping, move_step, move)
+// of fangq/trussnet. Every floating-point expression keeps the reference's
+// operand order; the library is compiled with --fmad=false and IEEE div/sqrt, so
+// a node's result is the reference CPU's bit for bit.
+//
+// Register-resident label lists: a brick's 16 labels are one 32-byte load kept
+// as 8 registers (LabList), so the label loops do not spill to local memory.
+#pragma once
+
+#include <cstdint>
+
+#include "v2m_types.cuh"
+
+namespace v2m {
+
+// ---- grid lookups ---------------------------------------------------------------
+__device__ __forceinline__ int label_at(const DGrid& g, int i, int j, int k) {
+    if (i < 0 || j < 0 || k < 0 || i >= g.nx || j >= g.ny || k >= g.nz) {
+        return 0;
+    }
+    return g.L[i + (size_t)g.nx * (j + (size_t)g.ny * k)];
+}
+
+__device__ __forceinline__ int brick_index(const DGrid& g, int i, int j, int k) {
+    return (i >> 3) + g.nbx * ((j >> 3) + g.nby * (k >> 3));
+}
+
+// The 16 labels of a brick as 8 packed registers.
+struct LabList {
+    uint32_t w[8];
+    __device__ __forceinline__ int get(int s) const {
+        return (int)((w[s >> 1] >> ((s & 1) * 16)) & 0xFFFFu);
+    }
+};
+
+__device__ __forceinline__ LabList load_labels(const DGrid& g, int b) {
+    const uint4* p = reinterpret_cast<const uint4*>(g.bl_lab + (size_t)b * V2M_BL);
+    const uint4 a = __ldg(p), c = __ldg(p + 1);
+    LabList r;
+    r.w[0] = a.x; r.w[1] = a.y; r.w[2] = a.z; r.w[3] = a.w;
+    r.w[4] = c.x; r.w[5] = c.y; r.w[6] = c.z; r.w[7] = c.w;
+    return r;
+}
+
+// Slot of label l in brick b (-1: uniform brick or l not listed); *has = listed.
+// (src/opencl/v2m_grid_body.cl:122-134)
+__device__ __forceinline__ int slot_lookup(const DGrid& g, int b, int l, int* has) {
+    const int n = __ldg(g.bl_cnt + b);
+    const LabList ll = load_labels(g, b);
+    *has = 0;
+    int idx = -1;
+#pragma unroll
+    for (int s = 0; s < V2M_BL; ++s) {
+        if (idx < 0 && s < n && ll.get(s) == l) {
+            idx = s;
+        }
+    }
+    if (idx < 0) {
+        return -1;
+    }
+    *has = 1;
+    const int first = __ldg(g.bl_slot + b);
+    return first < 0 ? -1 : first + idx;
+}
+
+// phi_l at voxel (i,j,k) (src/opencl/v2m_grid_body.cl:137-153)
+__device__ __forceinline__ float phi_voxel(const DGrid& g, int l, int i, int j, int k) {
+    if (i < 0 || j < 0 || k < 0 || i >= g.nx || j >= g.ny || k >= g.nz) {
+        return l == 0 ? 1.0f : 0.0f;
+    }
+    int has;
+    const int s = slot_lookup(g, brick_index(g, i, j, k), l, &has);
+    if (s < 0) {
+        return (has && g.L[i + (size_t)g.nx * (j + (size_t)g.ny * k)] == l) ? 1.0f : 0.0f;
+    }
+    return __ldg(g.phi + (size_t)s * V2M_SLOT + (i & 7) + V2M_BS * ((j & 7) + V2M_BS * (k & 7)));
+}
+
+// The 8 corners of phi_l's trilinear cell at (i0,j0,k0); corner bit 0 -> +i,
+// bit 1 -> +j, bit 2 -> +k (src/opencl/v2m_grid_body.cl:159-186).
+__device__ __forceinline__ void phi_corners(const DGrid& g, int l, int i0, int j0, int k0, float* c) {
+    if (i0 >= 0 && j0 >= 0 && k0 >= 0 && i0 + 1 < g.nx && j0 + 1 < g.ny && k0 + 1 < g.nz && (i0 & 7) != 7 &&
+        (j0 & 7) != 7 && (k0 & 7) != 7) {
+        int has;
+        const int s = slot_lookup(g, brick_index(g, i0, j0, k0), l, &has);
+        if (s >= 0) {
+            const float* base = g.phi + (size_t)s * V2M_SLOT + (i0 & 7) + V2M_BS * ((j0 & 7) + V2M_BS * (k0 & 7));
+#pragma unroll
+            for (int n = 0; n < 8; ++n) {
+                c[n] = __ldg(base + (n & 1) + V2M_BS * ((n >> 1) & 1) + V2M_BS * V2M_BS * (n >> 2));
+            }
+        } else {
+#pragma unroll
+            for (int n = 0; n < 8; ++n) {
+                c[n] = (has && g.L[(i0 + (n & 1)) + (size_t)g.nx * ((j0 + ((n >> 1) & 1)) + (size_t)g.ny * (k0 + (n >> 2)))] == l)
+                           ? 1.0f : 0.0f;
+            }
+        }
+        return;
+    }
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+        c[n] = phi_voxel(g, l, i0 + (n & 1), j0 + ((n >> 1) & 1), k0 + ((n >> 2) & 1));
+    }
+}
+
+// Trilinear blend of 8 corners at fractions (fx,fy,fz), the reference's order.
+__device__ __forceinline__ float trilerp8(const float* c, float fx, float fy, float fz) {
+    const float x00 = c[0] + fx * (c[1] - c[0]), x10 = c[2] + fx * (c[3] - c[2]);
+    const float x01 = c[4] + fx * (c[5] - c[4]), x11 = c[6] + fx * (c[7] - c[6]);
+    const float y0 = x00 + fy * (x10 - x00), y1 = x01 + fy * (x11 - x01);
+    return y0 + fz * (y1 - y0);
+}
+
+// phi_l trilinear at p (src/opencl/v2m_grid_body.cl:189-200)
+__device__ __forceinline__ float phi_point(const DGrid& g, int l, float px, float py, float pz) {
+    const float u = px / g.vx, v = py / g.vy, w = pz / g.vz;
+    const int i0 = (int)floorf(u), j0 = (int)floorf(v), k0 = (int)floorf(w);
+    const float fx = u - i0, fy = v - j0, fz = w - k0;
+    float c[8];
+    phi_corners(g, l, i0, j0, k0, c);
+    return trilerp8(c, fx, fy, fz);
+}
+
+// The labels that may appear at p: its brick's list (src/opencl/v2m_seed_body.cl:42-59).
+// Outside the grid: label 0 only.
+__device__ __forceinline__ int labels_near(const DGrid& g, float px, float py, float pz, LabList& out) {
+    const int i = (int)floorf(px / g.vx + 0.5f), j = (int)floorf(py / g.vy + 0.5f), k = (int)floorf(pz / g.vz + 0.5f);
+    if (i < 0 || j < 0 || k < 0 || i >= g.nx || j >= g.ny || k >= g.nz) {
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+            out.w[s] = 0u;
+        }
+        return 1;
+    }
+    const int b = brick_index(g, i, j, k);
+    const int c = __ldg(g.bl_cnt + b);
+    out = load_labels(g, b);
+    return c < V2M_BL ? c : V2M_BL;
+}
+
+// ---- gray-scale fields (src/opencl/v2m_seed_body.cl:65-114) ---------------------
+__device__ __forceinline__ float gray_sample(const DGrid& g, float px, float py, float pz, float* gr) {
+    const float u = px / g.vx, v = py / g.vy, w = pz / g.vz;
+    const int i0 = (int)floorf(u), j0 = (int)floorf(v), k0 = (int)floorf(w);
+    const float fx = u - i0, fy = v - j0, fz = w - k0;
+    const float outside = g.gTW[0] - g.gTW[g.gm];
+    float c[8];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+        const int ii = i0 + (n & 1), jj = j0 + ((n >> 1) & 1), kk = k0 + ((n >> 2) & 1);
+        c[n] = (ii < 0 || jj < 0 || kk < 0 || ii >= g.nx || jj >= g.ny || kk >= g.nz)
+                   ? outside : __ldg(g.gI + ii + (size_t)g.nx * (jj + (size_t)g.ny * kk));
+    }
+    const float x00 = c[0] + fx * (c[1] - c[0]), x10 = c[2] + fx * (c[3] - c[2]);
+    const float x01 = c[4] + fx * (c[5] - c[4]), x11 = c[6] + fx * (c[7] - c[6]);
+    const float y0 = x00 + fy * (x10 - x00), y1 = x01 + fy * (x11 - x01);
+    if (gr) {
+        const float dx0 = (c[1] - c[0]) + fy * ((c[3] - c[2]) - (c[1] - c[0]));
+        const float dx1 = (c[5] - c[4]) + fy * ((c[7] - c[6]) - (c[5] - c[4]));
+        gr[0] = (dx0 + fz * (dx1 - dx0)) / g.vx;
+        gr[1] = ((x10 - x00) + fz * ((x11 - x01) - (x10 - x00))) / g.vy;
+        gr[2] = (y1 - y0) / g.vz;
+    }
+    return y0 + fz * (y1 - y0);
+}
+
+// psi_ab straight from the intensity for adjacent gray labels; 0 if not applicable
+__device__ __forceinline__ int gray_psi(const DGrid& g, int a, int b, float px, float py, float pz, float* val, float* gr) {
+    if (g.gm <= 0 || (a - b != 1 && b - a != 1)) {
+        return 0;
+    }
+    const int k = a < b ? a : b;
+    const float sg = (a > b ? 2.0f : -2.0f) / g.gTW[g.gm + k];
+    *val = sg * (gray_sample(g, px, py, pz, gr) - g.gTW[k]);
+    if (gr) {
+        gr[0] *= sg;
+        gr[1] *= sg;
+        gr[2] *= sg;
+    }
+    return 1;
+}
+
+// The label owning p: argmax phi_l (smooth mode) or the voxel's label (voxel
+// mode), with the runner-up and the margin (src/opencl/v2m_seed_body.cl:116-175).
+__device__ __forceinline__ int owner_label(const DGrid& g, int voxmode, float px, float py, float pz, int* second,
+                                           float* margin) {
+    const int i = (int)floorf(px / g.vx + 0.5f), j = (int)floorf(py / g.vy + 0.5f), k = (int)floorf(pz / g.vz + 0.5f);
+    if (g.gm > 0 && !voxmode) {
+        const float I = gray_sample(g, px, py, pz, nullptr);
+        int l = 0;
+        while (l < g.gm && I >= g.gTW[l]) {
+            ++l;
+        }
+        const float dl = l > 0 ? (I - g.gTW[l - 1]) / g.gTW[g.gm + l - 1] : 1e30f;
+        const float du = l < g.gm ? (g.gTW[l] - I) / g.gTW[g.gm + l] : 1e30f;
+        *second = (dl < du) ? l - 1 : (l < g.gm ? l + 1 : V2M_NOLAB);
+        *margin = 2.0f * fminf(dl, du);
+        return l;
+    }
+    LabList ll;
+    const int n = labels_near(g, px, py, pz, ll);
+    int best = ll.get(0), sec = V2M_NOLAB;
+    float pb = -1.0f, ps = pb;
+    if (n == 1) {
+        *second = V2M_NOLAB;
+        *margin = 1.0f;
+        return best;
+    }
+#pragma unroll 1
+    for (int s = 0; s < n; ++s) {
+        const int ls = ll.get(s);
+        const float v = phi_point(g, ls, px, py, pz);
+        if (v > pb) {
+            ps = pb;
+            sec = best;
+            pb = v;
+            best = ls;
+        } else if (v > ps) {
+            ps = v;
+            sec = ls;
+        }
+    }
+    *second = sec;
+    *margin = pb - ps;
+    if (voxmode) {
+        return label_at(g, i, j, k);
+    }
+    return best;
+}
+
+// psi_ab = phi_a - phi_b at p (src/opencl/v2m_seed_body.cl:179-205)
+__device__ __forceinline__ float psi(const DGrid& g, int a, int b, float px, float py, float pz) {
+    float gv;
+    if (gray_psi(g, a, b, px, py, pz, &gv, nullptr)) {
+        return gv;
+    }
+    const float u = px / g.vx, v = py / g.vy, w = pz / g.vz;
+    const int i0 = (int)floorf(u), j0 = (int)floorf(v), k0 = (int)floorf(w);
+    const float fx = u - i0, fy = v - j0, fz = w - k0;
+    float c[8], e[8];
+    phi_corners(g, a, i0, j0, k0, c);
+    phi_corners(g, b, i0, j0, k0, e);
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+        c[n] -= e[n];
+    }
+    return trilerp8(c, fx, fy, fz);
+}
+
+// psi_ab and its cell-analytic gradient (src/opencl/v2m_seed_body.cl:211-247)
+__device__ __forceinline__ float psi_grad(const DGrid& g, int a, int b, float px, float py, float pz, float* gr) {
+    float gv;
+    if (gray_psi(g, a, b, px, py, pz, &gv, gr)) {
+        return gv;
+    }
+    const float u = px / g.vx, v = py / g.vy, w = pz / g.vz;
+    const int i0 = (int)floorf(u), j0 = (int)floorf(v), k0 = (int)floorf(w);
+    const float fx = u - i0, fy = v - j0, fz = w - k0;
+    float c[8], e[8];
+    phi_corners(g, a, i0, j0, k0, c);
+    phi_corners(g, b, i0, j0, k0, e);
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+        c[n] -= e[n];
+    }
+    const float x00 = c[0] + fx * (c[1] - c[0]), x10 = c[2] + fx * (c[3] - c[2]);
+    const float x01 = c[4] + fx * (c[5] - c[4]), x11 = c[6] + fx * (c[7] - c[6]);
+    const float y0 = x00 + fy * (x10 - x00), y1 = x01 + fy * (x11 - x01);
+    const float dx0 = (c[1] - c[0]) + fy * ((c[3] - c[2]) - (c[1] - c[0]));
+    const float dx1 = (c[5] - c[4]) + fy * ((c[7] - c[6]) - (c[5] - c[4]));
+    gr[0] = (dx0 + fz * (dx1 - dx0)) / g.vx;
+    gr[1] = ((x10 - x00) + fz * ((x11 - x01) - (x10 - x00))) / g.vy;
+    gr[2] = (y1 - y0) / g.vz;
+    return y0 + fz * (y1 - y0);
+}
+
+// Bracketed root of psi_ab along unit direction u from p, within rad: doubling
+// probes from the Newton guess tg, then Illinois regula falsi
+// (src/opencl/v2m_seed_body.cl:255-320). Moves p and returns 1 on success.
+__device__ __noinline__ int bisect_dir(const DGrid& g, int a, int b, float* p, const float* u, float v0, float rad,
+                                       float tg) {
+    if (v0 == 0.0f) {
+        return 1;
+    }
+    const float sg = v0 > 0.0f ? -1.0f : 1.0f;
+    float t0 = 0.0f, t1 = -1.0f, f0 = v0, f1 = 0.0f;
+    float t = (tg > 0.0f && tg < rad) ? tg : 0.25f * rad;
+    for (int k = 0; k < 8; ++k) {
+        const float v = psi(g, a, b, p[0] + sg * t * u[0], p[1] + sg * t * u[1], p[2] + sg * t * u[2]);
+        if ((v > 0.0f) != (v0 > 0.0f) || v == 0.0f) {
+            t1 = t;
+            f1 = v;
+            break;
+        }
+        t0 = t;
+        f0 = v;
+        if (t >= rad) {
+            break;
+        }
+        t = fminf(2.0f * t, rad);
+    }
+    if (t1 < 0.0f) {
+        return 0;
+    }
+    int side = 0;
+    for (int it = 0; it < 8 && f1 != 0.0f && fabsf(t1 - t0) > 1e-4f * rad; ++it) {
+        const float tm = (f0 != f1) ? t1 - f1 * (t1 - t0) / (f1 - f0) : 0.5f * (t0 + t1);
+        const float v = psi(g, a, b, p[0] + sg * tm * u[0], p[1] + sg * tm * u[1], p[2] + sg * tm * u[2]);
+        if ((v > 0.0f) == (f1 > 0.0f)) {
+            t1 = tm;
+            f1 = v;
+            if (side == -1) {
+                f0 *= 0.5f;
+            }
+            side = -1;
+        } else {
+            t0 = t1;
+            f0 = f1;
+            t1 = tm;
+            f1 = v;
+            side = 1;
+        }
+    }
+    for (int k = 0; k < 3; ++k) {
+        p[k] += sg * t1 * u[k];
+    }
+    return 1;
+}
+
+// Projection onto psi_ab = 0 along the local normal within rad (src/opencl/v2m_seed_body.cl:324-335)
+__device__ __noinline__ int project1(const DGrid& g, int a, int b, float* p, float rad) {
+    float gr[3];
+    const float v = psi_grad(g, a, b, p[0], p[1], p[2], gr);
+    const float gn = sqrtf(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
+    if (gn < 1e-9f) {
+        return 0;
+    }
+    const float u[3] = { gr[0] / gn, gr[1] / gn, gr[2] / gn };
+    return bisect_dir(g, a, b, p, u, v, rad, 1.5f * fabsf(v) / gn);
+}
+
+// Projection onto the junction curve psi_ab = psi_ac = 0 by alternating
+// bracketed legs (src/opencl/v2m_seed_body.cl:342-420, sampled fields).
+__device__ __noinline__ int project2(const DGrid& g, int a, int b, int c, float* p, float rad) {
+    float q[3] = { p[0], p[1], p[2] };
+    for (int it = 0; it < 3; ++it) {
+        float g1[3], g2[3];
+        if (!project1(g, a, b, q, rad)) {
+            return 0;
+        }
+        psi_grad(g, a, b, q[0], q[1], q[2], g1);
+        const float v2 = psi_grad(g, a, c, q[0], q[1], q[2], g2);
+        const float a11 = g1[0] * g1[0] + g1[1] * g1[1] + g1[2] * g1[2];
+        if (a11 < 1e-18f) {
+            return 0;
+        }
+        const float pr = (g1[0] * g2[0] + g1[1] * g2[1] + g1[2] * g2[2]) / a11;
+        float u[3] = { g2[0] - pr * g1[0], g2[1] - pr * g1[1], g2[2] - pr * g1[2] };
+        const float un = sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+        if (un < 1e-9f) {
+            return 0;
+        }
+        u[0] /= un;
+        u[1] /= un;
+        u[2] /= un;
+        if (!bisect_dir(g, a, c, q, u, v2, rad, 1.5f * fabsf(v2) / un)) {
+            return 0;
+        }
+    }
+    if (!project1(g, a, b, q, rad)) {
+        return 0;
+    }
+    const float m2 = (q[0] - p[0]) * (q[0] - p[0]) + (q[1] - p[1]) * (q[1] - p[1]) + (q[2] - p[2]) * (q[2] - p[2]);
+    if (m2 > rad * rad) {
+        return 0;
+    }
+    p[0] = q[0];
+    p[1] = q[1];
+    p[2] = q[2];
+    return 1;
+}
+
+// Crossing of p -> q with psi_ab = 0: 6 bisections and a secant (src/opencl/v2m_particle_body.cl:188-212)
+__device__ __noinline__ void crossing(const DGrid& g, int a, int b, const float* p, const float* q, float* c) {
+    float t0 = 0.0f, t1 = 1.0f;
+    float v0 = psi(g, a, b, p[0], p[1], p[2]);
+    float v1 = psi(g, a, b, q[0], q[1], q[2]);
+    for (int it = 0; it < 6; ++it) {
+        const float tm = 0.5f * (t0 + t1);
+        const float vm = psi(g, a, b, p[0] + tm * (q[0] - p[0]), p[1] + tm * (q[1] - p[1]), p[2] + tm * (q[2] - p[2]));
+        if (vm > 0.0f) {
+            t0 = tm;
+            v0 = vm;
+        } else {
+            t1 = tm;
+            v1 = vm;
+        }
+    }
+    const float t = (v0 - v1) != 0.0f ? t0 + (t1 - t0) * v0 / (v0 - v1) : 0.5f * (t0 + t1);
+    for (int k = 0; k < 3; ++k) {
+        c[k] = p[k] + t * (q[k] - p[k]);
+    }
+}
+
+// Drop v's component along psi_ab's normal at p (src/opencl/v2m_particle_body.cl:215-229)
+__device__ __forceinline__ void tangential(const DGrid& g, int a, int b, const float* p, float* v) {
+    float gr[3];
+    psi_grad(g, a, b, p[0], p[1], p[2], gr);
+    const float gn2 = gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2];
+    if (gn2 < 1e-12f) {
+        return;
+    }
+    const float vn = (v[0] * gr[0] + v[1] * gr[1] + v[2] * gr[2]) / gn2;
+    for (int k = 0; k < 3; ++k) {
+        v[k] -= vn * gr[k];
+    }
+}
+
+// A third label competing at q (phi_c > 0.5 phi_a), or NOLAB (src/opencl/v2m_particle_body.cl:232-260)
+__device__ __noinline__ int third_label(const DGrid& g, int a, int b, const float* q) {
+    LabList ll;
+    const int n = labels_near(g, q[0], q[1], q[2], ll);
+    int other = 0;
+#pragma unroll
+    for (int s = 0; s < V2M_BL; ++s) {
+        if (s < n) {
+            const int l = ll.get(s);
+            other |= l != a && l != b;
+        }
+    }
+    if (!other) {
+        return V2M_NOLAB;
+    }
+    const float pa = phi_point(g, a, q[0], q[1], q[2]);
+    int c = V2M_NOLAB;
+    float pc = 0.5f * pa;
+#pragma unroll 1
+    for (int s = 0; s < n; ++s) {
+        const int l = ll.get(s);
+        if (l != a && l != b) {
+            const float w = phi_point(g, l, q[0], q[1], q[2]);
+            if (w > pc) {
+                pc = w;
+                c = l;
+            }
+        }
+    }
+    return c;
+}
+
+// Do the node's labels dominate at q? (src/opencl/v2m_particle_body.cl:266-291)
+__device__ __noinline__ int valid_on(const DGrid& g, int a, int b, int c, const float* q) {
+    LabList ll;
+    const int n = labels_near(g, q[0], q[1], q[2], ll);
+    int other = 0;
+#pragma unroll
+    for (int s = 0; s < V2M_BL; ++s) {
+        if (s < n) {
+            const int l = ll.get(s);
+            other |= l != a && l != b && l != c;
+        }
+    }
+    if (!other) {
+        return 1;
+    }
+    float mine = fminf(phi_point(g, a, q[0], q[1], q[2]), phi_point(g, b, q[0], q[1], q[2]));
+    if (c != V2M_NOLAB) {
+        mine = fminf(mine, phi_point(g, c, q[0], q[1], q[2]));
+    }
+#pragma unroll 1
+    for (int s = 0; s < n; ++s) {
+        const int l = ll.get(s);
+        if (l != a && l != b && l != c && phi_point(g, l, q[0], q[1], q[2]) > mine + 0.02f) {
+            return 0;
+        }
+    }
+    return 1;
+}
+
+// ---- voxel trap mode (src/opencl/v2m_particle_body.cl:358-650) -------------------
+// Walk p -> p + s through label-a voxels (one face at a time); on the first face
+// into another label write the face point to x, that label to *lb and return
+// the ray fraction; -1 if the step stays inside label a.
+__device__ __noinline__ float dda_hit(const DGrid& g, int a, const float* p, const float* s, float* x, int* lb) {
+    const float vsz[3] = { g.vx, g.vy, g.vz };
+    float u[3], w[3];
+    int id[3];
+    for (int k = 0; k < 3; ++k) {
+        u[k] = p[k] / vsz[k] + 0.5f;
+        w[k] = s[k] / vsz[k];
+        id[k] = (int)floorf(u[k]);
+    }
+    int l = label_at(g, id[0], id[1], id[2]);
+    if (l != a) {
+        x[0] = p[0];
+        x[1] = p[1];
+        x[2] = p[2];
+        *lb = l;
+        return 0.0f;
+    }
+    float t = 0.0f;
+    for (int it = 0; it < 64; ++it) {
+        float ht[3];
+        for (int k = 0; k < 3; ++k) {
+            ht[k] = w[k] != 0.0f ? fabsf(((float)id[k] + (w[k] > 0.0f ? 1.0f : 0.0f) - u[k]) / w[k]) : 1e30f;
+        }
+        const float dt = fminf(fminf(ht[0], ht[1]), ht[2]);
+        const int ax = dt == ht[0] ? 0 : (dt == ht[1] ? 1 : 2);
+        if (t + dt >= 1.0f) {
+            return -1.0f;
+        }
+        t += dt;
+        for (int k = 0; k < 3; ++k) {
+            u[k] += dt * w[k];
+        }
+        u[ax] = (float)id[ax] + (w[ax] > 0.0f ? 1.0f : 0.0f);
+        id[ax] += w[ax] > 0.0f ? 1 : -1;
+        l = label_at(g, id[0], id[1], id[2]);
+        if (l != a) {
+            for (int k = 0; k < 3; ++k) {
+                x[k] = (u[k] - 0.5f) * vsz[k];
+            }
+            *lb = l;
+            return t;
+        }
+    }
+    return -1.0f;
+}
+
+// Nearest point to q on the a|b voxel faces (c == NOLAB) or on the a|b|c voxel
+// edges, within R voxels; squared distance or -1 (src/opencl/v2m_particle_body.cl:437-529).
+__device__ __noinline__ float vox_nearest(const DGrid& g, int a, int b, int c, const float* q, int R, float* out) {
+    const float vsz[3] = { g.vx, g.vy, g.vz };
+    float u[3];
+    int ci[3];
+    for (int k = 0; k < 3; ++k) {
+        u[k] = q[k] / vsz[k] + 0.5f;
+        ci[k] = (int)floorf(u[k]);
+    }
+    float best = -1.0f;
+    for (int vk = ci[2] - R; vk <= ci[2] + R; ++vk)
+        for (int vj = ci[1] - R; vj <= ci[1] + R; ++vj)
+            for (int vi = ci[0] - R; vi <= ci[0] + R; ++vi) {
+                if (label_at(g, vi, vj, vk) != a) {
+                    continue;
+                }
+                const int v[3] = { vi, vj, vk };
+                for (int ax = 0; ax < 3; ++ax) {
+                    const int o1 = (ax + 1) % 3, o2 = (ax + 2) % 3;
+                    if (c == V2M_NOLAB) {
+                        for (int sd = 0; sd < 2; ++sd) {
+                            int nn[3] = { v[0], v[1], v[2] };
+                            nn[ax] += sd ? 1 : -1;
+                            if (label_at(g, nn[0], nn[1], nn[2]) != b) {
+                                continue;
+                            }
+                            float y[3];
+                            y[ax] = (float)(v[ax] + sd);
+                            y[o1] = fminf(fmaxf(u[o1], (float)v[o1]), (float)(v[o1] + 1));
+                            y[o2] = fminf(fmaxf(u[o2], (float)v[o2]), (float)(v[o2] + 1));
+                            float d2 = 0.0f;
+                            for (int k = 0; k < 3; ++k) {
+                                y[k] = (y[k] - 0.5f) * vsz[k];
+                                d2 += (y[k] - q[k]) * (y[k] - q[k]);
+                            }
+                            if (best < 0.0f || d2 < best) {
+                                best = d2;
+                                out[0] = y[0];
+                                out[1] = y[1];
+                                out[2] = y[2];
+                            }
+                        }
+                    } else {
+                        for (int e = 0; e < 4; ++e) {
+                            const int e1 = e & 1, e2 = e >> 1;
+                            int hb = 0, hc = 0;
+                            for (int m = 0; m < 4; ++m) {
+                                int nn[3] = { v[0], v[1], v[2] };
+                                nn[o1] += e1 - 1 + (m & 1);
+                                nn[o2] += e2 - 1 + (m >> 1);
+                                const int ln = label_at(g, nn[0], nn[1], nn[2]);
+                                hb |= ln == b;
+                                hc |= ln == c;
+                            }
+                            if (!hb || !hc) {
+                                continue;
+                            }
+                            float y[3];
+                            y[ax] = fminf(fmaxf(u[ax], (float)v[ax]), (float)(v[ax] + 1));
+                            y[o1] = (float)(v[o1] + e1);
+                            y[o2] = (float)(v[o2] + e2);
+                            float d2 = 0.0f;
+                            for (int k = 0; k < 3; ++k) {
+                                y[k] = (y[k] - 0.5f) * vsz[k];
+                                d2 += (y[k] - q[k]) * (y[k] - q[k]);
+                            }
+                            if (best < 0.0f || d2 < best) {
+                                best = d2;
+                                out[0] = y[0];
+                                out[1] = y[1];
+                                out[2] = y[2];
+                            }
+                        }
+                    }
+                }
+            }
+    return best;
+}
+
+__device__ __forceinline__ int vox_third(const DGrid& g, int a, int b, const float* p) {
+    const int i0 = (int)floorf(p[0] / g.vx), j0 = (int)floorf(p[1] / g.vy), k0 = (int)floorf(p[2] / g.vz);
+    for (int m = 0; m < 8; ++m) {
+        const int l = label_at(g, i0 + (m & 1), j0 + ((m >> 1) & 1), k0 + (m >> 2));
+        if (l != a && l != b) {
+            return l;
+        }
+    }
+    return V2M_NOLAB;
+}
+
+// ---- the size field at a point ----------------------------------------------------
+// hmode 0: the nearest voxel, clamped (src/opencl/v2m_particle_body.cl:30-36);
+// hmode 1: trilinear between voxel centres, clamped to the grid (extension).
+__device__ __forceinline__ float size_at(const DGrid& g, int hmode, float px, float py, float pz) {
+    if (hmode == 0) {
+        int i = (int)floorf(px / g.vx + 0.5f), j = (int)floorf(py / g.vy + 0.5f), k = (int)floorf(pz / g.vz + 0.5f);
+        i = i < 0 ? 0 : (i >= g.nx ? g.nx - 1 : i);
+        j = j < 0 ? 0 : (j >= g.ny ? g.ny - 1 : j);
+        k = k < 0 ? 0 : (k >= g.nz ? g.nz - 1 : k);
+        return __ldg(g.hvox + i + (size_t)g.nx * (j + (size_t)g.ny * k));
+    }
+    float u = px / g.vx, v = py / g.vy, w = pz / g.vz;
+    u = fminf(fmaxf(u, 0.0f), (float)(g.nx - 1));
+    v = fminf(fmaxf(v, 0.0f), (float)(g.ny - 1));
+    w = fminf(fmaxf(w, 0.0f), (float)(g.nz - 1));
+    int i0 = (int)floorf(u), j0 = (int)floorf(v), k0 = (int)floorf(w);
+    i0 = i0 > g.nx - 2 ? (g.nx > 1 ? g.nx - 2 : 0) : i0;
+    j0 = j0 > g.ny - 2 ? (g.ny > 1 ? g.ny - 2 : 0) : j0;
+    k0 = k0 > g.nz - 2 ? (g.nz > 1 ? g.nz - 2 : 0) : k0;
+    const float fx = u - i0, fy = v - j0, fz = w - k0;
+    const int i1 = i0 + 1 < g.nx ? i0 + 1 : i0, j1 = j0 + 1 < g.ny ? j0 + 1 : j0, k1 = k0 + 1 < g.nz ? k0 + 1 : k0;
+    float c[8];
+    const int ii[2] = { i0, i1 }, jj[2] = { j0, j1 }, kk[2] = { k0, k1 };
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+        c[n] = __ldg(g.hvox + ii[n & 1] + (size_t)g.nx * (jj[(n >> 1) & 1] + (size_t)g.ny * kk[n >> 2]));
+    }
+    return trilerp8(c, fx, fy, fz);
+}
+
+// ---- the move --------------------------------------------------------------------
+// Node state a move reads and writes, held in registers.
+struct NodeState {
+    float p[3];   // position
+    int a;        // own label
+    int ty;       // type
+    int pb, pc;   // partner labels (part[2i], part[2i+1])
+    float hn;     // h at the node
+};
+
+// Voxel-mode move with step s (src/opencl/v2m_particle_body.cl:549-650).
+__device__ __noinline__ float move_voxel(const DGrid& g, int hmode, float h, float snap, const float* s, NodeState& st) {
+    const float vmin = fminf(fminf(g.vx, g.vy), g.vz);
+    float p[3], q[3], x[3];
+    p[0] = st.p[0];
+    p[1] = st.p[1];
+    p[2] = st.p[2];
+    const int a = st.a;
+    int ty = st.ty, b = st.pb, c = st.pc;
+    const float sl = sqrtf(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    const int R = 1 + (int)ceilf(sl / vmin);
+    for (int k = 0; k < 3; ++k) {
+        q[k] = p[k] + s[k];
+    }
+    if (ty == V2M_INTERIOR) {
+        int l;
+        const float t = dda_hit(g, a, p, s, x, &l);
+        if (t >= 0.0f) {
+            b = l;
+            if (vox_nearest(g, a, b, V2M_NOLAB, q, R, q) < 0.0f) {
+                q[0] = x[0];
+                q[1] = x[1];
+                q[2] = x[2];
+            }
+            ty = V2M_INTERFACE;
+        } else if (snap > 0.0f) {
+            const int Rs = 1 + (int)ceilf(snap * h / vmin);
+            float best = -1.0f, y[3];
+            for (int dz = -1; dz <= 1; ++dz)
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        const int l2 = label_at(g, (int)floorf(q[0] / g.vx + 0.5f) + dx * Rs,
+                                                (int)floorf(q[1] / g.vy + 0.5f) + dy * Rs,
+                                                (int)floorf(q[2] / g.vz + 0.5f) + dz * Rs);
+                        if (l2 == a || l2 == b) {
+                            continue;
+                        }
+                        const float d2 = vox_nearest(g, a, l2, V2M_NOLAB, q, Rs, y);
+                        if (d2 >= 0.0f && d2 < snap * snap * h * h && (best < 0.0f || d2 < best)) {
+                            best = d2;
+                            b = l2;
+                            x[0] = y[0];
+                            x[1] = y[1];
+                            x[2] = y[2];
+                        }
+                    }
+            if (best >= 0.0f) {
+                q[0] = x[0];
+                q[1] = x[1];
+                q[2] = x[2];
+                ty = V2M_INTERFACE;
+            }
+        }
+    } else if (ty == V2M_INTERFACE) {
+        if (vox_nearest(g, a, b, V2M_NOLAB, q, R, q) < 0.0f) {
+            return 0.0f;
+        }
+    } else {
+        if (vox_nearest(g, a, b, c, q, R, q) < 0.0f) {
+            return 0.0f;
+        }
+    }
+    if (ty == V2M_INTERFACE) {
+        const int cc = vox_third(g, a, b, q);
+        if (cc != V2M_NOLAB) {
+            float r[3];
+            const float d2 = vox_nearest(g, a, b, cc, q, 1, r);
+            if (d2 >= 0.0f && d2 < 0.0625f * h * h) {
+                q[0] = r[0];
+                q[1] = r[1];
+                q[2] = r[2];
+                ty = V2M_JUNCTION;
+                c = cc;
+            }
+        }
+    }
+    const float mv = sqrtf((q[0] - p[0]) * (q[0] - p[0]) + (q[1] - p[1]) * (q[1] - p[1]) + (q[2] - p[2]) * (q[2] - p[2]));
+    st.p[0] = q[0];
+    st.p[1] = q[1];
+    st.p[2] = q[2];
+    st.ty = ty;
+    st.pb = ty == V2M_INTERIOR ? V2M_NOLAB : b;
+    st.pc = ty >= V2M_JUNCTION ? c : V2M_NOLAB;
+    st.hn = size_at(g, hmode, q[0], q[1], q[2]);
+    return mv / h;
+}
+
+// The trapped move with the (capped) step s (src/opencl/v2m_particle_body.cl:659-833).
+// ty0 is the type before the move; st is updated in place exactly where the
+// reference writes the node's arrays.
+__device__ __noinline__ float move_step(const DGrid& g, int hmode, float h, float* s, float maxstep, float snap,
+                                        int voxmode, NodeState& st) {
+    float p[3], q[3];
+    p[0] = st.p[0];
+    p[1] = st.p[1];
+    p[2] = st.p[2];
+    const int a = st.a;
+    const int ty_in = st.ty;
+    int ty = ty_in;
+    if (voxmode) {
+        return move_voxel(g, hmode, h, snap, s, st);
+    }
+    int b = st.pb;
+    const int c = st.pc;
+    if (ty == V2M_INTERIOR) {
+        for (int k = 0; k < 3; ++k) {
+            q[k] = p[k] + s[k];
+        }
+        int sec;
+        float mg;
+        const int l = owner_label(g, 0, q[0], q[1], q[2], &sec, &mg);
+        if (l != a) {
+            b = l;
+            float x[3], r[3];
+            crossing(g, a, b, p, q, x);
+            for (int k = 0; k < 3; ++k) {
+                r[k] = q[k] - x[k];
+            }
+            tangential(g, a, b, x, r);
+            for (int k = 0; k < 3; ++k) {
+                q[k] = x[k] + r[k];
+            }
+            if (!project1(g, a, b, q, 0.5f * h)) {
+                q[0] = x[0];
+                q[1] = x[1];
+                q[2] = x[2];
+            }
+            ty = V2M_INTERFACE;
+            st.pb = b;
+        } else if (sec != V2M_NOLAB && snap > 0.0f) {
+            float gq[3];
+            const float v = psi_grad(g, a, sec, q[0], q[1], q[2], gq);
+            const float gn = sqrtf(gq[0] * gq[0] + gq[1] * gq[1] + gq[2] * gq[2]);
+            if (gn > 1e-9f && v / gn < snap * h && project1(g, a, sec, q, 1.2f * snap * h)) {
+                ty = V2M_INTERFACE;
+                b = sec;
+                st.pb = sec;
+            }
+        }
+    } else if (ty == V2M_INTERFACE) {
+        tangential(g, a, b, p, s);
+        for (int k = 0; k < 3; ++k) {
+            q[k] = p[k] + s[k];
+        }
+        if (!project1(g, a, b, q, 0.5f * h)) {
+            return 0.0f;
+        }
+    } else {
+        float g1[3], g2[3], td[3];
+        psi_grad(g, a, b, p[0], p[1], p[2], g1);
+        psi_grad(g, a, c, p[0], p[1], p[2], g2);
+        td[0] = g1[1] * g2[2] - g1[2] * g2[1];
+        td[1] = g1[2] * g2[0] - g1[0] * g2[2];
+        td[2] = g1[0] * g2[1] - g1[1] * g2[0];
+        const float tl2 = td[0] * td[0] + td[1] * td[1] + td[2] * td[2];
+        const float stp = tl2 > 1e-20f ? (s[0] * td[0] + s[1] * td[1] + s[2] * td[2]) / tl2 : 0.0f;
+        for (int k = 0; k < 3; ++k) {
+            q[k] = p[k] + stp * td[k];
+        }
+        if (!project2(g, a, b, c, q, 0.5f * h)) {
+            return 0.0f;
+        }
+    }
+    // an interface node meeting a third label joins the junction curve
+    if (ty == V2M_INTERFACE) {
+        const int cc = third_label(g, a, b, q);
+        if (cc != V2M_NOLAB) {
+            float r[3] = { q[0], q[1], q[2] };
+            if (project2(g, a, b, cc, r, 0.5f * h)) {
+                q[0] = r[0];
+                q[1] = r[1];
+                q[2] = r[2];
+                ty = V2M_JUNCTION;
+                st.pc = cc;
+            }
+        }
+    }
+    // safety net: a displacement beyond the step cap plus the projection reach (or NaN) stays
+    {
+        const float lim = (maxstep + fmaxf(snap, 0.5f)) * h;
+        const float m2 = (q[0] - p[0]) * (q[0] - p[0]) + (q[1] - p[1]) * (q[1] - p[1]) + (q[2] - p[2]) * (q[2] - p[2]);
+        if (!(m2 <= lim * lim)) {
+            if (ty_in == V2M_INTERIOR) {
+                st.pb = V2M_NOLAB;
+            }
+            return 0.0f;
+        }
+    }
+    // refuse a move onto an invalid branch of the constraint
+    if (ty != V2M_INTERIOR && !valid_on(g, a, st.pb, ty >= V2M_JUNCTION ? st.pc : V2M_NOLAB, q)) {
+        if (ty == V2M_INTERFACE || ty_in == V2M_INTERIOR) {
+            const int cc = third_label(g, a, st.pb, q);
+            float r[3] = { q[0], q[1], q[2] };
+            if (cc != V2M_NOLAB && project2(g, a, st.pb, cc, r, 0.5f * h) && valid_on(g, a, st.pb, cc, r)) {
+                q[0] = r[0];
+                q[1] = r[1];
+                q[2] = r[2];
+                ty = V2M_JUNCTION;
+                st.pc = cc;
+            } else {
+                // the node keeps its old type (an interior one drops its partner)
+                if (ty_in == V2M_INTERIOR) {
+                    st.pb = V2M_NOLAB;
+                }
+                return 0.0f;
+            }
+        } else {
+            return 0.0f;
+        }
+    }
+    const float mv = sqrtf((q[0] - p[0]) * (q[0] - p[0]) + (q[1] - p[1]) * (q[1] - p[1]) + (q[2] - p[2]) * (q[2] - p[2]));
+    st.p[0] = q[0];
+    st.p[1] = q[1];
+    st.p[2] = q[2];
+    st.ty = ty;
+    st.hn = size_at(g, hmode, q[0], q[1], q[2]);
+    return mv / h;
+}
+
+}  // namespace v2m

@@ -1,0 +1,1092 @@
+// v2m_host.cu -- host side of libv2m_cuda.so: sessions, the iteration loop
+// (plain launches or a captured CUDA graph) and the C ABI of include/v2m_cuda.h.
+//
+// The loop mirrors relax_cl / relax_cpu (src/v2m_gpu.cpp:116-553,
+// src/v2m_particles.cpp:728-976 of fangq/trussnet) with one difference of
+// structure: the per-iteration decisions (FIRE step, convergence, Verlet
+// rebuild) are taken on the device by k_control, so an iteration needs no host
+// round trip and a run of iterations replays as one graph. The host reads the
+// per-volume control blocks only between graph replays, to stop early.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/v2m_cuda.h"
+#include "v2m_kernels.h"
+
+using namespace v2m;
+
+namespace {
+
+thread_local std::string g_err;
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct ArgError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct KernelError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void ck(cudaError_t e, const char* where) {
+    if (e != cudaSuccess) {
+        throw CudaError(std::string(where) + ": CUDA error " + std::to_string((int)e) + " (" + cudaGetErrorString(e) + ")");
+    }
+}
+
+int64_t align_up(int64_t x, int64_t a) {
+    return (x + a - 1) / a * a;
+}
+
+int env_int(const char* name, int dflt) {
+    const char* e = std::getenv(name);
+    return e ? std::atoi(e) : dflt;
+}
+
+// Per-volume host bookkeeping.
+struct VolInfo {
+    int n = 0, nkeys = 0;
+    int64_t nofs = 0, kofs = 0;
+    int max_iters = 0;
+    int hmode = 0;
+};
+
+}  // namespace
+
+struct v2m_session {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int nvol = 0;
+    std::vector<DVol> hvols;
+    std::vector<VolInfo> info;
+    std::vector<v2m_relax_params> prm;
+    Dev d;
+    std::vector<void*> allocs;
+    float4* Pq0 = nullptr;
+    uint8_t* typ0 = nullptr;
+    uint32_t* part0 = nullptr;
+    VolCtl* ctl_init = nullptr;
+    int serial_power = 0;
+    int force_threads = 256;
+    int refresh_blocks = 0;
+    int max_iters = 0;
+    int graph_iters = 10;
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<cudaEvent_t> gev;   // force start/stop events recorded inside the graph
+    int64_t launches = 0, force_launches = 0;
+    double force_ms = 0.0;
+    int time_force = 0;
+    double ms_hash = 0.0, ms_loop = 0.0;
+
+    template <typename T>
+    T* alloc(size_t count) {
+        void* p = nullptr;
+        const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+        ck(cudaMalloc(&p, bytes), "cudaMalloc");
+        allocs.push_back(p);
+        return static_cast<T*>(p);
+    }
+
+    ~v2m_session() {
+        if (gexec) {
+            cudaGraphExecDestroy(gexec);
+        }
+        for (cudaEvent_t e : gev) {
+            cudaEventDestroy(e);
+        }
+        for (void* p : allocs) {
+            cudaFree(p);
+        }
+        if (stream) {
+            cudaStreamDestroy(stream);
+        }
+    }
+};
+
+namespace {
+
+void check_kernel_error(v2m_session* s) {
+    Global g;
+    ck(cudaMemcpyAsync(&g, s->d.G, sizeof(Global), cudaMemcpyDeviceToHost, s->stream), "read error flag");
+    ck(cudaStreamSynchronize(s->stream), "synchronize");
+    if (g.err) {
+        throw KernelError("kernel error " + std::to_string(g.err) + " at index " + std::to_string(g.err_info));
+    }
+}
+
+void validate(const v2m_grid_view* g, const v2m_relax_params* p, const v2m_nodes_view* nd) {
+    if (!g || !p || !nd) {
+        throw ArgError("null argument");
+    }
+    if (g->nx < 1 || g->ny < 1 || g->nz < 1) {
+        throw ArgError("grid dimensions must be positive");
+    }
+    if (g->nbx != (g->nx + 7) / 8 || g->nby != (g->ny + 7) / 8 || g->nbz != (g->nz + 7) / 8) {
+        throw ArgError("brick counts must be ceil(n / 8) per axis");
+    }
+    if (!(g->vs[0] > 0.0f && g->vs[1] > 0.0f && g->vs[2] > 0.0f)) {
+        throw ArgError("voxel sizes must be positive");
+    }
+    if (!g->L || !g->bl_cnt || !g->bl_lab || !g->bl_slot || !g->h || (g->nslots > 0 && !g->phi)) {
+        throw ArgError("grid array missing");
+    }
+    if (g->gm < 0) {
+        throw ArgError("analytic shape fields (gm < 0) are not supported by the CUDA relaxation");
+    }
+    if (g->gm > 0 && (!g->gI || !g->gTW)) {
+        throw ArgError("gray-scale fields need gI and gTW");
+    }
+    if (!(g->hmin > 0.0f) || !(g->hmax >= g->hmin)) {
+        throw ArgError("need 0 < hmin <= hmax");
+    }
+    if (nd->n < 0 || nd->n > (int64_t)0x7FFFFFFF / 2) {
+        throw ArgError("node count out of range");
+    }
+    if (nd->n > 0 && (!nd->P || !nd->lab || !nd->typ || !nd->part)) {
+        throw ArgError("node array missing");
+    }
+    if (p->max_iters < 0) {
+        throw ArgError("max_iters must be >= 0");
+    }
+    // brick tables: every slot a lookup can reach must exist
+    const int64_t nb = (int64_t)g->nbx * g->nby * g->nbz;
+    for (int64_t b = 0; b < nb; ++b) {
+        const int c = g->bl_cnt[b];
+        if (c < 0 || c > V2M_BL + 1) {
+            throw ArgError("brick label count out of range");
+        }
+        const int s = g->bl_slot[b];
+        if (s >= 0 && (int64_t)s + std::min(c, V2M_BL) > g->nslots) {
+            throw ArgError("brick slot beyond the phi array");
+        }
+    }
+    for (int64_t i = 0; i < nd->n; ++i) {
+        if (nd->typ[i] > V2M_CORNER) {
+            throw ArgError("node type out of range");
+        }
+        if (g->gm > 0 && nd->lab[i] > g->gm) {
+            throw ArgError("gray-scale node label above the threshold count");
+        }
+    }
+    if (!(p->t + p->skin > 0.0f)) {
+        throw ArgError("t + skin must be positive");
+    }
+}
+
+// Hash geometry of relax_cpu (src/v2m_particles.cpp:737-761), same float operations.
+DHash hash_geometry(const v2m_grid_view* g, const v2m_relax_params* p, int* nkeys) {
+    DHash H;
+    std::memset(&H, 0, sizeof(H));
+    H.b0 = (p->t + p->skin) * g->hmin;
+    H.ox = -0.5f * g->vs[0];
+    H.oy = -0.5f * g->vs[1];
+    H.oz = -0.5f * g->vs[2];
+    const float ext[3] = { g->nx * g->vs[0], g->ny * g->vs[1], g->nz * g->vs[2] };
+    H.nlev = 1;
+    while (H.nlev < V2M_MAXLEV && H.b0 * static_cast<float>(1 << (H.nlev - 1)) < (p->t + p->skin) * g->hmax) {
+        ++H.nlev;
+    }
+    int64_t nk = 0;
+    for (int L = 0; L < H.nlev; ++L) {
+        H.off[L] = (int)nk;
+        const float bL = H.b0 * static_cast<float>(1 << L);
+        for (int a = 0; a < 3; ++a) {
+            H.dim[L][a] = std::max(1, static_cast<int>(std::ceil(ext[a] / bL)));
+        }
+        nk += (int64_t)H.dim[L][0] * H.dim[L][1] * H.dim[L][2];
+    }
+    if (nk > 0x3FFFFFFF) {
+        throw ArgError("too many hash bins (hmin too small for the grid)");
+    }
+    *nkeys = (int)nk;
+    return H;
+}
+
+template <typename T>
+T* upload(v2m_session* s, const T* host, size_t count) {
+    T* d = s->alloc<T>(count);
+    if (count) {
+        ck(cudaMemcpyAsync(d, host, count * sizeof(T), cudaMemcpyHostToDevice, s->stream), "upload");
+    }
+    return d;
+}
+
+void init_ctl(v2m_session* s) {
+    std::vector<VolCtl> c(s->nvol);
+    for (int v = 0; v < s->nvol; ++v) {
+        std::memset(&c[v], 0, sizeof(VolCtl));
+        c[v].fdt = s->hvols[v].fire_dt0;
+        c[v].falpha = 0.1f;
+    }
+    ck(cudaMemcpyAsync(s->d.ctl, c.data(), sizeof(VolCtl) * s->nvol, cudaMemcpyHostToDevice, s->stream), "ctl");
+    ck(cudaStreamSynchronize(s->stream), "synchronize");
+}
+
+void do_reset(v2m_session* s) {
+    const Dev& d = s->d;
+    ck(cudaMemcpyAsync(d.Pq, s->Pq0, sizeof(float4) * d.N, cudaMemcpyDeviceToDevice, s->stream), "reset P");
+    ck(cudaMemcpyAsync(d.typ, s->typ0, d.N, cudaMemcpyDeviceToDevice, s->stream), "reset typ");
+    ck(cudaMemcpyAsync(d.part, s->part0, sizeof(uint32_t) * d.N, cudaMemcpyDeviceToDevice, s->stream), "reset part");
+    ck(cudaMemsetAsync(d.Vel, 0, sizeof(float4) * d.N, s->stream), "reset V");
+    ck(cudaMemsetAsync(d.F, 0, sizeof(float4) * d.N, s->stream), "reset F");
+    ck(cudaMemsetAsync(d.mv, 0, sizeof(float) * d.N, s->stream), "reset mv");
+    ck(cudaMemsetAsync(d.pw, 0, sizeof(float) * d.N, s->stream), "reset pw");
+    ck(cudaMemsetAsync(d.cnt, 0, sizeof(int) * d.KT, s->stream), "reset cnt");
+    ck(cudaMemsetAsync(d.G, 0, sizeof(Global), s->stream), "reset G");
+    init_ctl(s);
+    s->ms_hash = s->ms_loop = 0.0;
+}
+
+v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* pv, const v2m_nodes_view* nv, int device) {
+    if (nvol < 1 || nvol > kMaxVol) {
+        throw ArgError("volume count must be in [1, 1024]");
+    }
+    for (int v = 0; v < nvol; ++v) {
+        validate(gv + v, pv + v, nv + v);
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        cudaGetLastError();
+        throw CudaError("no CUDA device available");
+    }
+    const int dev = device < 0 ? 0 : device;
+    if (dev >= ndev) {
+        throw ArgError("device index out of range");
+    }
+    ck(cudaSetDevice(dev), "cudaSetDevice");
+    v2m_session* s = new v2m_session();
+    try {
+        s->device = dev;
+        s->nvol = nvol;
+        ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        s->serial_power = env_int("V2M_CUDA_SERIAL_POWER", 0);
+        s->force_threads = env_int("V2M_CUDA_FORCE_THREADS", 256);
+        if (s->force_threads != 64 && s->force_threads != 128 && s->force_threads != 256 && s->force_threads != 512) {
+            s->force_threads = 256;
+        }
+        s->graph_iters = std::max(1, env_int("V2M_CUDA_GRAPH_ITERS", 10));
+        s->time_force = env_int("V2M_CUDA_TIME_FORCE", 0);
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        s->refresh_blocks = sms * 4;
+        static const int env_div = std::getenv("V2M_REBUILD_DIV") ? std::atoi(std::getenv("V2M_REBUILD_DIV")) : 300;
+        // layout
+        int64_t N = 0, KT = 0;
+        s->hvols.resize(nvol);
+        s->info.resize(nvol);
+        s->prm.assign(pv, pv + nvol);
+        for (int v = 0; v < nvol; ++v) {
+            DVol& V = s->hvols[v];
+            std::memset(&V, 0, sizeof(DVol));
+            VolInfo& I = s->info[v];
+            I.n = (int)nv[v].n;
+            V.H = hash_geometry(gv + v, pv + v, &I.nkeys);
+            I.nofs = N;
+            N += align_up(std::max<int64_t>(I.n, 1), kNodeAlign);
+            I.kofs = KT;
+            KT += align_up((int64_t)I.nkeys + 1, kScanTile);
+            I.max_iters = pv[v].max_iters;
+            I.hmode = pv[v].h_mode;
+            s->max_iters = std::max(s->max_iters, I.max_iters);
+        }
+        if (N > 0x7FFFFFFF) {
+            throw ArgError("too many nodes in the session");
+        }
+        Dev& d = s->d;
+        d.nvol = nvol;
+        d.N = N;
+        d.KT = KT;
+        d.ntile_key = (int)(KT / kScanTile);
+        d.vols = s->alloc<DVol>(nvol);
+        d.ctl = s->alloc<VolCtl>(nvol);
+        d.G = s->alloc<Global>(1);
+        d.nodevol = s->alloc<uint16_t>(N);
+        d.tilevol = s->alloc<int16_t>(d.ntile_key);
+        d.Pq = s->alloc<float4>(N);
+        d.F = s->alloc<float4>(N);
+        d.Vel = s->alloc<float4>(N);
+        d.P0 = s->alloc<float4>(N);
+        d.Ps = s->alloc<float4>(N);
+        d.typ = s->alloc<uint8_t>(N);
+        d.lab = s->alloc<uint16_t>(N);
+        d.part = s->alloc<uint32_t>(N);
+        d.mv = s->alloc<float>(N);
+        d.pw = s->alloc<float>(N);
+        d.key = s->alloc<int>(N);
+        d.sorted = s->alloc<int>(N);
+        d.nbr = s->alloc<int>((size_t)N * V2M_K);
+        d.nnb = s->alloc<uint8_t>(N);
+        d.rlist = s->alloc<int>(N);
+        d.cnt = s->alloc<int>(KT);
+        d.cstart = s->alloc<int>(KT);
+        d.cursor = s->alloc<int>(KT);
+        d.tilesum = s->alloc<int>(d.ntile_key);
+        d.tileofs = s->alloc<int>(d.ntile_key);
+        d.psum = s->alloc<double>(N / kMoveThreads + 1);
+        d.pser = s->alloc<double>(nvol);
+        s->Pq0 = s->alloc<float4>(N);
+        s->typ0 = s->alloc<uint8_t>(N);
+        s->part0 = s->alloc<uint32_t>(N);
+        ck(cudaMemsetAsync(d.nnb, 0, N, s->stream), "memset");
+        ck(cudaMemsetAsync(d.nbr, 0, sizeof(int) * (size_t)N * V2M_K, s->stream), "memset");
+        ck(cudaMemsetAsync(d.Pq, 0, sizeof(float4) * N, s->stream), "memset");
+        ck(cudaMemsetAsync(d.P0, 0, sizeof(float4) * N, s->stream), "memset");
+        ck(cudaMemsetAsync(d.Ps, 0, sizeof(float4) * N, s->stream), "memset");
+        ck(cudaMemsetAsync(d.typ, 0, N, s->stream), "memset");
+        ck(cudaMemsetAsync(d.lab, 0, 2 * N, s->stream), "memset");
+        ck(cudaMemsetAsync(d.part, 0xFF, 4 * N, s->stream), "memset");
+        ck(cudaMemsetAsync(d.key, 0, 4 * N, s->stream), "memset");
+        ck(cudaMemsetAsync(d.sorted, 0, 4 * N, s->stream), "memset");
+        ck(cudaMemsetAsync(d.cstart, 0, 4 * KT, s->stream), "memset");
+        std::vector<uint16_t> nodevol(N, 0xFFFF);
+        std::vector<int16_t> tilevol(d.ntile_key, -1);
+        for (int v = 0; v < nvol; ++v) {
+            const VolInfo& I = s->info[v];
+            const v2m_grid_view* g = gv + v;
+            const v2m_relax_params* p = pv + v;
+            DVol& V = s->hvols[v];
+            const size_t nvox = (size_t)g->nx * g->ny * g->nz;
+            const size_t nb = (size_t)g->nbx * g->nby * g->nbz;
+            V.g.nx = g->nx;
+            V.g.ny = g->ny;
+            V.g.nz = g->nz;
+            V.g.nbx = g->nbx;
+            V.g.nby = g->nby;
+            V.g.nbz = g->nbz;
+            V.g.vx = g->vs[0];
+            V.g.vy = g->vs[1];
+            V.g.vz = g->vs[2];
+            V.g.L = upload(s, g->L, nvox);
+            V.g.bl_cnt = upload(s, g->bl_cnt, nb);
+            V.g.bl_lab = upload(s, g->bl_lab, nb * V2M_BL);
+            V.g.bl_slot = upload(s, g->bl_slot, nb);
+            V.g.phi = upload(s, g->phi, (size_t)g->nslots * V2M_SLOT);
+            V.g.hvox = upload(s, g->h, nvox);
+            V.g.gm = g->gm;
+            if (g->gm > 0) {
+                V.g.gI = upload(s, g->gI, nvox);
+                V.g.gTW = upload(s, g->gTW, 2 * (size_t)g->gm);
+            } else {
+                V.g.gI = nullptr;
+                V.g.gTW = s->alloc<float>(4);
+            }
+            V.nofs = I.nofs;
+            V.n = I.n;
+            V.kofs = I.kofs;
+            V.nkeys = I.nkeys;
+            V.tofs_key = (int)(I.kofs / kScanTile);
+            V.ntile_key = (int)(align_up((int64_t)I.nkeys + 1, kScanTile) / kScanTile);
+            V.tofs_node = (int)(I.nofs / kMoveThreads);
+            V.ntile_node = (int)((I.n + kMoveThreads - 1) / kMoveThreads);
+            V.t = p->t;
+            V.skin = p->skin;
+            V.fscale = p->fscale;
+            V.fsurf = p->fsurf;
+            V.dt = p->dt;
+            V.maxstep = p->maxstep;
+            V.snap = p->snap;
+            V.dptol = p->dptol;
+            V.voxmode = p->voxel_trap ? 1 : 0;
+            V.fire = (p->fire && !p->voxel_trap) ? 1 : 0;
+            V.max_iters = p->max_iters;
+            V.rebuild_div = p->rebuild_div > 0 ? p->rebuild_div : (env_div > 0 ? env_div : 1);
+            V.hmode = p->h_mode;
+            V.policy = p->rebuild_policy;
+            V.fire_dt0 = std::sqrt(p->dt);
+            V.fire_dtmax = p->fire_dtmax * V.fire_dt0;
+            std::fill(nodevol.begin() + I.nofs, nodevol.begin() + I.nofs + I.n, (uint16_t)v);
+            for (int t = 0; t < V.ntile_key; ++t) {
+                tilevol[V.tofs_key + t] = (int16_t)v;
+            }
+            if (I.n > 0) {
+                ck(cudaMemcpyAsync(d.lab + I.nofs, nv[v].lab, 2 * (size_t)I.n, cudaMemcpyHostToDevice, s->stream), "lab");
+                ck(cudaMemcpyAsync(d.typ + I.nofs, nv[v].typ, (size_t)I.n, cudaMemcpyHostToDevice, s->stream), "typ");
+                ck(cudaMemcpyAsync(d.part + I.nofs, nv[v].part, 4 * (size_t)I.n, cudaMemcpyHostToDevice, s->stream), "part");
+            }
+        }
+        ck(cudaMemcpyAsync(d.vols, s->hvols.data(), sizeof(DVol) * nvol, cudaMemcpyHostToDevice, s->stream), "vols");
+        ck(cudaMemcpyAsync(d.nodevol, nodevol.data(), 2 * N, cudaMemcpyHostToDevice, s->stream), "nodevol");
+        ck(cudaMemcpyAsync(d.tilevol, tilevol.data(), 2 * (size_t)d.ntile_key, cudaMemcpyHostToDevice, s->stream), "tilevol");
+        // positions: staged as float[3n] then packed with the size and type sign
+        for (int v = 0; v < nvol; ++v) {
+            const VolInfo& I = s->info[v];
+            if (I.n == 0) {
+                continue;
+            }
+            float* tmp = nullptr;
+            ck(cudaMallocAsync((void**)&tmp, 12 * (size_t)I.n, s->stream), "cudaMallocAsync");
+            ck(cudaMemcpyAsync(tmp, nv[v].P, 12 * (size_t)I.n, cudaMemcpyHostToDevice, s->stream), "P");
+            launch_pack_nodes(s->stream, d, v, I.n, tmp, d.typ);
+            ck(cudaFreeAsync(tmp, s->stream), "cudaFreeAsync");
+        }
+        ck(cudaGetLastError(), "pack");
+        ck(cudaMemcpyAsync(s->Pq0, d.Pq, sizeof(float4) * N, cudaMemcpyDeviceToDevice, s->stream), "seed P");
+        ck(cudaMemcpyAsync(s->typ0, d.typ, N, cudaMemcpyDeviceToDevice, s->stream), "seed typ");
+        ck(cudaMemcpyAsync(s->part0, d.part, 4 * N, cudaMemcpyDeviceToDevice, s->stream), "seed part");
+        do_reset(s);
+        return s;
+    } catch (...) {
+        delete s;
+        throw;
+    }
+}
+
+// relax_cl's rebuild (src/v2m_gpu.cpp:259-277) for the volumes whose rebuild flag is set.
+void enqueue_rebuild(v2m_session* s) {
+    const Dev& d = s->d;
+    launch_keys(s->stream, d);
+    launch_scan(s->stream, d);
+    launch_scatter(s->stream, d);
+    launch_neighbors(s->stream, d);
+    s->launches += 8;
+}
+
+void enqueue_force(v2m_session* s, cudaEvent_t e0, cudaEvent_t e1) {
+    if (e0) {
+        ck(cudaEventRecord(e0, s->stream), "event");
+    }
+    launch_force(s->stream, s->d, s->force_threads);
+    if (e1) {
+        ck(cudaEventRecord(e1, s->stream), "event");
+    }
+    s->launches += 1;
+    s->force_launches += 1;
+}
+
+// The rest of an iteration: move + reductions, control, self-refresh, rebuild.
+void enqueue_tail(v2m_session* s) {
+    const Dev& d = s->d;
+    launch_move(s->stream, d);
+    launch_control(s->stream, d, s->serial_power);
+    launch_refresh(s->stream, d, s->refresh_blocks);
+    s->launches += 3 + (s->serial_power ? 1 : 0);
+    enqueue_rebuild(s);
+}
+
+void read_ctl(v2m_session* s, std::vector<VolCtl>& c) {
+    c.resize(s->nvol);
+    ck(cudaMemcpyAsync(c.data(), s->d.ctl, sizeof(VolCtl) * s->nvol, cudaMemcpyDeviceToHost, s->stream), "read ctl");
+    ck(cudaStreamSynchronize(s->stream), "synchronize");
+}
+
+bool all_done(v2m_session* s, const std::vector<VolCtl>& c) {
+    for (int v = 0; v < s->nvol; ++v) {
+        if (!c[v].done && c[v].it < s->info[v].max_iters) {
+            return false;
+        }
+    }
+    return true;
+}
+
+void build_graph(v2m_session* s) {
+    if (s->gexec) {
+        return;
+    }
+    const int G = s->graph_iters;
+    s->gev.assign(2 * G, nullptr);
+    for (auto& e : s->gev) {
+        ck(cudaEventCreate(&e), "cudaEventCreate");
+    }
+    cudaGraph_t graph = nullptr;
+    const int64_t l0 = s->launches, f0 = s->force_launches;
+    ck(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+        for (int k = 0; k < G; ++k) {
+            enqueue_force(s, s->gev[2 * k], s->gev[2 * k + 1]);
+            enqueue_tail(s);
+        }
+    } catch (...) {
+        cudaStreamEndCapture(s->stream, &graph);
+        if (graph) {
+            cudaGraphDestroy(graph);
+        }
+        throw;
+    }
+    ck(cudaStreamEndCapture(s->stream, &graph), "end capture");
+    s->launches = l0;
+    s->force_launches = f0;
+    cudaError_t e = cudaGraphInstantiate(&s->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    ck(e, "cudaGraphInstantiate");
+}
+
+// Up to `iters` iterations of every volume still running.
+void do_iterate(v2m_session* s, int iters, int graph) {
+    std::vector<VolCtl> c;
+    read_ctl(s, c);
+    if (all_done(s, c)) {
+        return;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    if (graph) {
+        build_graph(s);
+        const int G = s->graph_iters;
+        int done_it = 0;
+        // per-iteration launches inside the graph: force + tail
+        const int per_it = 1 + 3 + (s->serial_power ? 1 : 0) + 8;
+        while (done_it < iters) {
+            ck(cudaGraphLaunch(s->gexec, s->stream), "cudaGraphLaunch");
+            s->launches += (int64_t)G * per_it;
+            s->force_launches += G;
+            done_it += G;
+            read_ctl(s, c);
+            if (s->time_force) {
+                for (int k = 0; k < G; ++k) {
+                    float ms = 0.0f;
+                    if (cudaEventElapsedTime(&ms, s->gev[2 * k], s->gev[2 * k + 1]) == cudaSuccess) {
+                        s->force_ms += ms;
+                    }
+                }
+            }
+            if (all_done(s, c)) {
+                break;
+            }
+        }
+    } else {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (s->time_force) {
+            ck(cudaEventCreate(&e0), "event");
+            ck(cudaEventCreate(&e1), "event");
+        }
+        for (int k = 0; k < iters; ++k) {
+            enqueue_force(s, e0, e1);
+            enqueue_tail(s);
+            ck(cudaGetLastError(), "launch");
+            if (s->time_force) {
+                ck(cudaEventSynchronize(e1), "event sync");
+                float ms = 0.0f;
+                ck(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+                s->force_ms += ms;
+            }
+            if ((k + 1) % 25 == 0 || k + 1 == iters) {
+                read_ctl(s, c);
+                if (all_done(s, c)) {
+                    break;
+                }
+            }
+        }
+        if (e0) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+        }
+    }
+    ck(cudaGetLastError(), "launch");
+    check_kernel_error(s);
+    s->ms_loop += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void do_rebuild(v2m_session* s) {
+    const auto t0 = std::chrono::steady_clock::now();
+    launch_set_rebuild(s->stream, s->d, 1);
+    s->launches += 1;
+    enqueue_rebuild(s);
+    launch_set_rebuild(s->stream, s->d, 0);
+    s->launches += 1;
+    ck(cudaGetLastError(), "launch");
+    check_kernel_error(s);
+    s->ms_hash += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void fill_stats(v2m_session* s, int v, v2m_relax_stats* st) {
+    std::vector<VolCtl> c;
+    read_ctl(s, c);
+    const VolInfo& I = s->info[v];
+    std::memset(st, 0, sizeof(*st));
+    st->iters = c[v].iters;
+    st->rebuilds = c[v].rebuilds;
+    st->last_move = c[v].last_move;
+    st->last_p99 = c[v].last_p99;
+    st->fire_resets = c[v].resets;
+    st->fire_dt = s->hvols[v].fire ? c[v].fdt : 0.0f;
+    if (I.n > 0) {
+        std::vector<uint8_t> t(I.n);
+        ck(cudaMemcpyAsync(t.data(), s->d.typ + I.nofs, I.n, cudaMemcpyDeviceToHost, s->stream), "typ");
+        ck(cudaStreamSynchronize(s->stream), "synchronize");
+        for (uint8_t x : t) {
+            st->n_interior += x == V2M_INTERIOR;
+            st->n_interface += x == V2M_INTERFACE;
+            st->n_junction += x == V2M_JUNCTION;
+            st->n_corner += x == V2M_CORNER;
+        }
+    }
+    st->ms_hash = s->ms_hash;
+    st->ms_move = s->ms_loop;
+    st->ms_force = s->force_ms;
+}
+
+void read_nodes(v2m_session* s, int v, v2m_nodes_view* nd) {
+    const VolInfo& I = s->info[v];
+    if (!nd || nd->n != I.n) {
+        throw ArgError("node view does not match the volume");
+    }
+    if (I.n == 0) {
+        return;
+    }
+    float* tmp = nullptr;
+    ck(cudaMallocAsync((void**)&tmp, 12 * (size_t)I.n, s->stream), "cudaMallocAsync");
+    launch_unpack_P(s->stream, s->d, I.nofs, I.n, tmp);
+    ck(cudaMemcpyAsync(nd->P, tmp, 12 * (size_t)I.n, cudaMemcpyDeviceToHost, s->stream), "P");
+    ck(cudaMemcpyAsync(nd->typ, s->d.typ + I.nofs, I.n, cudaMemcpyDeviceToHost, s->stream), "typ");
+    ck(cudaMemcpyAsync(nd->part, s->d.part + I.nofs, 4 * (size_t)I.n, cudaMemcpyDeviceToHost, s->stream), "part");
+    ck(cudaFreeAsync(tmp, s->stream), "cudaFreeAsync");
+    ck(cudaStreamSynchronize(s->stream), "synchronize");
+}
+
+template <typename F>
+int guard(F&& f) {
+    try {
+        f();
+        g_err.clear();
+        return V2M_OK;
+    } catch (const ArgError& e) {
+        g_err = e.what();
+        return V2M_ERR_ARG;
+    } catch (const KernelError& e) {
+        g_err = e.what();
+        return V2M_ERR_KERNEL;
+    } catch (const CudaError& e) {
+        g_err = e.what();
+        return V2M_ERR_CUDA;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return V2M_ERR_CUDA;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void v2m_relax_params_default(v2m_relax_params* p) {
+    std::memset(p, 0, sizeof(*p));
+    p->nseed = 8;
+    p->t = 1.3f;
+    p->skin = 0.3f;
+    p->fscale = 1.2f;
+    p->fsurf = 1.0f;
+    p->dt = 0.5f;
+    p->maxstep = 0.2f;
+    p->snap = 0.5f;
+    p->max_iters = 500;
+    p->dptol = 2e-3f;
+    p->jseed = 0.8f;
+    p->corners = 1;
+    p->voxel_trap = 0;
+    p->thin = 0.0f;
+    p->fire = 1;
+    p->fire_dtmax = 2.0f;
+    p->verbose = 0;
+}
+
+const char* v2m_cuda_last_error(void) {
+    return g_err.c_str();
+}
+
+int v2m_cuda_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+int v2m_session_create(int nvol, const v2m_grid_view* g, const v2m_relax_params* prm, const v2m_nodes_view* nd,
+                       int device, v2m_session** out) {
+    return guard([&] {
+        if (!out) {
+            throw ArgError("null output");
+        }
+        *out = create(nvol, g, prm, nd, device);
+    });
+}
+
+int v2m_session_destroy(v2m_session* s) {
+    return guard([&] {
+        if (s) {
+            cudaSetDevice(s->device);
+            cudaStreamSynchronize(s->stream);
+            delete s;
+        }
+    });
+}
+
+int v2m_session_reset(v2m_session* s) {
+    return guard([&] {
+        ck(cudaSetDevice(s->device), "cudaSetDevice");
+        do_reset(s);
+    });
+}
+
+int v2m_session_rebuild(v2m_session* s) {
+    return guard([&] {
+        ck(cudaSetDevice(s->device), "cudaSetDevice");
+        do_rebuild(s);
+    });
+}
+
+int v2m_session_force(v2m_session* s) {
+    return guard([&] {
+        ck(cudaSetDevice(s->device), "cudaSetDevice");
+        enqueue_force(s, nullptr, nullptr);
+        ck(cudaGetLastError(), "launch");
+        check_kernel_error(s);
+    });
+}
+
+int v2m_session_step_tail(v2m_session* s) {
+    return guard([&] {
+        ck(cudaSetDevice(s->device), "cudaSetDevice");
+        enqueue_tail(s);
+        ck(cudaGetLastError(), "launch");
+        check_kernel_error(s);
+    });
+}
+
+int v2m_session_iterate(v2m_session* s, int iters, int graph) {
+    return guard([&] {
+        ck(cudaSetDevice(s->device), "cudaSetDevice");
+        do_iterate(s, iters, graph);
+    });
+}
+
+int v2m_session_run(v2m_session* s, int graph) {
+    return guard([&] {
+        ck(cudaSetDevice(s->device), "cudaSetDevice");
+        do_rebuild(s);
+        do_iterate(s, s->max_iters, graph);
+    });
+}
+
+int v2m_session_synchronize(v2m_session* s) {
+    return guard([&] {
+        ck(cudaStreamSynchronize(s->stream), "synchronize");
+        check_kernel_error(s);
+    });
+}
+
+int v2m_session_read_nodes(v2m_session* s, int vol, v2m_nodes_view* nd) {
+    return guard([&] {
+        if (vol < 0 || vol >= s->nvol) {
+            throw ArgError("volume index out of range");
+        }
+        ck(cudaSetDevice(s->device), "cudaSetDevice");
+        read_nodes(s, vol, nd);
+    });
+}
+
+int v2m_session_stats(v2m_session* s, int vol, v2m_relax_stats* st) {
+    return guard([&] {
+        if (vol < 0 || vol >= s->nvol || !st) {
+            throw ArgError("bad argument");
+        }
+        ck(cudaSetDevice(s->device), "cudaSetDevice");
+        fill_stats(s, vol, st);
+    });
+}
+
+int v2m_session_info(v2m_session* s, int vol, int64_t* n, int64_t* nkeys, int32_t* nlev) {
+    return guard([&] {
+        if (vol < 0 || vol >= s->nvol) {
+            throw ArgError("volume index out of range");
+        }
+        if (n) {
+            *n = s->info[vol].n;
+        }
+        if (nkeys) {
+            *nkeys = s->info[vol].nkeys;
+        }
+        if (nlev) {
+            *nlev = s->hvols[vol].H.nlev;
+        }
+    });
+}
+
+int v2m_session_counters(v2m_session* s, int64_t* launches, int64_t* force_launches, double* force_ms) {
+    return guard([&] {
+        if (launches) {
+            *launches = s->launches;
+        }
+        if (force_launches) {
+            *force_launches = s->force_launches;
+        }
+        if (force_ms) {
+            *force_ms = s->force_ms;
+        }
+    });
+}
+
+int v2m_session_read_array(v2m_session* s, int vol, int what, void* host, int64_t bytes) {
+    return guard([&] {
+        if (vol < 0 || vol >= s->nvol || !host) {
+            throw ArgError("bad argument");
+        }
+        ck(cudaSetDevice(s->device), "cudaSetDevice");
+        const VolInfo& I = s->info[vol];
+        const Dev& d = s->d;
+        const int n = I.n;
+        auto need = [&](int64_t b) {
+            if (bytes < b) {
+                throw ArgError("host buffer too small");
+            }
+        };
+        auto d2h = [&](const void* src, int64_t b) {
+            need(b);
+            if (b) {
+                ck(cudaMemcpyAsync(host, src, (size_t)b, cudaMemcpyDeviceToHost, s->stream), "read");
+            }
+        };
+        void* tmp = nullptr;
+        auto scratch = [&](size_t b) {
+            ck(cudaMallocAsync(&tmp, std::max<size_t>(b, 16), s->stream), "cudaMallocAsync");
+            return tmp;
+        };
+        switch (what) {
+        case V2M_ARR_KEY: d2h(d.key + I.nofs, 4LL * n); break;
+        case V2M_ARR_SORTED: {
+            need(4LL * n);
+            int* t = (int*)scratch(4 * (size_t)n);
+            launch_local_ids(s->stream, d.sorted, I.nofs, n, t);
+            d2h(t, 4LL * n);
+            break;
+        }
+        case V2M_ARR_CSTART: {
+            need(4LL * (I.nkeys + 1));
+            int* t = (int*)scratch(4 * (size_t)(I.nkeys + 1));
+            launch_local_cstart(s->stream, d.cstart, I.kofs, I.nkeys + 1, I.nofs, t);
+            d2h(t, 4LL * (I.nkeys + 1));
+            break;
+        }
+        case V2M_ARR_PS: d2h(d.Ps + I.nofs, 16LL * n); break;
+        case V2M_ARR_NBR:
+        case V2M_ARR_NNB: {
+            int* t = (int*)scratch(4 * ((size_t)n * V2M_K + n));
+            launch_lists_rowmajor(s->stream, d, I.nofs, n, t, t + (size_t)n * V2M_K);
+            if (what == V2M_ARR_NBR) {
+                d2h(t, 4LL * n * V2M_K);
+            } else {
+                d2h(t + (size_t)n * V2M_K, 4LL * n);
+            }
+            break;
+        }
+        case V2M_ARR_F: d2h(d.F + I.nofs, 16LL * n); break;
+        case V2M_ARR_HN: {
+            need(4LL * n);
+            float* t = (float*)scratch(4 * (size_t)n);
+            launch_hn(s->stream, d, I.nofs, n, t);
+            d2h(t, 4LL * n);
+            break;
+        }
+        case V2M_ARR_MV: d2h(d.mv + I.nofs, 4LL * n); break;
+        case V2M_ARR_PW: d2h(d.pw + I.nofs, 4LL * n); break;
+        case V2M_ARR_V:
+        case V2M_ARR_P0: {
+            need(12LL * n);
+            std::vector<VolCtl> c;
+            read_ctl(s, c);
+            if (what == V2M_ARR_V && c[vol].vzero) {   // a FIRE reset zeroed every velocity
+                std::memset(host, 0, 12 * (size_t)n);
+                break;
+            }
+            float* t = (float*)scratch(12 * (size_t)n);
+            launch_float4_to3(s->stream, what == V2M_ARR_V ? d.Vel : d.P0, I.nofs, n, t);
+            d2h(t, 12LL * n);
+            break;
+        }
+        case V2M_ARR_P: {
+            need(12LL * n);
+            float* t = (float*)scratch(12 * (size_t)n);
+            launch_unpack_P(s->stream, d, I.nofs, n, t);
+            d2h(t, 12LL * n);
+            break;
+        }
+        case V2M_ARR_TYP: d2h(d.typ + I.nofs, n); break;
+        case V2M_ARR_PART: d2h(d.part + I.nofs, 4LL * n); break;
+        case V2M_ARR_HIST: {
+            need(4LL * 34);
+            std::vector<VolCtl> c;
+            read_ctl(s, c);
+            int* h = (int*)host;
+            std::memcpy(h, c[vol].hist, 32 * 4);
+            std::memcpy(h + 32, &c[vol].maxbits, 4);
+            h[33] = c[vol].nhalf;
+            break;
+        }
+        default: throw ArgError("unknown array");
+        }
+        if (tmp) {
+            ck(cudaFreeAsync(tmp, s->stream), "cudaFreeAsync");
+        }
+        ck(cudaStreamSynchronize(s->stream), "synchronize");
+    });
+}
+
+int v2m_session_write_array(v2m_session* s, int vol, int what, const void* host, int64_t bytes) {
+    return guard([&] {
+        if (vol < 0 || vol >= s->nvol || !host) {
+            throw ArgError("bad argument");
+        }
+        ck(cudaSetDevice(s->device), "cudaSetDevice");
+        const VolInfo& I = s->info[vol];
+        const Dev& d = s->d;
+        const int n = I.n;
+        auto exact = [&](int64_t b) {
+            if (bytes != b) {
+                throw ArgError("size mismatch");
+            }
+        };
+        void* tmp = nullptr;
+        auto staged = [&](int64_t b) {
+            ck(cudaMallocAsync(&tmp, std::max<size_t>((size_t)b, 16), s->stream), "cudaMallocAsync");
+            ck(cudaMemcpyAsync(tmp, host, (size_t)b, cudaMemcpyHostToDevice, s->stream), "write");
+            return tmp;
+        };
+        switch (what) {
+        case V2M_ARR_P: {
+            exact(12LL * n);
+            // keep the stored size: positions only
+            float* t = (float*)staged(12LL * n);
+            std::vector<float> hn(n);
+            float* hd = nullptr;
+            ck(cudaMallocAsync((void**)&hd, 4 * (size_t)n + 16, s->stream), "cudaMallocAsync");
+            launch_hn(s->stream, d, I.nofs, n, hd);
+            launch_float3_to4(s->stream, t, I.nofs, n, d.Pq);
+            launch_set_hn(s->stream, d, I.nofs, n, hd);
+            ck(cudaFreeAsync(hd, s->stream), "cudaFreeAsync");
+            break;
+        }
+        case V2M_ARR_TYP:
+            exact(n);
+            ck(cudaMemcpyAsync(d.typ + I.nofs, host, n, cudaMemcpyHostToDevice, s->stream), "write");
+            launch_resign(s->stream, d, I.nofs, n);
+            break;
+        case V2M_ARR_PART:
+            exact(4LL * n);
+            ck(cudaMemcpyAsync(d.part + I.nofs, host, 4 * (size_t)n, cudaMemcpyHostToDevice, s->stream), "write");
+            break;
+        case V2M_ARR_HN: {
+            exact(4LL * n);
+            float* t = (float*)staged(4LL * n);
+            launch_set_hn(s->stream, d, I.nofs, n, t);
+            break;
+        }
+        case V2M_ARR_V: {
+            exact(12LL * n);
+            float* t = (float*)staged(12LL * n);
+            launch_float3_to4(s->stream, t, I.nofs, n, d.Vel);
+            break;
+        }
+        default: throw ArgError("array not writable");
+        }
+        if (tmp) {
+            ck(cudaFreeAsync(tmp, s->stream), "cudaFreeAsync");
+        }
+        ck(cudaGetLastError(), "launch");
+        ck(cudaStreamSynchronize(s->stream), "synchronize");
+    });
+}
+
+int v2m_session_write_lists(v2m_session* s, int vol, const int32_t* nbr, const int32_t* nnb) {
+    return guard([&] {
+        if (vol < 0 || vol >= s->nvol || !nbr || !nnb) {
+            throw ArgError("bad argument");
+        }
+        ck(cudaSetDevice(s->device), "cudaSetDevice");
+        const VolInfo& I = s->info[vol];
+        const int n = I.n;
+        for (int i = 0; i < n; ++i) {
+            if (nnb[i] < 0 || nnb[i] > V2M_K) {
+                throw ArgError("list length out of range");
+            }
+            for (int k = 0; k < nnb[i]; ++k) {
+                const int j = nbr[(size_t)i * V2M_K + k];
+                if (j < 0 || j >= n) {
+                    throw ArgError("neighbour id out of range");
+                }
+            }
+        }
+        int* t = nullptr;
+        ck(cudaMallocAsync((void**)&t, 4 * ((size_t)n * V2M_K + n) + 16, s->stream), "cudaMallocAsync");
+        ck(cudaMemcpyAsync(t, nbr, 4 * (size_t)n * V2M_K, cudaMemcpyHostToDevice, s->stream), "write");
+        ck(cudaMemcpyAsync(t + (size_t)n * V2M_K, nnb, 4 * (size_t)n, cudaMemcpyHostToDevice, s->stream), "write");
+        launch_lists_from_rowmajor(s->stream, s->d, I.nofs, n, t, t + (size_t)n * V2M_K);
+        ck(cudaFreeAsync(t, s->stream), "cudaFreeAsync");
+        ck(cudaGetLastError(), "launch");
+        ck(cudaStreamSynchronize(s->stream), "synchronize");
+    });
+}
+
+int v2m_session_timed_runs(v2m_session* s, int runs, int graph, int time_force, float* ms) {
+    return guard([&] {
+        if (runs < 1 || !ms) {
+            throw ArgError("bad argument");
+        }
+        ck(cudaSetDevice(s->device), "cudaSetDevice");
+        s->time_force = time_force;
+        cudaEvent_t e0, e1;
+        ck(cudaEventCreate(&e0), "event");
+        ck(cudaEventCreate(&e1), "event");
+        ck(cudaStreamSynchronize(s->stream), "synchronize");
+        ck(cudaEventRecord(e0, s->stream), "event");
+        for (int r = 0; r < runs; ++r) {
+            do_reset(s);
+            do_rebuild(s);
+            do_iterate(s, s->max_iters, graph);
+        }
+        ck(cudaEventRecord(e1, s->stream), "event");
+        ck(cudaEventSynchronize(e1), "event sync");
+        ck(cudaEventElapsedTime(ms, e0, e1), "elapsed");
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    });
+}
+
+int v2m_session_clear_counters(v2m_session* s) {
+    return guard([&] {
+        s->launches = 0;
+        s->force_launches = 0;
+        s->force_ms = 0.0;
+    });
+}
+
+int v2m_relax_cuda(const v2m_grid_view* g, const v2m_relax_params* prm, v2m_nodes_view* nd, v2m_relax_stats* st,
+                   int device) {
+    return v2m_relax_cuda_batch(1, g, prm, nd, st, device);
+}
+
+int v2m_relax_cuda_batch(int nvol, const v2m_grid_view* g, const v2m_relax_params* prm, v2m_nodes_view* nd,
+                         v2m_relax_stats* st, int device) {
+    v2m_session* s = nullptr;
+    const int rc = guard([&] {
+        s = create(nvol, g, prm, nd, device);
+        do_rebuild(s);
+        do_iterate(s, s->max_iters, env_int("V2M_CUDA_GRAPH", 1));
+        for (int v = 0; v < nvol; ++v) {
+            read_nodes(s, v, nd + v);
+            if (st) {
+                fill_stats(s, v, st + v);
+            }
+        }
+    });
+    if (s) {
+        const std::string keep = g_err;
+        cudaStreamSynchronize(s->stream);
+        delete s;
+        g_err = keep;
+    }
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,1069 @@
+// v2m_kernels.cu -- the relaxation's kernels for sm_100a (B200).
+//
+// One launch per stage covers every volume of a session; a thread (or warp)
+// finds its volume through nodevol[] (node stages) or the 1024-aligned bin
+// ranges (scan stages), and a volume whose loop has finished, or that does not
+// rebuild this iteration, makes its threads return at once. Nothing waits on
+// another block: no spin loops, no grid-wide barriers, so every launch ends.
+//
+// Stage map (fangq/trussnet reference in brackets):
+//   k_keys        bin key of each node + bin counts          [k_keys, src/opencl/v2m_kernels.cl:106-120]
+//   k_scan_*      exclusive scan of the bin counts            [k_scan_block / k_scan_add :46-103]
+//   k_scatter     node ids into their bins                    [k_scatter :122-128]
+//   k_binsort     ascending ids within each bin + bin-order   [src/v2m_particles.cpp:791-806; k_gather :131-142]
+//                 positions/sizes (the CPU's stable order)
+//   k_neighbors   K-nearest truss of each node, one warp each [v2m_neighbors, src/opencl/v2m_particle_body.cl:73-151]
+//   k_force       bar forces, each node's bars summed in list [v2m_force :161-184]
+//                 order (an ordered fold: no float atomics)
+//   k_move        FIRE/Jacobi step + trapped move + the        [v2m_move :844-935; k_stats :196-267]
+//                 iteration's reductions (log2 histogram, max,
+//                 half-skin count, FIRE power per block)
+//   k_control     FIRE update, p99, stop test, rebuild trigger [src/v2m_particles.cpp:849-946; FireCtl src/v2m_particles.h:47-76]
+//   k_refresh     lists of nodes past a full skin rebuilt     [src/v2m_particles.cpp:917-937]
+#include <cstdint>
+#include <cstdio>
+
+#include "v2m_field.cuh"
+#include "v2m_kernels.h"
+
+namespace v2m {
+
+__device__ __forceinline__ void raise_error(Global* G, int code, int info) {
+    if (atomicCAS(&G->err, 0, code) == 0) {
+        G->err_info = info;
+    }
+}
+
+// ---- hash geometry (src/opencl/v2m_particle_body.cl:38-58) -----------------------
+__device__ __forceinline__ int level_of(const DHash& H, float R) {
+    int L = 0;
+    while (L + 1 < H.nlev && H.b0 * (float)(1 << L) < R) {
+        ++L;
+    }
+    return L;
+}
+
+__device__ __forceinline__ int bin_coord(const DHash& H, int L, float x, float o, int ax) {
+    const int c = (int)floorf((x - o) / (H.b0 * (float)(1 << L)));
+    const int n = H.dim[L][ax];
+    return c < 0 ? 0 : (c >= n ? n - 1 : c);
+}
+
+__device__ __forceinline__ int bin_key(const DHash& H, int L, float px, float py, float pz) {
+    const int cx = bin_coord(H, L, px, H.ox, 0), cy = bin_coord(H, L, py, H.oy, 1), cz = bin_coord(H, L, pz, H.oz, 2);
+    return H.off[L] + cx + H.dim[L][0] * (cy + H.dim[L][1] * cz);
+}
+
+// Position + signed size: the sign bit of w marks a non-INTERIOR node.
+__device__ __forceinline__ float pack_h(float h, int ty) {
+    return ty != V2M_INTERIOR ? -h : h;
+}
+
+// ---- keys + counts ---------------------------------------------------------------
+__global__ void k_keys(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl, const uint16_t* __restrict__ nodevol,
+                       const float4* __restrict__ Pq, int* __restrict__ key, int* __restrict__ cnt,
+                       float4* __restrict__ P0, int64_t N, Global* G) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) {
+        return;
+    }
+    const int v = nodevol[i];
+    if (v == 0xFFFF || !ctl[v].rebuild) {
+        return;
+    }
+    const DVol& V = vols[v];
+    const float4 p = Pq[i];
+    const float hh = size_at(V.g, V.hmode, p.x, p.y, p.z);
+    const int k = bin_key(V.H, level_of(V.H, (V.t + V.skin) * hh), p.x, p.y, p.z);
+    if (k < 0 || k >= V.nkeys) {
+        raise_error(G, 1, (int)i);
+        return;
+    }
+    key[i] = k;
+    atomicAdd(cnt + V.kofs + k, 1);
+    P0[i] = make_float4(p.x, p.y, p.z, 0.0f);
+}
+
+// ---- exclusive scan of the bin counts, per volume, based at the volume's first node --
+// Bin entries are tiled by kScanTile; every tile lies in one volume (1024-aligned).
+__global__ void k_scan_tiles(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
+                             const int16_t* __restrict__ tilevol, const int* __restrict__ cnt, int* __restrict__ tilesum,
+                             int64_t KT) {
+    const int t = blockIdx.x;
+    const int v = tilevol[t];
+    if (v < 0 || !ctl[v].rebuild) {
+        return;
+    }
+    const DVol& V = vols[v];
+    const int64_t base = (int64_t)t * kScanTile;
+    const int64_t end = V.kofs + V.nkeys + 1;
+    int s = 0;
+    for (int q = threadIdx.x; q < kScanTile; q += blockDim.x) {
+        const int64_t e = base + q;
+        if (e < end && e >= V.kofs) {
+            s += cnt[e];
+        }
+    }
+    __shared__ int red[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[threadIdx.x >> 5] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0;
+        for (int o = 16; o > 0; o >>= 1) {
+            s += __shfl_down_sync(0xffffffffu, s, o);
+        }
+        if (threadIdx.x == 0) {
+            tilesum[t] = s;
+        }
+    }
+}
+
+// One block per volume: exclusive scan over its tiles' sums, starting at nofs.
+__global__ void k_scan_vol(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl, const int* __restrict__ tilesum,
+                           int* __restrict__ tileofs) {
+    const int v = blockIdx.x;
+    if (!ctl[v].rebuild) {
+        return;
+    }
+    const DVol& V = vols[v];
+    const int t0 = V.tofs_key, nt = V.ntile_key;
+    __shared__ int carry;
+    if (threadIdx.x == 0) {
+        carry = (int)V.nofs;
+    }
+    __syncthreads();
+    for (int b = 0; b < nt; b += blockDim.x) {
+        const int t = b + threadIdx.x;
+        int x = t < nt ? tilesum[t0 + t] : 0;
+        // block inclusive scan
+        int incl = x;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if ((threadIdx.x & 31) >= o) {
+                incl += y;
+            }
+        }
+        __shared__ int wsum[32];
+        if ((threadIdx.x & 31) == 31) {
+            wsum[threadIdx.x >> 5] = incl;
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            int w = threadIdx.x < (blockDim.x >> 5) ? wsum[threadIdx.x] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, w, o);
+                if (threadIdx.x >= o) {
+                    w += y;
+                }
+            }
+            wsum[threadIdx.x] = w;
+        }
+        __syncthreads();
+        const int wp = (threadIdx.x >> 5) ? wsum[(threadIdx.x >> 5) - 1] : 0;
+        if (t < nt) {
+            tileofs[t0 + t] = carry + wp + incl - x;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            carry += wsum[(blockDim.x >> 5) - 1];
+        }
+        __syncthreads();
+    }
+}
+
+// Per tile: cstart = tile offset + exclusive scan of the counts; the scatter's
+// cursors start there; the counts are cleared for the next rebuild.
+__global__ void k_scan_apply(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
+                             const int16_t* __restrict__ tilevol, int* __restrict__ cnt, const int* __restrict__ tileofs,
+                             int* __restrict__ cstart, int* __restrict__ cursor) {
+    const int t = blockIdx.x;
+    const int v = tilevol[t];
+    if (v < 0 || !ctl[v].rebuild) {
+        return;
+    }
+    const DVol& V = vols[v];
+    const int64_t base = (int64_t)t * kScanTile;
+    const int64_t end = V.kofs + V.nkeys + 1;
+    constexpr int PER = kScanTile / kScanThreads;
+    int x[PER];
+    int s = 0;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int64_t e = base + threadIdx.x * PER + q;
+        x[q] = (e < end && e >= V.kofs) ? cnt[e] : 0;
+        s += x[q];
+    }
+    int incl = s;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if ((threadIdx.x & 31) >= o) {
+            incl += y;
+        }
+    }
+    __shared__ int wsum[kScanThreads / 32];
+    if ((threadIdx.x & 31) == 31) {
+        wsum[threadIdx.x >> 5] = incl;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        int w = threadIdx.x < kScanThreads / 32 ? wsum[threadIdx.x] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (threadIdx.x >= o) {
+                w += y;
+            }
+        }
+        if (threadIdx.x < kScanThreads / 32) {
+            wsum[threadIdx.x] = w;
+        }
+    }
+    __syncthreads();
+    int run = tileofs[t] + ((threadIdx.x >> 5) ? wsum[(threadIdx.x >> 5) - 1] : 0) + incl - s;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int64_t e = base + threadIdx.x * PER + q;
+        if (e < end && e >= V.kofs) {
+            cstart[e] = run;
+            cursor[e] = run;
+            cnt[e] = 0;
+        }
+        run += x[q];
+    }
+}
+
+// ---- scatter and in-bin order ------------------------------------------------------
+__global__ void k_scatter(const VolCtl* __restrict__ ctl, const DVol* __restrict__ vols, const uint16_t* __restrict__ nodevol,
+                          const int* __restrict__ key, int* __restrict__ cursor, int* __restrict__ sorted, int64_t N,
+                          Global* G) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) {
+        return;
+    }
+    const int v = nodevol[i];
+    if (v == 0xFFFF || !ctl[v].rebuild) {
+        return;
+    }
+    const DVol& V = vols[v];
+    const int pos = atomicAdd(cursor + V.kofs + key[i], 1);
+    if (pos < V.nofs || pos >= V.nofs + V.n) {
+        raise_error(G, 2, (int)i);
+        return;
+    }
+    sorted[pos] = (int)i;
+}
+
+// One thread per bin: the bin's ids ascending (the CPU's stable counting sort,
+// src/v2m_particles.cpp:791-795), then their positions and sizes in bin order.
+__global__ void k_binsort(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl, const int16_t* __restrict__ tilevol,
+                          const int* __restrict__ cstart, int* __restrict__ sorted, const float4* __restrict__ Pq,
+                          float4* __restrict__ Ps, int64_t KT) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= KT) {
+        return;
+    }
+    const int v = tilevol[e / kScanTile];
+    if (v < 0 || !ctl[v].rebuild) {
+        return;
+    }
+    const DVol& V = vols[v];
+    if (e < V.kofs || e >= V.kofs + V.nkeys) {
+        return;
+    }
+    const int s0 = cstart[e], s1 = cstart[e + 1];
+    for (int a = s0 + 1; a < s1; ++a) {
+        const int x = sorted[a];
+        int b = a - 1;
+        while (b >= s0 && sorted[b] > x) {
+            sorted[b + 1] = sorted[b];
+            --b;
+        }
+        sorted[b + 1] = x;
+    }
+    for (int s = s0; s < s1; ++s) {
+        const float4 p = Pq[sorted[s]];
+        Ps[s] = make_float4(p.x, p.y, p.z, fabsf(p.w));
+    }
+}
+
+// ---- K-nearest truss lists ----------------------------------------------------------
+// One warp per node. The accepted candidates (distance and label tests of
+// src/opencl/v2m_particle_body.cl:104-123) gather in a per-warp shared buffer;
+// the list is the K smallest by (distance, id) -- the reference's insertion
+// order is a total order, so its list is exactly these K, whatever the scan
+// order. Node ids are flat; within a volume they order like the reference's.
+constexpr int kCap = 64;
+
+struct NbrWarpSmem {
+    float d[kCap];
+    int id[kCap];
+};
+
+__device__ __forceinline__ bool pair_less(float da, int ia, float db, int ib) {
+    return da < db || (da == db && ia < ib);
+}
+
+// Keep the K smallest of buf[0..m) in rank order; returns the new count.
+__device__ __forceinline__ int warp_prune(NbrWarpSmem& sm, int m, int lane) {
+    float dd[2];
+    int ii[2], rk[2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        const int e = lane + 32 * r;
+        rk[r] = kCap;
+        if (e < m) {
+            dd[r] = sm.d[e];
+            ii[r] = sm.id[e];
+            int c = 0;
+            for (int f = 0; f < m; ++f) {
+                c += pair_less(sm.d[f], sm.id[f], dd[r], ii[r]);
+            }
+            rk[r] = c;
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        if (rk[r] < V2M_K) {
+            sm.d[rk[r]] = dd[r];
+            sm.id[rk[r]] = ii[r];
+        }
+    }
+    __syncwarp();
+    return m < V2M_K ? m : V2M_K;
+}
+
+__device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& sm, const float4* __restrict__ Pq,
+                               const uint8_t* __restrict__ typ, const uint16_t* __restrict__ lab,
+                               const int* __restrict__ cstart, const int* __restrict__ sorted,
+                               const float4* __restrict__ Ps, int* __restrict__ nbr, uint8_t* __restrict__ nnb, int64_t N) {
+    const DHash& H = V.H;
+    const float4 pi = Pq[i];
+    const float px = pi.x, py = pi.y, pz = pi.z;
+    const float hi = fabsf(pi.w);
+    const float ts = V.t + V.skin;
+    const float Ri = ts * hi;
+    const int ti_int = typ[i] == V2M_INTERIOR;
+    const int li = lab[i];
+    const int Li = level_of(H, Ri);
+    const int* cs = cstart + V.kofs;
+    int m = 0;
+    for (int L = Li - 1; L <= Li + 1; ++L) {
+        if (L < 0 || L >= H.nlev) {
+            continue;
+        }
+        const float bL = H.b0 * (float)(1 << L);
+        const float r = 0.5f * (Ri + bL);
+        const int x0 = bin_coord(H, L, px - r, H.ox, 0), x1 = bin_coord(H, L, px + r, H.ox, 0);
+        const int y0 = bin_coord(H, L, py - r, H.oy, 1), y1 = bin_coord(H, L, py + r, H.oy, 1);
+        const int z0 = bin_coord(H, L, pz - r, H.oz, 2), z1 = bin_coord(H, L, pz + r, H.oz, 2);
+        const int nbx = x1 - x0 + 1, nby = y1 - y0 + 1;
+        const int nbins = nbx * nby * (z1 - z0 + 1);
+        for (int bb = 0; bb < nbins; bb += 32) {
+            const int b = bb + lane;
+            int s0 = 0, c = 0;
+            if (b < nbins) {
+                const int cx = x0 + b % nbx, cy = y0 + (b / nbx) % nby, cz = z0 + b / (nbx * nby);
+                const int key = H.off[L] + cx + H.dim[L][0] * (cy + H.dim[L][1] * cz);
+                s0 = cs[key];
+                c = cs[key + 1] - s0;
+            }
+            int incl = c;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) {
+                    incl += y;
+                }
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            for (int cb = 0; cb < total; cb += 32) {
+                const int q = cb + lane;
+                // bin of candidate q: the first lane whose inclusive count exceeds q
+                int lo = 0, hi2 = 31;
+#pragma unroll
+                for (int st = 0; st < 5; ++st) {
+                    const int mid = (lo + hi2) >> 1;
+                    const int vm = __shfl_sync(0xffffffffu, incl, mid);
+                    if (q < vm) {
+                        hi2 = mid;
+                    } else {
+                        lo = mid + 1;
+                    }
+                }
+                const int bs0 = __shfl_sync(0xffffffffu, s0, lo);
+                const int bexc = __shfl_sync(0xffffffffu, incl - c, lo);
+                bool ok = false;
+                float dist = 0.0f;
+                int j = -1;
+                if (q < total) {
+                    const int s = bs0 + (q - bexc);
+                    j = sorted[s];
+                    if (j != (int)i) {
+                        const float4 ps = Ps[s];
+                        const float ex = ps.x - px, ey = ps.y - py, ez = ps.z - pz;
+                        const float d2 = ex * ex + ey * ey + ez * ez;
+                        const float rj = ts * 0.5f * (hi + ps.w);
+                        ok = !(d2 >= rj * rj);
+                        if (ok && ti_int && typ[j] == V2M_INTERIOR && lab[j] != li) {
+                            ok = false;
+                        }
+                        if (ok) {
+                            dist = sqrtf(d2);
+                        }
+                    }
+                }
+                const unsigned mask = __ballot_sync(0xffffffffu, ok);
+                if (ok) {
+                    const int slot = m + __popc(mask & ((1u << lane) - 1u));
+                    sm.d[slot] = dist;
+                    sm.id[slot] = j;
+                }
+                m += __popc(mask);
+                __syncwarp();
+                if (m > kCap - 32) {
+                    m = warp_prune(sm, m, lane);
+                }
+            }
+        }
+    }
+    // final ranks
+    m = warp_prune(sm, m, lane);
+    if (lane < m) {
+        nbr[(int64_t)lane * N + i] = sm.id[lane];
+    }
+    if (lane == 0) {
+        nnb[i] = (uint8_t)m;
+    }
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(kNbrThreads) k_neighbors(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
+                                                           const uint16_t* __restrict__ nodevol, const float4* __restrict__ Pq,
+                                                           const uint8_t* __restrict__ typ, const uint16_t* __restrict__ lab,
+                                                           const int* __restrict__ cstart, const int* __restrict__ sorted,
+                                                           const float4* __restrict__ Ps, int* __restrict__ nbr,
+                                                           uint8_t* __restrict__ nnb, int64_t N) {
+    __shared__ NbrWarpSmem sm[kNbrThreads / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t i = blockIdx.x * (int64_t)(kNbrThreads / 32) + w;
+    if (i >= N) {
+        return;
+    }
+    const int v = nodevol[i];
+    if (v == 0xFFFF || !ctl[v].rebuild) {
+        return;
+    }
+    warp_neighbors(vols[v], i, lane, sm[w], Pq, typ, lab, cstart, sorted, Ps, nbr, nnb, N);
+}
+
+// The self-refresh of the nodes past a full skin (list filled by k_move), one
+// warp per entry; the last block to finish empties the list.
+__global__ void __launch_bounds__(kNbrThreads) k_refresh(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
+                                                         const uint16_t* __restrict__ nodevol, const float4* __restrict__ Pq,
+                                                         const uint8_t* __restrict__ typ, const uint16_t* __restrict__ lab,
+                                                         const int* __restrict__ cstart, const int* __restrict__ sorted,
+                                                         const float4* __restrict__ Ps, int* __restrict__ nbr,
+                                                         uint8_t* __restrict__ nnb, float4* __restrict__ P0,
+                                                         const int* __restrict__ rlist, Global* G, int64_t N) {
+    __shared__ NbrWarpSmem sm[kNbrThreads / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int cnt = *((volatile int*)&G->nrefresh);
+    const int nw = gridDim.x * (kNbrThreads / 32);
+    for (int e = blockIdx.x * (kNbrThreads / 32) + w; e < cnt; e += nw) {
+        const int64_t i = rlist[e];
+        const int v = nodevol[i];
+        if (ctl[v].done) {
+            continue;
+        }
+        warp_neighbors(vols[v], i, lane, sm[w], Pq, typ, lab, cstart, sorted, Ps, nbr, nnb, N);
+        if (lane == 0) {
+            const float4 p = Pq[i];
+            P0[i] = make_float4(p.x, p.y, p.z, 0.0f);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const int d = atomicAdd(&G->blocks_done, 1);
+        if (d == (int)gridDim.x - 1) {
+            G->nrefresh = 0;
+            G->blocks_done = 0;
+            __threadfence();
+        }
+    }
+}
+
+// ---- bar forces ----------------------------------------------------------------
+// One thread per node; the lists are slot-major (nbr[k*N + i]) so a warp's k-th
+// entries are one coalesced 128-byte row; neighbour position + signed size is
+// one 16-byte gather. Bars are added in list order, as v2m_force does.
+__global__ void __launch_bounds__(256) k_force(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
+                                               const uint16_t* __restrict__ nodevol, const float4* __restrict__ Pq,
+                                               const int* __restrict__ nbr, const uint8_t* __restrict__ nnb,
+                                               float4* __restrict__ F, int64_t N) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) {
+        return;
+    }
+    const int v = nodevol[i];
+    if (v == 0xFFFF) {
+        return;
+    }
+    const VolCtl& c = ctl[v];
+    const DVol& V = vols[v];
+    if (c.done || c.it >= V.max_iters) {
+        return;
+    }
+    const float fscale = V.fscale, fsurf = V.fsurf;
+    const float4 p = Pq[i];
+    const float hi = fabsf(p.w);
+    const bool ni = signbit(p.w);
+    const int n = nnb[i];
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f, fa = 0.0f;
+    const int* row = nbr + i;
+    for (int k = 0; k < n; ++k) {
+        const int j = __ldg(row + (int64_t)k * N);
+        const float4 q = __ldg(Pq + j);
+        const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
+        const float l = sqrtf(ex * ex + ey * ey + ez * ez);
+        const float hj = fabsf(q.w);
+        const float l0 = ((ni && signbit(q.w)) ? fsurf : fscale) * 0.5f * (hi + hj);
+        if (l >= l0 || l <= 0.0f) {
+            continue;
+        }
+        const float f = (l0 - l) / l;
+        fx += f * ex;
+        fy += f * ey;
+        fz += f * ez;
+        fa += 1.0f;
+    }
+    F[i] = make_float4(fx, fy, fz, fa);
+}
+
+// ---- move + per-iteration reductions ------------------------------------------------
+// bin of |dp|/h in the log2 histogram: floor(log2(m)) of the correctly rounded
+// float log2 (computed in double and rounded once), as glibc's log2f gives
+__device__ __forceinline__ int hist_bin(float m) {
+    if (!(m > 0.0f)) {
+        return 0;
+    }
+    const float lf = (float)log2((double)m);
+    int b = 20 + (int)floorf(lf);
+    return b < 0 ? 0 : (b > 31 ? 31 : b);
+}
+
+__global__ void __launch_bounds__(kMoveThreads) k_move(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl,
+                                                      const uint16_t* __restrict__ nodevol, float4* __restrict__ Pq,
+                                                      const float4* __restrict__ F, float4* __restrict__ Vel,
+                                                      uint8_t* __restrict__ typ, const uint16_t* __restrict__ lab,
+                                                      uint32_t* __restrict__ part, float* __restrict__ mvout,
+                                                      float* __restrict__ pwout, const float4* __restrict__ P0,
+                                                      double* __restrict__ psum, int* __restrict__ rlist, Global* G,
+                                                      int64_t N) {
+    __shared__ int sh_hist[32];
+    __shared__ unsigned sh_max, sh_maxd;
+    __shared__ int sh_half, sh_vol;
+    __shared__ double sh_pw[kMoveThreads / 32];
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (threadIdx.x < 32) {
+        sh_hist[threadIdx.x] = 0;
+    }
+    if (threadIdx.x == 0) {
+        sh_max = 0u;
+        sh_maxd = 0u;
+        sh_half = 0;
+        sh_vol = -1;
+    }
+    __syncthreads();
+    // every node of a block lies in one volume (node ranges are kMoveThreads-aligned;
+    // padding sits at the end of a range)
+    const int v = i < N ? nodevol[i] : 0xFFFF;
+    bool active = v != 0xFFFF;
+    float pwv = 0.0f;
+    if (active) {
+        const DVol& Vd = vols[v];
+        const VolCtl& c = ctl[v];
+        if (c.done || c.it >= Vd.max_iters) {
+            active = false;
+        } else {
+            if (threadIdx.x == 0) {
+                sh_vol = v;
+            }
+            const DGrid& g = Vd.g;
+            const int fire = Vd.fire;
+            const float fdt = c.fdt, falpha = c.falpha;
+            const float4 pq = Pq[i];
+            NodeState st;
+            st.p[0] = pq.x;
+            st.p[1] = pq.y;
+            st.p[2] = pq.z;
+            st.hn = fabsf(pq.w);
+            st.a = lab[i];
+            st.ty = typ[i];
+            const uint32_t pp = part[i];
+            st.pb = (int)(pp & 0xFFFFu);
+            st.pc = (int)(pp >> 16);
+            const int ty0 = st.ty;
+            const float p0 = pq.x, p1 = pq.y, p2 = pq.z;
+            const float h = size_at(g, Vd.hmode, p0, p1, p2);
+            float m = 0.0f;
+            float4 vnew = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (ty0 != V2M_CORNER) {
+                const float4 f4 = F[i];
+                const float stiff = f4.w > 1.0f ? f4.w : 1.0f;
+                float ac[3] = { f4.x / stiff, f4.y / stiff, f4.z / stiff };
+                float s[3];
+                bool go = true;
+                if (fire) {
+                    float vv[3] = { 0.0f, 0.0f, 0.0f };
+                    if (!c.vzero) {
+                        const float4 v4 = Vel[i];
+                        vv[0] = v4.x;
+                        vv[1] = v4.y;
+                        vv[2] = v4.z;
+                    }
+                    const float pv = ac[0] * vv[0] + ac[1] * vv[1] + ac[2] * vv[2];
+                    pwv = pv;
+                    if (pv < 0.0f) {
+                        vv[0] = vv[1] = vv[2] = 0.0f;
+                    } else {
+                        const float vn = sqrtf(vv[0] * vv[0] + vv[1] * vv[1] + vv[2] * vv[2]);
+                        const float an = sqrtf(ac[0] * ac[0] + ac[1] * ac[1] + ac[2] * ac[2]);
+                        if (an > 0.0f) {
+                            for (int k = 0; k < 3; ++k) {
+                                vv[k] = (1.0f - falpha) * vv[k] + falpha * vn * ac[k] / an;
+                            }
+                        }
+                    }
+                    for (int k = 0; k < 3; ++k) {
+                        vv[k] += fdt * ac[k];
+                        s[k] = fdt * vv[k];
+                    }
+                } else {
+                    for (int k = 0; k < 3; ++k) {
+                        s[k] = Vd.dt * ac[k];
+                    }
+                }
+                const float sl = sqrtf(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+                if (sl < 5e-4f * h) {
+                    go = false;
+                }
+                if (go) {
+                    if (sl > Vd.maxstep * h) {
+                        for (int k = 0; k < 3; ++k) {
+                            s[k] *= Vd.maxstep * h / sl;
+                        }
+                    }
+                    m = move_step(g, Vd.hmode, h, s, Vd.maxstep, Vd.snap, Vd.voxmode, st);
+                    if (fire && m > 0.0f && st.ty == ty0) {
+                        vnew = make_float4((st.p[0] - p0) / fdt, (st.p[1] - p1) / fdt, (st.p[2] - p2) / fdt, 0.0f);
+                    }
+                }
+            }
+            if (fire) {
+                Vel[i] = vnew;
+                pwout[i] = pwv;
+            }
+            mvout[i] = m;
+            Pq[i] = make_float4(st.p[0], st.p[1], st.p[2], pack_h(st.hn, st.ty));
+            typ[i] = (uint8_t)st.ty;
+            part[i] = (uint32_t)(st.pb & 0xFFFF) | ((uint32_t)(st.pc & 0xFFFF) << 16);
+            // the iteration's reductions
+            atomicAdd(&sh_hist[hist_bin(m)], 1);
+            atomicMax(&sh_max, __float_as_uint(m));
+            const float4 q0 = P0[i];
+            const float ex = st.p[0] - q0.x, ey = st.p[1] - q0.y, ez = st.p[2] - q0.z;
+            const float hh = st.hn;
+            const float m2 = ex * ex + ey * ey + ez * ez, s2 = Vd.skin * Vd.skin * hh * hh;
+            if (Vd.policy == 1) {
+                atomicMax(&sh_maxd, __float_as_uint(sqrtf(m2) / hh));
+            }
+            if (m2 > s2) {
+                const int e = atomicAdd(&G->nrefresh, 1);
+                rlist[e] = (int)i;
+                atomicAdd(&ctl[v].nrefresh, 1);
+            } else if (m2 > 0.25f * s2) {
+                atomicAdd(&sh_half, 1);
+            }
+        }
+    }
+    // FIRE power of the block, fixed-shape double tree (deterministic)
+    double pd = active ? (double)pwv : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+        pd += __shfl_down_sync(0xffffffffu, pd, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sh_pw[threadIdx.x >> 5] = pd;
+    }
+    __syncthreads();
+    const int bv = sh_vol;
+    if (bv < 0) {
+        return;
+    }
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kMoveThreads / 32; ++w) {
+            t += sh_pw[w];
+        }
+        psum[blockIdx.x] = t;
+        VolCtl* cv = ctl + bv;
+        if (sh_max) {
+            atomicMax(&cv->maxbits, sh_max);
+        }
+        if (sh_half) {
+            atomicAdd(&cv->nhalf, sh_half);
+        }
+        if (sh_maxd) {
+            atomicMax(reinterpret_cast<unsigned*>(&cv->pad1), sh_maxd);
+        }
+    }
+    if (threadIdx.x < 32 && sh_hist[threadIdx.x]) {
+        atomicAdd(&ctl[bv].hist[threadIdx.x], sh_hist[threadIdx.x]);
+    }
+}
+
+// Serial FIRE power (the CPU's order: node 0 first, one double accumulator),
+// for bit-exact replays; one thread per volume.
+__global__ void k_power_serial(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl, const float* __restrict__ pw,
+                               double* __restrict__ pser, int nvol) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nvol) {
+        return;
+    }
+    const DVol& V = vols[v];
+    if (!V.fire || ctl[v].done || ctl[v].it >= V.max_iters) {
+        return;
+    }
+    double t = 0.0;
+    for (int64_t i = 0; i < V.n; ++i) {
+        t += (double)pw[V.nofs + i];
+    }
+    pser[v] = t;
+}
+
+// ---- the loop's control (one block per volume) ---------------------------------------
+__global__ void k_control(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl, const double* __restrict__ psum,
+                          const double* __restrict__ pser, int serial, int move_threads) {
+    const int v = blockIdx.x;
+    const DVol& V = vols[v];
+    VolCtl& c = ctl[v];
+    __shared__ double red[kCtlThreads];
+    __shared__ int s_skip;
+    if (threadIdx.x == 0) {
+        s_skip = c.done || c.it >= V.max_iters;
+        if (s_skip) {
+            c.rebuild = 0;
+        }
+    }
+    __syncthreads();
+    if (s_skip) {
+        return;
+    }
+    double P = 0.0;
+    if (V.fire && !serial) {
+        const int b0 = (int)(V.nofs / move_threads);
+        const int nb = (V.n + move_threads - 1) / move_threads;
+        double t = 0.0;
+        for (int b = threadIdx.x; b < nb; b += kCtlThreads) {
+            t += psum[b0 + b];
+        }
+        red[threadIdx.x] = t;
+        __syncthreads();
+        for (int w = kCtlThreads / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) {
+                red[threadIdx.x] += red[threadIdx.x + w];
+            }
+            __syncthreads();
+        }
+        P = red[0];
+    } else if (V.fire) {
+        P = pser[v];
+    }
+    if (threadIdx.x != 0) {
+        return;
+    }
+    const int it = c.it;
+    if (V.fire) {
+        c.power = P;
+        if (P >= 0.0) {
+            if (++c.npos > 5) {
+                c.fdt = fminf(c.fdt * 1.1f, V.fire_dtmax);
+                c.falpha *= 0.99f;
+            }
+            c.vzero = 0;
+        } else {
+            c.npos = 0;
+            c.fdt = fmaxf(c.fdt * 0.5f, 0.05f * V.fire_dt0);
+            c.falpha = 0.1f;
+            ++c.resets;
+            c.vzero = 1;
+        }
+    }
+    c.iters = it + 1;
+    c.last_move = __uint_as_float(c.maxbits);
+    int acc = 0, b99 = 31;
+    for (int b = 0; b < 32; ++b) {
+        acc += c.hist[b];
+        if ((double)acc >= 0.99 * (double)V.n) {
+            b99 = b;
+            break;
+        }
+    }
+    const float p99 = ldexpf(1.0f, b99 - 20 + 1);
+    c.last_p99 = p99;
+    c.nhalf_last = c.nhalf;
+    c.nrefresh_last = c.nrefresh;
+    const float maxd = __uint_as_float((unsigned)c.pad1);
+    for (int b = 0; b < 32; ++b) {
+        c.hist[b] = 0;
+    }
+    c.maxbits = 0u;
+    c.nhalf = 0;
+    c.nrefresh = 0;
+    c.pad1 = 0;
+    c.it = it + 1;
+    if (p99 < V.dptol && (!V.fire || c.fdt >= 0.25f * V.fire_dt0)) {
+        c.done = 1;
+        c.rebuild = 0;
+        c.stop_reason = 1;
+        return;
+    }
+    int reb;
+    if (V.policy == 1) {
+        reb = maxd > 0.1f;
+    } else {
+        const bool endgame = it >= V.max_iters * 4 / 5 || p99 < 4.0f * V.dptol;
+        const int div = endgame ? (V.rebuild_div > 1000 ? V.rebuild_div : 1000) : V.rebuild_div;
+        reb = c.nhalf_last > V.n / div;
+    }
+    c.rebuild = reb;
+    if (reb) {
+        ++c.rebuilds;
+    }
+}
+
+// ---- small utilities -----------------------------------------------------------------
+__global__ void k_set_rebuild(VolCtl* ctl, int nvol, int val) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < nvol && !ctl[v].done) {
+        ctl[v].rebuild = val;
+        if (val) {
+            ++ctl[v].rebuilds;
+        }
+    }
+}
+
+// Row-major copy of the slot-major lists of one volume (for checks and read-back).
+__global__ void k_lists_rowmajor(const int* __restrict__ nbr, const uint8_t* __restrict__ nnb, int64_t nofs, int n,
+                                 int64_t N, int* __restrict__ out, int* __restrict__ nout) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)n * V2M_K) {
+        return;
+    }
+    const int64_t i = t / V2M_K;
+    const int k = (int)(t % V2M_K);
+    const int c = nnb[nofs + i];
+    out[t] = k < c ? nbr[(int64_t)k * N + nofs + i] - (int)nofs : 0;
+    if (k == 0) {
+        nout[i] = c;
+    }
+}
+
+// The inverse: row-major host lists (local ids) into the slot-major store.
+__global__ void k_lists_from_rowmajor(int* __restrict__ nbr, uint8_t* __restrict__ nnb, int64_t nofs, int n, int64_t N,
+                                      const int* __restrict__ in, const int* __restrict__ nin) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)n * V2M_K) {
+        return;
+    }
+    const int64_t i = t / V2M_K;
+    const int k = (int)(t % V2M_K);
+    const int c = nin[i];
+    if (k < c) {
+        nbr[(int64_t)k * N + nofs + i] = in[t] + (int)nofs;
+    }
+    if (k == 0) {
+        nnb[nofs + i] = (uint8_t)c;
+    }
+}
+
+// Positions / types / sizes between the reference's layout and the packed one.
+__global__ void k_pack_nodes(const float* __restrict__ P, const uint8_t* __restrict__ typ, const DVol* __restrict__ vols,
+                             int v, float4* __restrict__ Pq) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const DVol& V = vols[v];
+    if (t >= V.n) {
+        return;
+    }
+    const float x = P[3 * t], y = P[3 * t + 1], z = P[3 * t + 2];
+    const float h = size_at(V.g, V.hmode, x, y, z);
+    Pq[V.nofs + t] = make_float4(x, y, z, pack_h(h, typ[V.nofs + t]));
+}
+
+__global__ void k_unpack_P(const float4* __restrict__ Pq, int64_t nofs, int n, float* __restrict__ P) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n) {
+        return;
+    }
+    const float4 p = Pq[nofs + t];
+    P[3 * t] = p.x;
+    P[3 * t + 1] = p.y;
+    P[3 * t + 2] = p.z;
+}
+
+__global__ void k_hn(const float4* __restrict__ Pq, int64_t nofs, int n, float* __restrict__ out) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) {
+        out[t] = fabsf(Pq[nofs + t].w);
+    }
+}
+
+__global__ void k_set_hn(float4* __restrict__ Pq, int64_t nofs, int n, const float* __restrict__ in,
+                         const uint8_t* __restrict__ typ) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) {
+        const float4 p = Pq[nofs + t];
+        Pq[nofs + t] = make_float4(p.x, p.y, p.z, pack_h(in[t], typ[nofs + t]));
+    }
+}
+
+// Re-sign w after a host write of the types.
+__global__ void k_resign(float4* __restrict__ Pq, const uint8_t* __restrict__ typ, int64_t nofs, int n) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) {
+        const float4 p = Pq[nofs + t];
+        Pq[nofs + t] = make_float4(p.x, p.y, p.z, pack_h(fabsf(p.w), typ[nofs + t]));
+    }
+}
+
+__global__ void k_float4_to3(const float4* __restrict__ a, int64_t nofs, int n, float* __restrict__ out) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) {
+        const float4 p = a[nofs + t];
+        out[3 * t] = p.x;
+        out[3 * t + 1] = p.y;
+        out[3 * t + 2] = p.z;
+    }
+}
+
+__global__ void k_float3_to4(const float* __restrict__ in, int64_t nofs, int n, float4* __restrict__ a) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) {
+        a[nofs + t] = make_float4(in[3 * t], in[3 * t + 1], in[3 * t + 2], 0.0f);
+    }
+}
+
+// Local ids of a volume's bin-sorted node list.
+__global__ void k_local_ids(const int* __restrict__ a, int64_t nofs, int n, int* __restrict__ out) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) {
+        out[t] = a[nofs + t] - (int)nofs;
+    }
+}
+
+__global__ void k_local_cstart(const int* __restrict__ a, int64_t kofs, int cnt, int64_t nofs, int* __restrict__ out) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < cnt) {
+        out[t] = a[kofs + t] - (int)nofs;
+    }
+}
+
+// ---- launchers -----------------------------------------------------------------------
+static inline unsigned nblk(int64_t n, int b) {
+    return (unsigned)((n + b - 1) / b);
+}
+
+void launch_keys(cudaStream_t s, const Dev& d) {
+    k_keys<<<nblk(d.N, 256), 256, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.key, d.cnt, d.P0, d.N, d.G);
+}
+
+void launch_scan(cudaStream_t s, const Dev& d) {
+    k_scan_tiles<<<d.ntile_key, kScanThreads, 0, s>>>(d.vols, d.ctl, d.tilevol, d.cnt, d.tilesum, d.KT);
+    k_scan_vol<<<d.nvol, 1024, 0, s>>>(d.vols, d.ctl, d.tilesum, d.tileofs);
+    k_scan_apply<<<d.ntile_key, kScanThreads, 0, s>>>(d.vols, d.ctl, d.tilevol, d.cnt, d.tileofs, d.cstart, d.cursor);
+}
+
+void launch_scatter(cudaStream_t s, const Dev& d) {
+    k_scatter<<<nblk(d.N, 256), 256, 0, s>>>(d.ctl, d.vols, d.nodevol, d.key, d.cursor, d.sorted, d.N, d.G);
+    k_binsort<<<nblk(d.KT, 256), 256, 0, s>>>(d.vols, d.ctl, d.tilevol, d.cstart, d.sorted, d.Pq, d.Ps, d.KT);
+}
+
+void launch_neighbors(cudaStream_t s, const Dev& d) {
+    k_neighbors<<<nblk(d.N, kNbrThreads / 32), kNbrThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.typ, d.lab,
+                                                                     d.cstart, d.sorted, d.Ps, d.nbr, d.nnb, d.N);
+}
+
+void launch_force(cudaStream_t s, const Dev& d, int threads) {
+    k_force<<<nblk(d.N, threads), threads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.nbr, d.nnb, d.F, d.N);
+}
+
+void launch_move(cudaStream_t s, const Dev& d) {
+    k_move<<<nblk(d.N, kMoveThreads), kMoveThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.F, d.Vel, d.typ, d.lab,
+                                                            d.part, d.mv, d.pw, d.P0, d.psum, d.rlist, d.G, d.N);
+}
+
+void launch_control(cudaStream_t s, const Dev& d, int serial) {
+    if (serial) {
+        k_power_serial<<<nblk(d.nvol, 32), 32, 0, s>>>(d.vols, d.ctl, d.pw, d.pser, d.nvol);
+    }
+    k_control<<<d.nvol, kCtlThreads, 0, s>>>(d.vols, d.ctl, d.psum, d.pser, serial, kMoveThreads);
+}
+
+void launch_refresh(cudaStream_t s, const Dev& d, int blocks) {
+    k_refresh<<<blocks, kNbrThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.typ, d.lab, d.cstart, d.sorted, d.Ps,
+                                              d.nbr, d.nnb, d.P0, d.rlist, d.G, d.N);
+}
+
+void launch_set_rebuild(cudaStream_t s, const Dev& d, int val) {
+    k_set_rebuild<<<nblk(d.nvol, 128), 128, 0, s>>>(d.ctl, d.nvol, val);
+}
+
+void launch_lists_rowmajor(cudaStream_t s, const Dev& d, int64_t nofs, int n, int* out, int* nout) {
+    k_lists_rowmajor<<<nblk((int64_t)n * V2M_K, 256), 256, 0, s>>>(d.nbr, d.nnb, nofs, n, d.N, out, nout);
+}
+
+void launch_lists_from_rowmajor(cudaStream_t s, const Dev& d, int64_t nofs, int n, const int* in, const int* nin) {
+    k_lists_from_rowmajor<<<nblk((int64_t)n * V2M_K, 256), 256, 0, s>>>(d.nbr, d.nnb, nofs, n, d.N, in, nin);
+}
+
+void launch_pack_nodes(cudaStream_t s, const Dev& d, int v, int n, const float* P, const uint8_t* typ_all) {
+    k_pack_nodes<<<nblk(n, 256), 256, 0, s>>>(P, typ_all, d.vols, v, d.Pq);
+}
+
+void launch_unpack_P(cudaStream_t s, const Dev& d, int64_t nofs, int n, float* P) {
+    k_unpack_P<<<nblk(n, 256), 256, 0, s>>>(d.Pq, nofs, n, P);
+}
+
+void launch_hn(cudaStream_t s, const Dev& d, int64_t nofs, int n, float* out) {
+    k_hn<<<nblk(n, 256), 256, 0, s>>>(d.Pq, nofs, n, out);
+}
+
+void launch_set_hn(cudaStream_t s, const Dev& d, int64_t nofs, int n, const float* in) {
+    k_set_hn<<<nblk(n, 256), 256, 0, s>>>(d.Pq, nofs, n, in, d.typ);
+}
+
+void launch_resign(cudaStream_t s, const Dev& d, int64_t nofs, int n) {
+    k_resign<<<nblk(n, 256), 256, 0, s>>>(d.Pq, d.typ, nofs, n);
+}
+
+void launch_float4_to3(cudaStream_t s, const float4* a, int64_t nofs, int n, float* out) {
+    k_float4_to3<<<nblk(n, 256), 256, 0, s>>>(a, nofs, n, out);
+}
+
+void launch_float3_to4(cudaStream_t s, const float* in, int64_t nofs, int n, float4* a) {
+    k_float3_to4<<<nblk(n, 256), 256, 0, s>>>(in, nofs, n, a);
+}
+
+void launch_local_ids(cudaStream_t s, const int* a, int64_t nofs, int n, int* out) {
+    k_local_ids<<<nblk(n, 256), 256, 0, s>>>(a, nofs, n, out);
+}
+
+void launch_local_cstart(cudaStream_t s, const int* a, int64_t kofs, int cnt, int64_t nofs, int* out) {
+    k_local_cstart<<<nblk(cnt, 256), 256, 0, s>>>(a, kofs, cnt, nofs, out);
+}
+
+}  // namespace v2m

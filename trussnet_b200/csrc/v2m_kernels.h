@@ -1,0 +1,75 @@
+// v2m_kernels.h -- device buffers of a session and the kernel launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "v2m_types.cuh"
+
+namespace v2m {
+
+constexpr int kScanTile = 1024;     // bin entries per scan tile (volume bin ranges are aligned to it)
+constexpr int kScanThreads = 256;
+constexpr int kNbrThreads = 128;    // 4 warps, one node each
+constexpr int kMoveThreads = 256;   // volume node ranges are aligned to it
+constexpr int kCtlThreads = 256;
+constexpr int kNodeAlign = kMoveThreads;
+
+// Every device array of a session (flat over its volumes).
+struct Dev {
+    int nvol = 0;
+    int64_t N = 0;       // nodes incl. per-volume padding
+    int64_t KT = 0;      // bin-start entries incl. padding
+    int ntile_key = 0;
+    DVol* vols = nullptr;
+    VolCtl* ctl = nullptr;
+    Global* G = nullptr;
+    uint16_t* nodevol = nullptr;   // volume of each node, 0xFFFF = padding
+    int16_t* tilevol = nullptr;    // volume of each scan tile, -1 = none
+    float4* Pq = nullptr;          // x, y, z, +-h (sign: non-interior)
+    float4* F = nullptr;           // force + active bars
+    float4* Vel = nullptr;         // FIRE velocity
+    float4* P0 = nullptr;          // positions at the last list build
+    float4* Ps = nullptr;          // bin-order positions + h at the last build
+    uint8_t* typ = nullptr;
+    uint16_t* lab = nullptr;
+    uint32_t* part = nullptr;      // two uint16 partner labels
+    float* mv = nullptr;
+    float* pw = nullptr;
+    int* key = nullptr;
+    int* sorted = nullptr;
+    int* nbr = nullptr;            // slot-major: nbr[k*N + i]
+    uint8_t* nnb = nullptr;
+    int* rlist = nullptr;
+    int* cnt = nullptr;
+    int* cstart = nullptr;
+    int* cursor = nullptr;
+    int* tilesum = nullptr;
+    int* tileofs = nullptr;
+    double* psum = nullptr;        // FIRE power per move block
+    double* pser = nullptr;        // serial FIRE power per volume
+};
+
+void launch_keys(cudaStream_t s, const Dev& d);
+void launch_scan(cudaStream_t s, const Dev& d);
+void launch_scatter(cudaStream_t s, const Dev& d);
+void launch_neighbors(cudaStream_t s, const Dev& d);
+void launch_force(cudaStream_t s, const Dev& d, int threads);
+void launch_move(cudaStream_t s, const Dev& d);
+void launch_control(cudaStream_t s, const Dev& d, int serial);
+void launch_refresh(cudaStream_t s, const Dev& d, int blocks);
+void launch_set_rebuild(cudaStream_t s, const Dev& d, int val);
+void launch_lists_rowmajor(cudaStream_t s, const Dev& d, int64_t nofs, int n, int* out, int* nout);
+void launch_lists_from_rowmajor(cudaStream_t s, const Dev& d, int64_t nofs, int n, const int* in, const int* nin);
+void launch_pack_nodes(cudaStream_t s, const Dev& d, int v, int n, const float* P, const uint8_t* typ_all);
+void launch_unpack_P(cudaStream_t s, const Dev& d, int64_t nofs, int n, float* P);
+void launch_hn(cudaStream_t s, const Dev& d, int64_t nofs, int n, float* out);
+void launch_set_hn(cudaStream_t s, const Dev& d, int64_t nofs, int n, const float* in);
+void launch_resign(cudaStream_t s, const Dev& d, int64_t nofs, int n);
+void launch_float4_to3(cudaStream_t s, const float4* a, int64_t nofs, int n, float* out);
+void launch_float3_to4(cudaStream_t s, const float* in, int64_t nofs, int n, float4* a);
+void launch_local_ids(cudaStream_t s, const int* a, int64_t nofs, int n, int* out);
+void launch_local_cstart(cudaStream_t s, const int* a, int64_t kofs, int cnt, int64_t nofs, int* out);
+
+}  // namespace v2m

@@ -1,0 +1,96 @@
+// v2m_types.cuh -- the device-side descriptors of the relaxation (host and device).
+//
+// A launch covers every volume of a session at once: node, bin and tile indices
+// are flat over the volumes, and each thread block works inside one volume (its
+// tile), whose descriptor (DVol) and mutable control block (VolCtl) it reads.
+#pragma once
+
+#include <cstdint>
+
+#ifndef V2M_K
+#define V2M_K 24
+#define V2M_MAXLEV 8
+#define V2M_BS 8
+#define V2M_SLOT 512
+#define V2M_BL 16
+#define V2M_INTERIOR 0
+#define V2M_INTERFACE 1
+#define V2M_JUNCTION 2
+#define V2M_CORNER 3
+#define V2M_NOLAB 0xFFFF
+#endif
+
+namespace v2m {
+
+// The read-only fields of one volume (tn::Grid, src/v2m_grid.h:45-81), device pointers.
+struct DGrid {
+    int nx, ny, nz, nbx, nby, nbz;
+    float vx, vy, vz;
+    const uint16_t* L;
+    const int* bl_cnt;
+    const uint16_t* bl_lab;
+    const int* bl_slot;
+    const float* phi;
+    const float* hvox;
+    const float* gI;
+    const float* gTW;
+    int gm;
+};
+
+// Multi-level hash geometry (V2mHash, src/opencl/v2m_particle_body.cl:21-27).
+struct DHash {
+    float b0;
+    int nlev;
+    float ox, oy, oz;
+    int dim[V2M_MAXLEV][3];
+    int off[V2M_MAXLEV];
+};
+
+// One volume: fields, hash, where its nodes / bins / tiles live, its parameters.
+struct DVol {
+    DGrid g;
+    DHash H;
+    int64_t nofs;      // first node (flat)
+    int n;             // nodes
+    int64_t kofs;      // first bin-start entry (flat; the volume owns nkeys + 1 entries)
+    int nkeys;
+    // tiles: [tofs_node, +ntile_node) node tiles, [tofs_key, +ntile_key) bin tiles
+    int tofs_node, ntile_node, tofs_key, ntile_key;
+    // parameters (tn::RelaxParams)
+    float t, skin, fscale, fsurf, dt, maxstep, snap, dptol;
+    int voxmode, fire, max_iters, rebuild_div, hmode, policy;
+    float fire_dt0, fire_dtmax;
+};
+
+// Mutable per-volume loop state (relax_cpu's locals, src/v2m_particles.cpp:822-946).
+struct VolCtl {
+    int it;            // iterations done
+    int done;          // 1: converged or max_iters reached (every later stage is a no-op)
+    int rebuild;       // 1: the rebuild stages run at the end of this iteration
+    int vzero;         // 1: FIRE reset: the next move starts from zero velocities
+    float fdt, falpha; // FIRE time step and steering
+    int npos, resets;
+    int rebuilds;      // lists built so far
+    int iters;         // RelaxStats.iters
+    float last_move, last_p99;
+    double power;      // last FIRE power sum
+    int nhalf_last, nrefresh_last, stop_reason, pad0;
+    // accumulators of the current iteration (cleared by the control stage)
+    int hist[32];
+    unsigned int maxbits;
+    int nhalf;
+    int nrefresh;
+    int pad1;
+};
+
+// Session-wide counters and the self-refresh work list.
+struct Global {
+    int nrefresh;        // entries in the refresh list
+    int blocks_done;     // last-block-done counter of the refresh kernel
+    int err;             // kernel error flag (first error code)
+    int err_info;
+};
+
+constexpr int kMaxVol = 1024;
+
+}  // namespace v2m

@@ -1,0 +1,172 @@
+"""The relaxation's public Python surface, mirroring the reference's C++ one.
+
+  relax_cl(g, prm, nd, st=None, device=-1)
+      tn::relax_cl (src/v2m_gpu.h:16-18 of fangq/trussnet): relax the nodes in
+      place on a CUDA device; same contract as tn::relax_cpu
+      (src/v2m_particles.h:99). Raises V2mError (a RuntimeError, as the
+      reference throws std::runtime_error) when the device path fails; there is
+      no CPU fallback inside -- the caller decides, as run_pipeline does
+      (src/v2m_pipeline.cpp:492-526).
+  relax_cl_batch(grids, prms, nodes, device=-1)
+      many independent volumes in one set of launches (no reference counterpart).
+  Session
+      the relaxation state kept on the device: the stages one at a time, repeated
+      runs from the same seeds, internal arrays for checks.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib
+from .types import (ARR, V2M_K, Grid, GridView, Nodes, NodesView, RelaxParams, RelaxParamsC, RelaxStats,
+                    RelaxStatsC)
+
+_ARR_DTYPE = {"key": np.int32, "sorted": np.int32, "cstart": np.int32, "Ps": np.float32, "nbr": np.int32,
+              "nnb": np.int32, "F": np.float32, "hn": np.float32, "mv": np.float32, "V": np.float32, "pw": np.float32,
+              "P0": np.float32, "hist": np.int32, "P": np.float32, "typ": np.uint8, "part": np.uint16}
+_PER_NODE = {"key": 1, "sorted": 1, "Ps": 4, "nbr": V2M_K, "nnb": 1, "F": 4, "hn": 1, "mv": 1, "V": 3, "pw": 1,
+             "P0": 3, "P": 3, "typ": 1, "part": 2}
+
+
+def device_count() -> int:
+    return int(_lib.load().v2m_cuda_device_count())
+
+
+def _views(grids, prms, nodes):
+    gv = (GridView * len(grids))(*[g.view() for g in grids])
+    pv = (RelaxParamsC * len(prms))(*[p.to_c() for p in prms])
+    nv = (NodesView * len(nodes))(*[nd.view() for nd in nodes])
+    return gv, pv, nv
+
+
+def relax_cl(g: Grid, prm: RelaxParams, nd: Nodes, st: RelaxStats | None = None, device: int = -1) -> RelaxStats:
+    """tn::relax_cl: relax `nd` in place on CUDA device `device` (-1 = the first)."""
+    L = _lib.load()
+    gv, pv, nv = _views([g], [prm], [nd])
+    sv = (RelaxStatsC * 1)()
+    _lib.check(L.v2m_relax_cuda(gv, pv, nv, sv, device))
+    out = RelaxStats.from_c(sv[0])
+    if st is not None:
+        st.__dict__.update(out.__dict__)
+    return out
+
+
+def relax_cl_batch(grids: Sequence[Grid], prms: Sequence[RelaxParams], nodes: Sequence[Nodes],
+                   device: int = -1) -> list[RelaxStats]:
+    """Relax many independent volumes together; each volume's result is the one
+    relax_cl gives for it alone."""
+    L = _lib.load()
+    if not (len(grids) == len(prms) == len(nodes)):
+        raise ValueError("grids, params and nodes must have the same length")
+    gv, pv, nv = _views(grids, prms, nodes)
+    sv = (RelaxStatsC * len(grids))()
+    _lib.check(L.v2m_relax_cuda_batch(len(grids), gv, pv, nv, sv, device))
+    return [RelaxStats.from_c(s) for s in sv]
+
+
+class Session:
+    """Device-resident relaxation state of one or more volumes."""
+
+    def __init__(self, grids, prms, nodes, device: int = -1):
+        if isinstance(grids, Grid):
+            grids, prms, nodes = [grids], [prms], [nodes]
+        self.L = _lib.load()
+        self.nvol = len(grids)
+        self.n = [nd.size() for nd in nodes]
+        gv, pv, nv = _views(grids, prms, nodes)
+        h = C.c_void_p()
+        _lib.check(self.L.v2m_session_create(self.nvol, gv, pv, nv, device, C.byref(h)))
+        self.h = h
+        self.nkeys = []
+        self.nlev = []
+        for v in range(self.nvol):
+            n, nk, nl = C.c_int64(), C.c_int64(), C.c_int32()
+            _lib.check(self.L.v2m_session_info(self.h, v, C.byref(n), C.byref(nk), C.byref(nl)))
+            self.nkeys.append(nk.value)
+            self.nlev.append(nl.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.v2m_session_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def reset(self):
+        _lib.check(self.L.v2m_session_reset(self.h))
+
+    def rebuild(self):
+        _lib.check(self.L.v2m_session_rebuild(self.h))
+
+    def force(self):
+        _lib.check(self.L.v2m_session_force(self.h))
+
+    def step_tail(self):
+        _lib.check(self.L.v2m_session_step_tail(self.h))
+
+    def iterate(self, iters: int, graph: bool = True):
+        _lib.check(self.L.v2m_session_iterate(self.h, int(iters), int(graph)))
+
+    def run(self, graph: bool = True):
+        _lib.check(self.L.v2m_session_run(self.h, int(graph)))
+
+    def synchronize(self):
+        _lib.check(self.L.v2m_session_synchronize(self.h))
+
+    def stats(self, vol: int = 0) -> RelaxStats:
+        sv = RelaxStatsC()
+        _lib.check(self.L.v2m_session_stats(self.h, vol, C.byref(sv)))
+        return RelaxStats.from_c(sv)
+
+    def read_nodes(self, nd: Nodes, vol: int = 0) -> Nodes:
+        v = nd.view()
+        _lib.check(self.L.v2m_session_read_nodes(self.h, vol, C.byref(v)))
+        return nd
+
+    def read(self, name: str, vol: int = 0) -> np.ndarray:
+        dt = _ARR_DTYPE[name]
+        if name == "cstart":
+            count = self.nkeys[vol] + 1
+        elif name == "hist":
+            count = 34
+        else:
+            count = self.n[vol] * _PER_NODE[name]
+        out = np.zeros(max(count, 1), dt)
+        _lib.check(self.L.v2m_session_read_array(self.h, vol, ARR[name], out.ctypes.data, out.nbytes))
+        return out[:count]
+
+    def write(self, name: str, a: np.ndarray, vol: int = 0):
+        a = np.ascontiguousarray(a, _ARR_DTYPE[name])
+        _lib.check(self.L.v2m_session_write_array(self.h, vol, ARR[name], a.ctypes.data, a.nbytes))
+
+    def write_lists(self, nbr: np.ndarray, nnb: np.ndarray, vol: int = 0):
+        nbr = np.ascontiguousarray(nbr, np.int32)
+        nnb = np.ascontiguousarray(nnb, np.int32)
+        _lib.check(self.L.v2m_session_write_lists(self.h, vol, nbr.ctypes.data, nnb.ctypes.data))
+
+    def timed_runs(self, runs: int, graph: bool = True, time_force: bool = False) -> float:
+        """Device milliseconds of `runs` whole relaxations from the seeds (CUDA events)."""
+        ms = C.c_float()
+        _lib.check(self.L.v2m_session_timed_runs(self.h, int(runs), int(graph), int(time_force), C.byref(ms)))
+        return ms.value
+
+    def clear_counters(self):
+        _lib.check(self.L.v2m_session_clear_counters(self.h))
+
+    def counters(self):
+        a, b, c = C.c_int64(), C.c_int64(), C.c_double()
+        _lib.check(self.L.v2m_session_counters(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return dict(launches=a.value, force_launches=b.value, force_ms=c.value)
