@@ -1,0 +1,126 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes access to oracle/liboracle.so, the plain-C
+restatement of the relaxation (v2m_oracle.c / v2m_oracle_body.h) in FP32
+without contraction ("f32") and in FP64 ("f64").
+
+Only tests, the smoke check and the benchmark's CPU-baseline leg use it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from trussnet_b200.types import ARR, V2M_K, Grid, GridView, Nodes, NodesView, RelaxParams, RelaxStats, RelaxStatsC
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SO = os.path.join(HERE, "liboracle.so")
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(SO):
+            raise FileNotFoundError(f"{SO} is not built (make -f oracle/Makefile)")
+        L = C.CDLL(SO)
+        vp = C.c_void_p
+        for suf in ("f32", "f64"):
+            getattr(L, f"orc_create_{suf}").restype = vp
+            getattr(L, f"orc_create_{suf}").argtypes = [C.POINTER(GridView), vp, C.POINTER(NodesView)]
+            getattr(L, f"orc_free_{suf}").argtypes = [vp]
+            for f in ("rebuild", "force", "move", "tail", "run"):
+                getattr(L, f"orc_{f}_{suf}").argtypes = [vp]
+            getattr(L, f"orc_info_{suf}").argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+            getattr(L, f"orc_counts_{suf}").argtypes = [vp, vp, vp]
+            getattr(L, f"orc_read_{suf}").restype = C.c_int64
+            getattr(L, f"orc_read_{suf}").argtypes = [vp, C.c_int, vp, C.c_int64]
+            getattr(L, f"orc_write_{suf}").argtypes = [vp, C.c_int, vp, C.c_int64]
+        L.orc_relax_f32.argtypes = [C.POINTER(GridView), vp, C.POINTER(NodesView), C.POINTER(RelaxStatsC)]
+        _lib = L
+    return _lib
+
+
+_INT = {"key": np.int32, "sorted": np.int32, "cstart": np.int32, "nbr": np.int32, "nnb": np.int32,
+        "typ": np.uint8, "part": np.uint16, "hist": np.int32}
+_PER = {"key": 1, "sorted": 1, "Ps": 4, "nbr": V2M_K, "nnb": 1, "F": 4, "hn": 1, "mv": 1, "V": 3, "pw": 1,
+        "P0": 3, "P": 3, "typ": 1, "part": 2}
+
+
+class Oracle:
+    """One precision of the restatement: Oracle('f32') or Oracle('f64')."""
+
+    def __init__(self, variant: str = "f32"):
+        assert variant in ("f32", "f64")
+        self.v = variant
+        self.real = np.float32 if variant == "f32" else np.float64
+        self.L = load()
+
+    def relax(self, g: Grid, prm: RelaxParams, nd: Nodes) -> RelaxStats:
+        """A whole relaxation (float) into nd, like relax_cpu."""
+        assert self.v == "f32"
+        gv, pv, nv, sv = g.view(), prm.to_c(), nd.view(), RelaxStatsC()
+        if self.L.orc_relax_f32(C.byref(gv), C.byref(pv), C.byref(nv), C.byref(sv)) != 0:
+            raise RuntimeError("oracle relax failed")
+        return RelaxStats.from_c(sv)
+
+    def state(self, g: Grid, prm: RelaxParams, nd: Nodes) -> "OracleState":
+        return OracleState(self, g, prm, nd)
+
+
+class OracleState:
+    def __init__(self, o: Oracle, g: Grid, prm: RelaxParams, nd: Nodes):
+        self.o, self.L, self.v = o, o.L, o.v
+        self._keep = (g, nd)     # the oracle reads the grid arrays in place
+        gv, pv, nv = g.view(), prm.to_c(), nd.view()
+        self.h = getattr(self.L, f"orc_create_{self.v}")(C.byref(gv), C.byref(pv), C.byref(nv))
+        if not self.h:
+            raise RuntimeError("oracle create failed")
+        self.n = nd.size()
+        nk, nl = C.c_int64(), C.c_int32()
+        getattr(self.L, f"orc_info_{self.v}")(self.h, C.byref(nk), C.byref(nl))
+        self.nkeys, self.nlev = nk.value, nl.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            getattr(self.L, f"orc_free_{self.v}")(self.h)
+            self.h = None
+
+    def _call(self, f):
+        return getattr(self.L, f"orc_{f}_{self.v}")(self.h)
+
+    def rebuild(self):
+        self._call("rebuild")
+
+    def force(self):
+        self._call("force")
+
+    def move_only(self):
+        self._call("move")
+
+    def tail(self) -> bool:
+        return bool(self._call("tail"))
+
+    def run(self):
+        self._call("run")
+
+    def counts(self) -> dict:
+        iv = np.zeros(8, np.int32)
+        dv = np.zeros(5, np.float64)
+        getattr(self.L, f"orc_counts_{self.v}")(self.h, iv.ctypes.data, dv.ctypes.data)
+        return dict(it=int(iv[0]), stopped=int(iv[1]), nhalf=int(iv[2]), nrefresh=int(iv[3]), rebuilds=int(iv[4]),
+                    fire_resets=int(iv[5]), fire_dt=dv[0], fire_alpha=dv[1], power=dv[2], mmax=dv[3], p99=dv[4])
+
+    def read(self, name: str) -> np.ndarray:
+        dt = _INT.get(name, self.o.real)
+        count = self.nkeys + 1 if name == "cstart" else (32 if name == "hist" else self.n * _PER[name])
+        out = np.zeros(max(count, 1), dt)
+        nb = getattr(self.L, f"orc_read_{self.v}")(self.h, ARR[name], out.ctypes.data, out.nbytes)
+        if nb < 0:
+            raise RuntimeError(f"oracle read {name} failed")
+        return out[:count]
+
+    def write(self, name: str, a: np.ndarray):
+        a = np.ascontiguousarray(a, _INT.get(name, self.o.real))
+        if getattr(self.L, f"orc_write_{self.v}")(self.h, ARR[name], a.ctypes.data, a.nbytes) != 0:
+            raise RuntimeError(f"oracle write {name} failed")

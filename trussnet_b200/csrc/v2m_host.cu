@@ -453,13 +453,22 @@ void enqueue_rebuild(v2m_session* s) {
     s->launches += 8;
 }
 
+// (inside a stream capture an event record only becomes a graph node with
+// cudaEventRecordExternal; without it the event is a capture dependency only)
+void record(v2m_session* s, cudaEvent_t e) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    ck(cudaStreamIsCapturing(s->stream, &cs), "capture status");
+    ck(cudaEventRecordWithFlags(e, s->stream, cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : 0),
+       "event");
+}
+
 void enqueue_force(v2m_session* s, cudaEvent_t e0, cudaEvent_t e1) {
     if (e0) {
-        ck(cudaEventRecord(e0, s->stream), "event");
+        record(s, e0);
     }
     launch_force(s->stream, s->d, s->force_threads);
     if (e1) {
-        ck(cudaEventRecord(e1, s->stream), "event");
+        record(s, e1);
     }
     s->launches += 1;
     s->force_launches += 1;
@@ -545,9 +554,8 @@ void do_iterate(v2m_session* s, int iters, int graph) {
             if (s->time_force) {
                 for (int k = 0; k < G; ++k) {
                     float ms = 0.0f;
-                    if (cudaEventElapsedTime(&ms, s->gev[2 * k], s->gev[2 * k + 1]) == cudaSuccess) {
-                        s->force_ms += ms;
-                    }
+                    ck(cudaEventElapsedTime(&ms, s->gev[2 * k], s->gev[2 * k + 1]), "force event time");
+                    s->force_ms += ms;
                 }
             }
             if (all_done(s, c)) {
