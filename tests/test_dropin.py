@@ -1,0 +1,47 @@
+"""The drop-in: tn::relax_cl (libv2m_relax_cl.so) called by the reference
+pipeline's own dispatch over the reference's types (tests/dropin_driver.cpp).
+
+CPU: without a device relax_cl throws std::runtime_error and the pipeline's
+fallback (restore the seeds, relax_cpu) produces the reference result.
+GPU: relax_cl runs on the device and its nodes equal relax_cpu's bit for bit
+(FIRE power summed in the CPU's serial order).
+"""
+import os
+import subprocess
+
+import pytest
+
+from trussnet_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DRIVER = os.path.join(ROOT, "tests", "_bin", "dropin_driver")
+
+needs_driver = pytest.mark.skipif(not os.path.exists(DRIVER), reason="drop-in driver not built (needs the reference)")
+
+
+def run(env=None, dim=40, iters=30):
+    e = dict(os.environ)
+    e.update(env or {})
+    r = subprocess.run([DRIVER, str(dim), str(iters)], capture_output=True, text=True, env=e, timeout=600)
+    assert r.returncode == 0, r.stderr
+    fields = dict(kv.split("=") for kv in r.stdout.split())
+    return fields, r.stderr
+
+
+@needs_driver
+@pytest.mark.skipif(_lib.load().v2m_cuda_device_count() > 0, reason="a CUDA device is present")
+def test_fallback_without_device():
+    f, err = run()
+    assert f["path"] == "cpu-fallback"
+    assert "relax_cl failed" in err and "no CUDA device" in err
+    assert f["identical"] == "1"
+
+
+@needs_driver
+@pytest.mark.gpu
+def test_dropin_on_device_equals_relax_cpu():
+    f, err = run({"V2M_CUDA_SERIAL_POWER": "1"})
+    assert f["path"] == "cuda", err
+    assert f["identical"] == "1"
+    a, b = f["iters"].split("/")
+    assert a == b

@@ -1,0 +1,146 @@
+"""CPU: the C restatement (oracle/liboracle.so) pinned to the reference.
+
+1. Against the golden fixtures (outputs of the reference's own relax_cpu and
+   its stages, tests/golden/make_golden.py): bit-exact.
+2. Against the compiled reference itself (oracle/_ref) where it is built, on
+   fresh seeded inputs: bit-exact.
+3. FP32 against FP64 for one step from identical positions and lists: forces
+   and positions within the stated relative tolerance.
+"""
+import numpy as np
+import pytest
+
+import cases
+import golden_io
+from cases import first_diff, same_bits
+from oracle.oracle import Oracle
+
+GOLDEN = golden_io.names()
+
+
+@pytest.fixture(scope="module")
+def f32():
+    return Oracle("f32")
+
+
+@pytest.mark.parametrize("name", GOLDEN)
+def test_golden_rebuild_and_force(name, f32):
+    g, nd, prm, d = golden_io.load(name)
+    s = f32.state(g, prm, nd.copy())
+    s.rebuild()
+    for a in ("key", "sorted", "cstart", "nnb", "nbr", "Ps"):
+        diff = first_diff(s.read(a), d[a])
+        assert diff is None, f"{a}: {diff}"
+    s.force()
+    assert same_bits(s.read("F"), d["F"])
+    s.tail()
+    for a in ("P", "typ", "part", "mv"):
+        diff = first_diff(s.read(a), d["it1_" + a])
+        assert diff is None, f"iteration 1 {a}: {diff}"
+
+
+@pytest.mark.parametrize("name", GOLDEN)
+def test_golden_full_relax(name, f32):
+    g, nd, prm, d = golden_io.load(name)
+    x = nd.copy()
+    st = f32.relax(g, prm, x)
+    assert same_bits(x.P, d["run_P"]), first_diff(x.P, d["run_P"])
+    assert same_bits(x.typ, d["run_typ"]) and same_bits(x.part, d["run_part"])
+    it, builds, resets, ni, nf, nj, nc = (int(v) for v in d["run_stats"])
+    assert (st.iters, st.rebuilds, st.fire_resets) == (it, builds, resets)
+    assert (st.n_interior, st.n_interface, st.n_junction, st.n_corner) == (ni, nf, nj, nc)
+
+
+@pytest.mark.parametrize("name", ["sphere_small", "shells_small", "tpm_small", "ref_phantom"])
+@pytest.mark.parametrize("fire", [True, False])
+def test_against_reference(name, fire, ref, f32):
+    g, nd = cases.ref_phantom(ref) if name == "ref_phantom" else getattr(cases, name)()
+    prm = cases.params(25, fire=fire)
+    a = nd.copy()
+    st_ref = ref.relax_cpu(g, prm, a)
+    b = nd.copy()
+    st = f32.relax(g, prm, b)
+    assert same_bits(b.P, a.P), first_diff(b.P, a.P)
+    assert same_bits(b.typ, a.typ) and same_bits(b.part, a.part)
+    assert (st.iters, st.rebuilds, st.fire_resets) == (st_ref.iters, st_ref.rebuilds, st_ref.fire_resets)
+
+
+def test_stages_against_reference(ref, f32):
+    g, nd = cases.ref_phantom(ref)
+    prm = cases.params(10)
+    r = ref.state(g, prm, nd.copy())
+    o = f32.state(g, prm, nd.copy())
+    r.rebuild()
+    o.rebuild()
+    for it in range(4):
+        r.force()
+        o.force()
+        assert same_bits(o.read("F"), r.read("F")), it
+        r.tail()
+        o.tail()
+        for a in ("P", "typ", "part", "mv", "V", "pw", "nnb", "P0"):
+            assert same_bits(o.read(a), r.read(a)), (it, a, first_diff(o.read(a), r.read(a)))
+        rc, oc = r.counts(), o.counts()
+        for k in ("it", "nhalf", "nrefresh", "rebuilds", "fire_resets"):
+            assert rc[k] == oc[k], (it, k)
+        assert rc["power"] == oc["power"]
+
+
+# FP32 against FP64 -------------------------------------------------------------
+# Tolerance, for one step from identical positions and lists:
+#  * forces: each node's |F32 - F64|_inf within REL_TOL of its per-bar force
+#    scale h_i * n_active_i (a bar pushes with at most l0 - l < l0 ~ h);
+#  * positions of free steps (INTERIOR before and after, no projection):
+#    |P32 - P64|_inf within REL_TOL of |P64|_inf (a float position is itself
+#    rounded to 6e-8 of its magnitude);
+#  * positions of trapped nodes (crossing, glide, projection): they end where a
+#    bracketed root search stops, whose own tolerance is 1e-4 of its radius and
+#    whose sign tests near the root can go either way in either precision; their
+#    error is measured and bounded by PROJ_TOL of h_i (|P32 - P64|_inf / h_i).
+# Nodes whose discrete decisions differ between the precisions (active-bar
+# count, type after the move) are excluded and counted (at most 0.1%).
+REL_TOL = 1e-6
+PROJ_TOL = 1e-2
+
+
+def fp64_step_errors(g, nd, prm):
+    o32, o64 = Oracle("f32").state(g, prm, nd.copy()), Oracle("f64").state(g, prm, nd.copy())
+    o32.rebuild()
+    o64.write("nbr", o32.read("nbr"))
+    o64.write("nnb", o32.read("nnb"))
+    o32.force()
+    o64.force()
+    F32 = o32.read("F").reshape(-1, 4).astype(np.float64)
+    F64 = o64.read("F").reshape(-1, 4)
+    hn = o64.read("hn")
+    same_active = F32[:, 3] == F64[:, 3]
+    ok = same_active & (F64[:, 3] > 0)
+    ferr = np.abs(F32[ok, :3] - F64[ok, :3]).max(axis=1) / (hn[ok] * F64[ok, 3])
+    # one move from identical forces (the FP32 ones), so both take the same step
+    o64.write("F", F32.reshape(-1))
+    o32.move_only()
+    o64.move_only()
+    P32 = o32.read("P").reshape(-1, 3).astype(np.float64)
+    P64 = o64.read("P").reshape(-1, 3)
+    t32 = o32.read("typ")
+    same_type = t32 == o64.read("typ")
+    dif = np.abs(P32 - P64).max(axis=1)
+    free = same_type & (nd.typ == 0) & (t32 == 0)
+    trapped = same_type & ~free
+    perr = (dif / np.maximum(np.abs(P64).max(axis=1), hn))[free]
+    proj = (dif / hn)[trapped] if trapped.any() else np.zeros(1)
+    return ferr, perr, int((~same_active).sum()), int((~same_type).sum()), proj
+
+
+@pytest.mark.parametrize("name", ["sphere_small", "shells_small", "tpm_small"])
+def test_fp32_within_tolerance_of_fp64(name, record_property):
+    g, nd = getattr(cases, name)()
+    prm = cases.params(1)
+    ferr, perr, nact, ntyp, proj = fp64_step_errors(g, nd, prm)
+    record_property("max_force_rel_err", float(ferr.max()))
+    record_property("max_free_position_rel_err", float(perr.max()))
+    record_property("max_trapped_position_rel_err", float(proj.max()))
+    assert ferr.max() <= REL_TOL, f"force error {ferr.max():.3g}"
+    assert perr.max() <= REL_TOL, f"position error {perr.max():.3g}"
+    assert proj.max() <= PROJ_TOL, f"trapped position error {proj.max():.3g}"
+    assert nact <= len(nd.P) // 1000 and ntyp <= len(nd.P) // 1000

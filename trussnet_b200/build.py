@@ -90,6 +90,27 @@ def build_shim(force: bool = False) -> str | None:
     return SHIM
 
 
+def build_dropin(force: bool = False) -> str | None:
+    """tests/_bin/dropin_driver: the reference pipeline's relax dispatch over the
+    reference's types, linked with the shim and the reference CPU path (a test
+    program; built only where the reference headers exist, then it travels)."""
+    out = os.path.join(ROOT, "tests", "_bin", "dropin_driver")
+    src = os.path.join(ROOT, "tests", "dropin_driver.cpp")
+    refso = os.path.join(ROOT, "oracle", "_ref", "libv2m_ref.so")
+    if not os.path.isdir(os.path.join(REF, "src")) or not os.path.exists(SHIM) or not os.path.exists(refso):
+        return out if os.path.exists(out) else None
+    if not force and not _stale(out, [src, SHIM, refso]):
+        return out
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    cmd = ["/usr/bin/g++", "-O2", "-std=c++17", "-I", os.path.join(REF, "src"), src, "-o", out,
+           "-L", HERE, "-lv2m_relax_cl", "-lv2m_cuda", "-L", os.path.dirname(refso), "-lv2m_ref",
+           "-Wl,-rpath,$ORIGIN/../../trussnet_b200:$ORIGIN/../../oracle/_ref", "-fopenmp"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"drop-in driver build failed:\n{r.stderr[-4000:]}")
+    return out
+
+
 def build_oracle() -> None:
     """The CPU checkers under oracle/ (test infrastructure)."""
     env = dict(os.environ)
@@ -103,6 +124,7 @@ def build_all(force: bool = False) -> None:
     build_cuda(force=force)
     build_shim(force=force)
     build_oracle()
+    build_dropin(force=force)
 
 
 if __name__ == "__main__":
