@@ -203,14 +203,18 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+_PINNED = []   # the torch tensors that own the pinned pages of pinned_copy's arrays
+
+
 def pinned_copy(a: np.ndarray) -> np.ndarray:
+    """A copy of `a` in page-locked host memory."""
     import torch
     t = torch.empty(a.shape, dtype={np.dtype(np.float32): torch.float32, np.dtype(np.uint16): torch.int16,
                                     np.dtype(np.int32): torch.int32, np.dtype(np.uint8): torch.uint8}[a.dtype],
                     pin_memory=True)
+    _PINNED.append(t)
     out = t.numpy().view(a.dtype)
     out[...] = a
-    out._keep = t  # noqa: the tensor owns the pinned pages
     return out
 
 
@@ -265,33 +269,9 @@ def run_cuda(args):
     st = sess.stats()
     sess.close()
     # end to end through the public call (tn::relax_cl's C ABI) with pinned host buffers
-    gp = Grid(nx=g.nx, ny=g.ny, nz=g.nz, vs=g.vs, L=pinned_copy(g.L), bl_cnt=pinned_copy(g.bl_cnt),
-              bl_lab=pinned_copy(g.bl_lab), bl_slot=pinned_copy(g.bl_slot), phi=pinned_copy(g.phi),
-              h=pinned_copy(g.h), hmin=g.hmin, hmax=g.hmax)
-    npin = Nodes(P=pinned_copy(nd.P), lab=pinned_copy(nd.lab), typ=pinned_copy(nd.typ), part=pinned_copy(nd.part))
-    e2e_times = []
-    for k in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
-        npin.P[...] = nd.P
-        npin.typ[...] = nd.typ
-        npin.part[...] = nd.part
-        barrier()
-        t0 = time.perf_counter()
-        relax_cl(gp, prm, npin, device=local)
-        torch.cuda.synchronize(local)
-        t1 = time.perf_counter()
-        if k > 0:   # the first call loads the module and warms the allocator
-            e2e_times.append(t1 - t0)
     e2e = None
-    if e2e_times:
-        e2e_s = statistics.mean(e2e_times)
-        if world > 1:
-            t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        h2d = g.nbytes() + nd.nbytes()
-        d2h = nd.P.nbytes + nd.typ.nbytes + nd.part.nbytes
-        e2e = {"value": world * n * iters / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "s_per_step": e2e_s}
+    if args.e2e_steps > 0:
+        e2e = e2e_leg(args, g, nd, prm, n, iters, world, local, barrier)
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(g, nd, prm, args.ref_iters)
@@ -309,6 +289,40 @@ def run_cuda(args):
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def e2e_leg(args, g, nd, prm, n, iters, world, local, barrier):
+    """The same metric through relax_cl (the C ABI's v2m_relax_cuda) from pinned
+    host buffers: every step uploads the grid and the seeds, relaxes, and reads
+    the nodes back."""
+    import torch
+    from trussnet_b200 import relax_cl
+    from trussnet_b200.types import Grid, Nodes
+    gp = Grid(nx=g.nx, ny=g.ny, nz=g.nz, vs=g.vs, L=pinned_copy(g.L), bl_cnt=pinned_copy(g.bl_cnt),
+              bl_lab=pinned_copy(g.bl_lab), bl_slot=pinned_copy(g.bl_slot), phi=pinned_copy(g.phi),
+              h=pinned_copy(g.h), hmin=g.hmin, hmax=g.hmax)
+    npin = Nodes(P=pinned_copy(nd.P), lab=pinned_copy(nd.lab), typ=pinned_copy(nd.typ), part=pinned_copy(nd.part))
+    e2e_times = []
+    for k in range(args.e2e_steps + 1):
+        npin.P[...] = nd.P
+        npin.typ[...] = nd.typ
+        npin.part[...] = nd.part
+        barrier()
+        t0 = time.perf_counter()
+        relax_cl(gp, prm, npin, device=local)
+        torch.cuda.synchronize(local)
+        t1 = time.perf_counter()
+        if k > 0:   # the first call loads the module and warms the allocator
+            e2e_times.append(t1 - t0)
+    e2e_s = statistics.mean(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = g.nbytes() + nd.nbytes()
+    d2h = nd.P.nbytes + nd.typ.nbytes + nd.part.nbytes
+    return {"value": world * n * iters / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "s_per_step": e2e_s}
 
 
 def main():

@@ -78,3 +78,9 @@ def first_diff(a: np.ndarray, b: np.ndarray):
 
 def copy_nodes(nd: Nodes) -> Nodes:
     return nd.copy()
+
+
+@functools.lru_cache(maxsize=None)
+def gray_small():
+    """48^3 gray-scale sphere, 2 thresholds (labels 0..2)."""
+    return synth.gray_sphere(dim=48, seed=6)

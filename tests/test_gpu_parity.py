@@ -16,7 +16,7 @@ from trussnet_b200.types import V2M_CORNER, V2M_K, RelaxParams
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["sphere_small", "shells_small", "tpm_small", "ref_phantom"]
+CASES = ["sphere_small", "shells_small", "tpm_small", "ref_phantom", "gray_small"]
 
 
 def load_case(name, ref):
@@ -213,3 +213,64 @@ def test_edge_cases(ref, cuda_lib):
     z = nd.copy()
     relax_cl(g, cases.params(0), z)
     assert same_bits(z.P, nd.P)
+
+
+def test_trilinear_h_matches_oracle(cuda_lib):
+    """Extension: h sampled trilinearly (h_mode 1) -- no reference counterpart;
+    bit-exact with the FP32 restatement in the same mode."""
+    from oracle.oracle import Oracle
+    g, nd = cases.shells_small()
+    prm = cases.params(30, h_mode=1)
+    a = nd.copy()
+    Oracle("f32").relax(g, prm, a)
+    b = nd.copy()
+    import os
+    os.environ["V2M_CUDA_SERIAL_POWER"] = "1"
+    try:
+        relax_cl(g, prm, b)
+    finally:
+        del os.environ["V2M_CUDA_SERIAL_POWER"]
+    for f in ("P", "typ", "part"):
+        d = first_diff(getattr(b, f), getattr(a, f))
+        assert d is None, f"{f}: {d}"
+
+
+@pytest.mark.parametrize("name", ["sphere_small", "shells_small", "tpm_small"])
+def test_step_within_tolerance_of_fp64(name, cuda_lib, record_property):
+    """One step from identical positions and lists: CUDA forces within 1e-6 of the
+    FP64 restatement (per-bar scale h_i * active bars), free-step positions within
+    1e-6 of |P|; trapped positions within the projection tolerance (1e-2 h)."""
+    from oracle.oracle import Oracle
+    g, nd = getattr(cases, name)()
+    prm = cases.params(1)
+    o64 = Oracle("f64").state(g, prm, nd.copy())
+    with Session(g, prm, nd.copy()) as s:
+        s.rebuild()
+        n = nd.size()
+        nbr, nnb = s.read("nbr"), s.read("nnb")
+        o64.write("nbr", rowmajor_lists(nbr, nnb, n).reshape(-1))
+        o64.write("nnb", nnb)
+        s.force()
+        o64.force()
+        F = s.read("F").reshape(-1, 4).astype(np.float64)
+        F64 = o64.read("F").reshape(-1, 4)
+        hn = o64.read("hn")
+        ok = (F[:, 3] == F64[:, 3]) & (F64[:, 3] > 0)
+        ferr = np.abs(F[ok, :3] - F64[ok, :3]).max(axis=1) / (hn[ok] * F64[ok, 3])
+        o64.write("F", F.reshape(-1))
+        s.step_tail()
+        o64.move_only()
+        P = s.read("P").reshape(-1, 3).astype(np.float64)
+        P64 = o64.read("P").reshape(-1, 3)
+        t = s.read("typ")
+        same = t == o64.read("typ")
+        free = same & (nd.typ == 0) & (t == 0)
+        dif = np.abs(P - P64).max(axis=1)
+        perr = (dif / np.maximum(np.abs(P64).max(axis=1), hn))[free]
+        proj = (dif / hn)[same & ~free]
+    record_property("max_force_rel_err", float(ferr.max()))
+    record_property("max_free_position_rel_err", float(perr.max()))
+    record_property("max_trapped_position_rel_err", float(proj.max()) if proj.size else 0.0)
+    assert ferr.max() <= 1e-6 and perr.max() <= 1e-6
+    assert proj.size == 0 or proj.max() <= 1e-2
+    assert (~same).sum() <= n // 1000

@@ -51,7 +51,7 @@ def test_golden_full_relax(name, f32):
     assert (st.n_interior, st.n_interface, st.n_junction, st.n_corner) == (ni, nf, nj, nc)
 
 
-@pytest.mark.parametrize("name", ["sphere_small", "shells_small", "tpm_small", "ref_phantom"])
+@pytest.mark.parametrize("name", ["sphere_small", "shells_small", "tpm_small", "ref_phantom", "gray_small"])
 @pytest.mark.parametrize("fire", [True, False])
 def test_against_reference(name, fire, ref, f32):
     g, nd = cases.ref_phantom(ref) if name == "ref_phantom" else getattr(cases, name)()

@@ -307,3 +307,25 @@ WORKLOADS = {
     "tpm182": lambda **kw: tpm(**kw),
     "ellipsoids128": lambda **kw: ellipsoids(**kw),
 }
+
+
+def gray_sphere(dim=48, seed=0, thresholds=(0.3, 0.6), widths=(0.2, 0.2), h=2.0, spacing=2.0):
+    """Gray-scale input (tn::Grid gI / gTW / gm, src/v2m_grid.h:70-73): a smooth
+    radial intensity with seeded noise; label = number of thresholds <= I; the
+    interfaces are the iso-surfaces I = t_k."""
+    rng = np.random.default_rng(seed)
+    c = (dim - 1) / 2.0
+    z, y, x = np.mgrid[0:dim, 0:dim, 0:dim].astype(np.float32)
+    r = np.sqrt((x - c) ** 2 + (y - c) ** 2 + (z - c) ** 2) / (0.45 * dim)
+    I = (1.0 - r + 0.05 * value_noise((dim, dim, dim), 2, 2, rng)).astype(np.float32)
+    t = np.asarray(thresholds, np.float32)
+    L = np.zeros(I.shape, np.uint16)
+    for tk in t:
+        L += (I >= tk).astype(np.uint16)
+    hf = np.full(L.shape, h, np.float32)
+    g = build_grid(L, hf, h, h)
+    g.gI = np.ascontiguousarray(I.reshape(-1))
+    g.gTW = np.concatenate([t, np.asarray(widths, np.float32)]).astype(np.float32)
+    g.gm = int(t.size)
+    nd = seed_lattice(L, hf, rng, density=h / spacing, hmin=h, hmax=h)
+    return g, nd
