@@ -206,7 +206,49 @@ int v2m_session_counters(v2m_session* s, int64_t* launches, int64_t* force_launc
  * launch (read back with v2m_session_counters).
  */
 int v2m_session_timed_runs(v2m_session* s, int runs, int graph, int time_force, float* ms);
+
+/*
+ * Autotuner: times the launch shapes that cannot change a result (the force
+ * kernel's block, the list kernel's warps per block) on the session's own
+ * lists, keeps the fastest, appends it to the tuning cache
+ * (V2M_CUDA_TUNE_CACHE, default $HOME/.cache/v2m_cuda_tune.txt) and resets the
+ * session to its seeds. A session created with V2M_CUDA_AUTOTUNE=1 uses the
+ * cached shapes or tunes once. `report` (may be NULL) receives the timings.
+ */
+int v2m_session_autotune(v2m_session* s, int reps, char* report, int64_t report_len);
+int v2m_session_shapes(v2m_session* s, int32_t* force_threads, int32_t* nbr_threads);
 int v2m_session_clear_counters(v2m_session* s);
+
+/*
+ * The differentiable relaxation unroll and its adjoint (no counterpart in the
+ * reference). K Jacobi relaxation steps on frozen lists (row-major nbr[i*K+k],
+ * local ids, as v2m_session_read_array returns them), the target size h(x)
+ * interpolated trilinearly in a sizing grid G of m[0] x m[1] x m[2] values
+ * (x fastest) at x = (a cs[0], b cs[1], c cs[2]); the active bars of each step
+ * are taped by the forward pass and replayed by the backward pass; checkpoints
+ * every `ckpt` steps. Loss = sum over the list entries of (l_ij / h_ij - 1)^2.
+ * Position, gradient and grid arrays are DEVICE pointers (float, x/y/z
+ * interleaved per node); the calls synchronize before returning.
+ */
+typedef struct v2m_unroll v2m_unroll;
+int v2m_unroll_create(int64_t n, const int32_t* nbr, const int32_t* nnb, const uint8_t* typ, const int32_t* m,
+                      const float* cs, float fscale, float fsurf, float dt, int K, int ckpt, int device,
+                      v2m_unroll** out);
+int v2m_unroll_destroy(v2m_unroll* u);
+/* K steps from x0 into xK; replay != 0 reuses the tape of the last recording forward pass */
+int v2m_unroll_forward(v2m_unroll* u, const float* x0, const float* G, float* xK, int replay);
+/* loss at x (host double) */
+int v2m_unroll_loss(v2m_unroll* u, const float* x, const float* G, double* loss);
+/* gx = gscale dLoss/dx at x; gG = gscale dLoss/dG (accumulate != 0: added to the internal grid accumulator) */
+int v2m_unroll_loss_backward(v2m_unroll* u, const float* x, const float* G, float gscale, float* gx, float* gG,
+                             int accumulate);
+/* reverse of the last forward pass: gx0 = dL/dx0 and gG = dL/dG (+ gG_in if not NULL) from gxK = dL/dxK */
+int v2m_unroll_backward(v2m_unroll* u, const float* G, const float* gxK, float* gx0, float* gG, const float* gG_in);
+/* the tape (K x n active-bar masks) to host memory */
+int v2m_unroll_tape(v2m_unroll* u, uint32_t* host, int64_t count);
+/* device milliseconds of the last forward (K steps) and backward passes */
+int v2m_unroll_timing(v2m_unroll* u, float* ms_forward, float* ms_backward);
+const char* v2m_unroll_last_error(void);
 
 #ifdef __cplusplus
 }

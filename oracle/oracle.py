@@ -124,3 +124,52 @@ class OracleState:
         a = np.ascontiguousarray(a, _INT.get(name, self.o.real))
         if getattr(self.L, f"orc_write_{self.v}")(self.h, ARR[name], a.ctypes.data, a.nbytes) != 0:
             raise RuntimeError(f"oracle write {name} failed")
+
+
+# ---- the differentiable unroll (v2m_unroll_oracle.c), FP64 ----------------------
+def _unroll_args(nbr, nnb, typ, G, cs):
+    L = load()
+    if not hasattr(L, "_unroll_set"):
+        vp = C.c_void_p
+        for f in ("orc_unroll_forward_f64", "orc_unroll_grad_f64"):
+            getattr(L, f).restype = C.c_double
+            getattr(L, f).argtypes = [C.c_int, vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_double, C.c_int,
+                                      vp, vp] + ([vp] if f.endswith("grad_f64") else []) + [vp, C.c_int]
+        L._unroll_set = True
+    nbr = np.ascontiguousarray(nbr, np.int32).reshape(-1)
+    nnb = np.ascontiguousarray(nnb, np.int32)
+    typ = np.ascontiguousarray(typ, np.uint8)
+    G = np.ascontiguousarray(G, np.float64)
+    m = np.array(G.shape[::-1], np.int32)          # G is [m2, m1, m0] (x fastest)
+    cs = np.ascontiguousarray(cs, np.float64)
+    return L, nbr, nnb, typ, G, m, cs
+
+
+def unroll_forward_f64(nbr, nnb, typ, G, cs, fscale, fsurf, dt, K, x0, tape=None):
+    """FP64: K unroll steps from x0 [n,3]; returns (xK, loss at xK, tape). With
+    tape=None the active bars are decided and recorded; with a tape (uint32
+    [K, n]) they are replayed (the taped function)."""
+    L, nbr, nnb, typ, G, m, cs = _unroll_args(nbr, nnb, typ, G, cs)
+    x0 = np.ascontiguousarray(x0, np.float64)
+    xK = np.zeros_like(x0)
+    replay = tape is not None
+    tape = np.zeros((K, len(nnb)), np.uint32) if tape is None else np.ascontiguousarray(tape, np.uint32)
+    loss = L.orc_unroll_forward_f64(len(nnb), nbr.ctypes.data, nnb.ctypes.data, typ.ctypes.data, m.ctypes.data,
+                                    cs.ctypes.data, G.ctypes.data, fscale, fsurf, dt, K, x0.ctypes.data,
+                                    xK.ctypes.data, tape.ctypes.data, int(replay))
+    return xK, loss, tape
+
+
+def unroll_grad_f64(nbr, nnb, typ, G, cs, fscale, fsurf, dt, K, x0, tape=None):
+    """FP64: (loss, dloss/dx0 [n,3], dloss/dG [shape of G], tape) by reverse mode
+    of the taped function (recorded here when tape is None)."""
+    L, nbr, nnb, typ, G, m, cs = _unroll_args(nbr, nnb, typ, G, cs)
+    x0 = np.ascontiguousarray(x0, np.float64)
+    gx = np.zeros_like(x0)
+    gG = np.zeros_like(G)
+    replay = tape is not None
+    tape = np.zeros((K, len(nnb)), np.uint32) if tape is None else np.ascontiguousarray(tape, np.uint32)
+    loss = L.orc_unroll_grad_f64(len(nnb), nbr.ctypes.data, nnb.ctypes.data, typ.ctypes.data, m.ctypes.data,
+                                 cs.ctypes.data, G.ctypes.data, fscale, fsurf, dt, K, x0.ctypes.data, gx.ctypes.data,
+                                 gG.ctypes.data, tape.ctypes.data, int(replay))
+    return loss, gx, gG, tape

@@ -1,0 +1,124 @@
+"""GPU: the hand-written adjoint of the relaxation unroll (csrc/v2m_adjoint.cu)
+behind torch.autograd.Function (trussnet_b200/adjoint.py).
+
+Checks, on the taped function (active bars recorded by the GPU forward pass and
+replayed by every evaluation):
+  * the loss and the gradients w.r.t. the node positions and the sizing grid
+    against the FP64 reverse-mode gradient (oracle/v2m_unroll_oracle.c):
+    relative error (2-norm) <= 1e-4;
+  * directional derivatives against FP64 central finite differences with
+    eps = 1e-3: relative error <= 1e-4;
+  * run-to-run bit-identical gradients (fixed-point accumulation);
+  * the adjoint costs <= 3x a forward step (backward time / K against
+    forward time / K, both CUDA-event timed).
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import unroll_forward_f64, unroll_grad_f64
+from trussnet_b200 import Session, synth
+from trussnet_b200.types import RelaxParams
+
+pytestmark = pytest.mark.gpu
+
+FSCALE, FSURF, DT = 1.2, 1.0, 0.2
+
+
+def setup(dim, m, K, ckpt, density=1.66, seed=0):
+    import torch
+    from trussnet_b200.adjoint import Unroll
+    g, nd, G, cs = synth.ellipsoids_adjoint(dim=dim, m=m, density=density, seed=seed)
+    with Session(g, RelaxParams(max_iters=1), nd) as s:
+        s.rebuild()
+        nbr, nnb = s.read("nbr"), s.read("nnb")
+    u = Unroll(nbr, nnb, nd.typ, G.shape[::-1], cs, FSCALE, FSURF, DT, K, ckpt)
+    x0 = torch.tensor(nd.P, device="cuda")
+    Gt = torch.tensor(G, device="cuda")
+    return u, x0, Gt, nd, nbr, nnb, G, cs
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.mark.parametrize("cfg", [(48, 16, 12, 5), (128, 64, 50, 10)], ids=["small", "ellipsoids128_K50"])
+def test_adjoint_against_fp64_and_fd(cfg, cuda_lib, record_property):
+    dim, m, K, ckpt = cfg
+    u, x0, Gt, nd, nbr, nnb, G, cs = setup(dim, m, K, ckpt)
+    xK = u.forward(x0, Gt)
+    loss = u.loss(xK, Gt)
+    gxK, gG1 = u.loss_backward(xK, Gt)
+    gx0, gG2 = u.backward(Gt, gxK)
+    gx0 = gx0.cpu().numpy().astype(np.float64)
+    gG = (gG1 + gG2).cpu().numpy().astype(np.float64)
+    tape = u.tape()
+    args = (nbr, nnb, nd.typ, G.astype(np.float64), cs, FSCALE, FSURF, DT, K)
+    L64, gx64, gG64, _ = unroll_grad_f64(*args, nd.P.astype(np.float64), tape)
+    e_loss = abs(loss - L64) / abs(L64)
+    e_x, e_G = rel(gx0, gx64), rel(gG, gG64)
+    record_property("loss_rel_err", e_loss)
+    record_property("grad_x_rel_err_vs_fp64", e_x)
+    record_property("grad_G_rel_err_vs_fp64", e_G)
+    assert e_loss <= 1e-4 and e_x <= 1e-4 and e_G <= 1e-4, (e_loss, e_x, e_G)
+    # central finite differences (FP64, the same tape), eps = 1e-3
+    rng = np.random.default_rng(1)
+    eps = 1e-3
+    worst = 0.0
+    for _ in range(3):
+        d = rng.standard_normal(nd.P.shape)
+        d /= np.linalg.norm(d)
+        lp = unroll_forward_f64(*args, nd.P.astype(np.float64) + eps * d, tape)[1]
+        lm = unroll_forward_f64(*args, nd.P.astype(np.float64) - eps * d, tape)[1]
+        fd = (lp - lm) / (2 * eps)
+        an = float(np.sum(gx0 * d))
+        worst = max(worst, abs(fd - an) / max(abs(fd), 1e-12))
+        dG = rng.standard_normal(G.shape)
+        dG /= np.linalg.norm(dG)
+        lp = unroll_forward_f64(nbr, nnb, nd.typ, G.astype(np.float64) + eps * dG, cs, FSCALE, FSURF, DT, K,
+                                nd.P.astype(np.float64), tape)[1]
+        lm = unroll_forward_f64(nbr, nnb, nd.typ, G.astype(np.float64) - eps * dG, cs, FSCALE, FSURF, DT, K,
+                                nd.P.astype(np.float64), tape)[1]
+        fd = (lp - lm) / (2 * eps)
+        an = float(np.sum(gG * dG))
+        worst = max(worst, abs(fd - an) / max(abs(fd), 1e-12))
+    record_property("fd_rel_err", worst)
+    assert worst <= 1e-4, worst
+
+
+def test_adjoint_deterministic_and_cost(cuda_lib, record_property):
+    u, x0, Gt, *_ = setup(128, 64, 50, 10)
+    outs = []
+    for _ in range(2):
+        xK = u.forward(x0, Gt)
+        gxK, _ = u.loss_backward(xK, Gt)
+        gx0, gG = u.backward(Gt, gxK)
+        outs.append((gx0.cpu().numpy(), gG.cpu().numpy()))
+    assert np.array_equal(outs[0][0].view(np.uint32), outs[1][0].view(np.uint32))
+    assert np.array_equal(outs[0][1].view(np.uint32), outs[1][1].view(np.uint32))
+    # timing: warm runs
+    for _ in range(3):
+        xK = u.forward(x0, Gt)
+        gxK, _ = u.loss_backward(xK, Gt)
+        u.backward(Gt, gxK)
+    fwd, bwd = u.timing()
+    ratio = bwd / fwd
+    record_property("forward_ms_per_step", fwd / 50)
+    record_property("adjoint_ms_per_step", bwd / 50)
+    record_property("adjoint_over_forward", ratio)
+    assert ratio <= 3.0, ratio
+
+
+def test_autograd_function(cuda_lib):
+    import torch
+    from trussnet_b200.adjoint import unrolled_loss
+    u, x0, Gt, *_ = setup(48, 16, 12, 5)
+    x = x0.clone().requires_grad_(True)
+    G = Gt.clone().requires_grad_(True)
+    L = unrolled_loss(x, G, u)
+    L.backward()
+    xK = u.forward(x0, Gt)
+    gxK, gG1 = u.loss_backward(xK, Gt)
+    gx0, gG2 = u.backward(Gt, gxK)
+    assert torch.equal(x.grad, gx0)
+    assert torch.allclose(G.grad, gG1 + gG2, rtol=0, atol=0)
+    assert float(L) == pytest.approx(u.loss(xK, Gt), rel=0, abs=0)

@@ -23,7 +23,9 @@ EXPORTS = [
     "v2m_session_force", "v2m_session_step_tail", "v2m_session_iterate", "v2m_session_run", "v2m_session_synchronize",
     "v2m_session_read_nodes", "v2m_session_stats", "v2m_session_read_array", "v2m_session_write_array",
     "v2m_session_write_lists", "v2m_session_info", "v2m_session_counters", "v2m_session_timed_runs",
-    "v2m_session_clear_counters",
+    "v2m_session_clear_counters", "v2m_unroll_create", "v2m_unroll_destroy", "v2m_unroll_forward",
+    "v2m_unroll_loss", "v2m_unroll_loss_backward", "v2m_unroll_backward", "v2m_unroll_tape", "v2m_unroll_timing",
+    "v2m_unroll_last_error", "v2m_session_autotune", "v2m_session_shapes",
 ]
 
 _lock = threading.Lock()
@@ -69,6 +71,18 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.v2m_session_counters.argtypes = [vp, P(C.c_int64), P(C.c_int64), P(C.c_double)]
         L.v2m_session_timed_runs.argtypes = [vp, C.c_int, C.c_int, C.c_int, P(C.c_float)]
         L.v2m_session_clear_counters.argtypes = [vp]
+        L.v2m_unroll_last_error.restype = C.c_char_p
+        L.v2m_session_autotune.argtypes = [vp, C.c_int, C.c_char_p, C.c_int64]
+        L.v2m_session_shapes.argtypes = [vp, P(C.c_int32), P(C.c_int32)]
+        L.v2m_unroll_create.argtypes = [C.c_int64, vp, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_int,
+                                        C.c_int, C.c_int, P(vp)]
+        L.v2m_unroll_destroy.argtypes = [vp]
+        L.v2m_unroll_forward.argtypes = [vp, vp, vp, vp, C.c_int]
+        L.v2m_unroll_loss.argtypes = [vp, vp, vp, P(C.c_double)]
+        L.v2m_unroll_loss_backward.argtypes = [vp, vp, vp, C.c_float, vp, vp, C.c_int]
+        L.v2m_unroll_backward.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.v2m_unroll_tape.argtypes = [vp, vp, C.c_int64]
+        L.v2m_unroll_timing.argtypes = [vp, P(C.c_float), P(C.c_float)]
         _lib = L
         return L
 
@@ -76,4 +90,10 @@ def load(path: str = LIB_PATH) -> C.CDLL:
 def check(rc: int) -> None:
     if rc != V2M_OK:
         msg = load().v2m_cuda_last_error().decode(errors="replace")
+        raise V2mError(rc, msg)
+
+
+def check_unroll(rc: int) -> None:
+    if rc != V2M_OK:
+        msg = load().v2m_unroll_last_error().decode(errors="replace")
         raise V2mError(rc, msg)

@@ -1,0 +1,683 @@
+// v2m_adjoint.cu -- the differentiable relaxation unroll and its hand-written
+// adjoint, for sm_100a.
+//
+// The unroll is the relaxation step (v2m_force + the Jacobi branch of
+// v2m_move, src/opencl/v2m_particle_body.cl:161-184, 898-900 of
+// fangq/trussnet) with its discrete decisions frozen:
+//   h_i  = H(x_i), trilinear in the sizing grid G (m0 x m1 x m2 values at
+//          x = (a cs0, b cs1, c cs2), x fastest), the point clamped to G's box;
+//   the lists are fixed (one list build before the unroll);
+//   the active bars of every step are recorded on a tape (24-bit mask per node
+//          and step) by the forward pass and replayed by the backward pass, so
+//          the stiffness c_i = popcount(mask) is frozen (its jumps would make the
+//          step discontinuous);
+//   x_i' = x_i + dt sum_k f_k (x_i - x_j) / max(c_i, 1), f = (l0 - l) / l,
+//          l0 = a_ij (h_i + h_j), a_ij = fsurf/2 (both non-INTERIOR) or fscale/2;
+//          CORNER nodes stay.
+// Loss: sum over every list entry (i, j) of (l_ij / hm_ij - 1)^2, hm = (h_i+h_j)/2.
+//
+// Reverse mode with checkpoints every `ckpt` steps: the backward pass recomputes
+// each segment's states from its checkpoint, then walks it backwards. Gradient
+// contributions that scatter (to a neighbour j, to the 8 corners of G) are
+// added as 64-bit fixed point (2^-32) with integer atomics, which are exact
+// and associative: the gradients are bit-identical run to run.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/v2m_cuda.h"
+
+namespace v2m_adj {
+
+constexpr double kFix = 4294967296.0;   // 2^32
+constexpr int kT = 256;
+
+struct Dims {
+    int m0, m1, m2;
+    float cs0, cs1, cs2;
+};
+
+__device__ __forceinline__ void fx_add(unsigned long long* a, double v) {
+    const long long q = __double2ll_rn(v * kFix);
+    atomicAdd(a, (unsigned long long)q);
+}
+
+__device__ __forceinline__ double fx_get(unsigned long long a) {
+    return (double)(long long)a / kFix;
+}
+
+// h at p, optionally its gradient, the 8 corner ids and weights
+__device__ __forceinline__ float size_at(const Dims& D, const float* __restrict__ G, float px, float py, float pz,
+                                         float* grad, int* idx, float* w) {
+    const float ms[3] = { (float)(D.m0 - 1), (float)(D.m1 - 1), (float)(D.m2 - 1) };
+    const float cs[3] = { D.cs0, D.cs1, D.cs2 };
+    const int mm[3] = { D.m0, D.m1, D.m2 };
+    const float p[3] = { px, py, pz };
+    float f[3];
+    int i0[3], inside[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        float v = p[d] / cs[d];
+        inside[d] = v > 0.0f && v < ms[d];
+        v = fminf(fmaxf(v, 0.0f), ms[d]);
+        int a = (int)floorf(v);
+        if (a > mm[d] - 2) {
+            a = mm[d] > 1 ? mm[d] - 2 : 0;
+        }
+        i0[d] = a;
+        f[d] = v - (float)a;
+    }
+    float c[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        int a = min(i0[0] + (k & 1), D.m0 - 1), b = min(i0[1] + ((k >> 1) & 1), D.m1 - 1),
+            cc = min(i0[2] + (k >> 2), D.m2 - 1);
+        const int id = a + D.m0 * (b + D.m1 * cc);
+        c[k] = __ldg(G + id);
+        if (idx) {
+            idx[k] = id;
+        }
+    }
+    float h = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const float wk = ((k & 1) ? f[0] : 1.0f - f[0]) * (((k >> 1) & 1) ? f[1] : 1.0f - f[1]) *
+                         ((k >> 2) ? f[2] : 1.0f - f[2]);
+        if (w) {
+            w[k] = wk;
+        }
+        h += wk * c[k];
+    }
+    if (grad) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            float g = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                float prod = ((k >> d) & 1) ? 1.0f : -1.0f;
+#pragma unroll
+                for (int e = 0; e < 3; ++e) {
+                    if (e != d) {
+                        prod *= ((k >> e) & 1) ? f[e] : 1.0f - f[e];
+                    }
+                }
+                g += prod * c[k];
+            }
+            grad[d] = inside[d] ? g / cs[d] : 0.0f;
+        }
+    }
+    return h;
+}
+
+__global__ void k_pack(const float* __restrict__ x3, float4* __restrict__ x4, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        x4[i] = make_float4(x3[3 * i], x3[3 * i + 1], x3[3 * i + 2], 0.0f);
+    }
+}
+
+__global__ void k_unpack(const float4* __restrict__ x4, float* __restrict__ x3, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const float4 p = x4[i];
+        x3[3 * i] = p.x;
+        x3[3 * i + 1] = p.y;
+        x3[3 * i + 2] = p.z;
+    }
+}
+
+__global__ void k_size(Dims D, const float* __restrict__ G, const float4* __restrict__ x, float* __restrict__ h, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const float4 p = x[i];
+        h[i] = size_at(D, G, p.x, p.y, p.z, nullptr, nullptr, nullptr);
+    }
+}
+
+// one step; records (replay = 0) or replays the active-bar masks
+__global__ void k_step(const float4* __restrict__ x, const float* __restrict__ h, const int* __restrict__ nbr,
+                       const uint8_t* __restrict__ nnb, const uint8_t* __restrict__ typ, float fscale, float fsurf,
+                       float dt, uint32_t* __restrict__ mask, int replay, float4* __restrict__ y, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const float4 p = x[i];
+    const int ti = typ[i];
+    if (ti == V2M_CORNER) {
+        y[i] = p;
+        if (!replay) {
+            mask[i] = 0u;
+        }
+        return;
+    }
+    const float hi = h[i];
+    const int c = nnb[i];
+    uint32_t bits = replay ? mask[i] : 0u;
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+    int act = 0;
+    for (int k = 0; k < c; ++k) {
+        const int j = __ldg(nbr + (size_t)k * n + i);
+        const float4 q = __ldg(x + j);
+        const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
+        const float l = sqrtf(ex * ex + ey * ey + ez * ez);
+        const float a = ((ti != V2M_INTERIOR && typ[j] != V2M_INTERIOR) ? fsurf : fscale) * 0.5f;
+        const float l0 = a * (hi + __ldg(h + j));
+        const bool on = replay ? ((bits >> k) & 1u) != 0u : (l < l0 && l > 0.0f);
+        if (!on) {
+            continue;
+        }
+        if (!replay) {
+            bits |= 1u << k;
+        }
+        const float f = (l0 - l) / l;
+        fx += f * ex;
+        fy += f * ey;
+        fz += f * ez;
+        ++act;
+    }
+    if (!replay) {
+        mask[i] = bits;
+    }
+    const float s = dt / (float)(act > 1 ? act : 1);
+    y[i] = make_float4(p.x + s * fx, p.y + s * fy, p.z + s * fz, 0.0f);
+}
+
+__global__ void k_loss(const float4* __restrict__ x, const float* __restrict__ h, const int* __restrict__ nbr,
+                       const uint8_t* __restrict__ nnb, double* __restrict__ part, int n) {
+    __shared__ double red[kT / 32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double s = 0.0;
+    if (i < n) {
+        const float4 p = x[i];
+        const float hi = h[i];
+        for (int k = 0; k < nnb[i]; ++k) {
+            const int j = __ldg(nbr + (size_t)k * n + i);
+            const float4 q = __ldg(x + j);
+            const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
+            const float l = sqrtf(ex * ex + ey * ey + ez * ez);
+            const float r = l / (0.5f * (hi + __ldg(h + j))) - 1.0f;
+            s += (double)r * (double)r;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[threadIdx.x >> 5] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kT / 32; ++w) {
+            t += red[w];
+        }
+        part[blockIdx.x] = t;
+    }
+}
+
+__global__ void k_loss_bwd(const float4* __restrict__ x, const float* __restrict__ h, const int* __restrict__ nbr,
+                           const uint8_t* __restrict__ nnb, float gscale, unsigned long long* __restrict__ lam,
+                           unsigned long long* __restrict__ gh, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const float4 p = x[i];
+    const float hi = h[i];
+    double li[3] = { 0.0, 0.0, 0.0 }, ghi = 0.0;
+    for (int k = 0; k < nnb[i]; ++k) {
+        const int j = __ldg(nbr + (size_t)k * n + i);
+        const float4 q = __ldg(x + j);
+        const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
+        const float l = sqrtf(ex * ex + ey * ey + ez * ez);
+        const float hm = 0.5f * (hi + __ldg(h + j));
+        const float r = l / hm - 1.0f;
+        const float dl = gscale * 2.0f * r / hm, dhm = -gscale * 2.0f * r * l / (hm * hm);
+        const float e[3] = { ex / l, ey / l, ez / l };
+        for (int d = 0; d < 3; ++d) {
+            li[d] += (double)(dl * e[d]);
+            fx_add(lam + 3 * (size_t)j + d, -(double)(dl * e[d]));
+        }
+        ghi += 0.5 * (double)dhm;
+        fx_add(gh + j, 0.5 * (double)dhm);
+    }
+    for (int d = 0; d < 3; ++d) {
+        fx_add(lam + 3 * (size_t)i + d, li[d]);
+    }
+    fx_add(gh + i, ghi);
+}
+
+// reverse of one step: lam_in = dL/dx_{t+1}; accumulates dL/dx_t and dL/dh_t
+__global__ void k_step_bwd(const float4* __restrict__ x, const float* __restrict__ h, const int* __restrict__ nbr,
+                           const uint8_t* __restrict__ nnb, const uint8_t* __restrict__ typ, float fscale, float fsurf,
+                           float dt, const uint32_t* __restrict__ mask, const float4* __restrict__ lam_in,
+                           unsigned long long* __restrict__ lam, unsigned long long* __restrict__ gh, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const float4 li4 = lam_in[i];
+    double li[3] = { (double)li4.x, (double)li4.y, (double)li4.z }, ghi = 0.0;
+    const int ti = typ[i];
+    if (ti != V2M_CORNER) {
+        const float4 p = x[i];
+        const float hi = h[i];
+        const uint32_t bits = mask[i];
+        const int act = __popc(bits);
+        const float s = dt / (float)(act > 1 ? act : 1);
+        const float mu[3] = { s * li4.x, s * li4.y, s * li4.z };
+        for (int k = 0; k < nnb[i]; ++k) {
+            if (!((bits >> k) & 1u)) {
+                continue;
+            }
+            const int j = __ldg(nbr + (size_t)k * n + i);
+            const float4 q = __ldg(x + j);
+            const float e[3] = { p.x - q.x, p.y - q.y, p.z - q.z };
+            const float l = sqrtf(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+            const float a = ((ti != V2M_INTERIOR && typ[j] != V2M_INTERIOR) ? fsurf : fscale) * 0.5f;
+            const float l0 = a * (hi + __ldg(h + j));
+            const float f = (l0 - l) / l, dfl = -l0 / (l * l);
+            const float em = e[0] * mu[0] + e[1] * mu[1] + e[2] * mu[2];
+            for (int d = 0; d < 3; ++d) {
+                const float v = f * mu[d] + e[d] / l * dfl * em;
+                li[d] += (double)v;
+                fx_add(lam + 3 * (size_t)j + d, -(double)v);
+            }
+            const double sa = (double)(a * (em / l));
+            ghi += sa;
+            fx_add(gh + j, sa);
+        }
+    }
+    for (int d = 0; d < 3; ++d) {
+        fx_add(lam + 3 * (size_t)i + d, li[d]);
+    }
+    fx_add(gh + i, ghi);
+}
+
+// dL/dh into dL/dx (own) and dL/dG (8 corners), then the float adjoint, buffers cleared
+__global__ void k_size_bwd(Dims D, const float* __restrict__ G, const float4* __restrict__ x,
+                           unsigned long long* __restrict__ gh, unsigned long long* __restrict__ lam,
+                           unsigned long long* __restrict__ gG, float4* __restrict__ lam_out, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const double g = fx_get(gh[i]);
+    gh[i] = 0ull;
+    double l3[3] = { fx_get(lam[3 * (size_t)i]), fx_get(lam[3 * (size_t)i + 1]), fx_get(lam[3 * (size_t)i + 2]) };
+    lam[3 * (size_t)i] = lam[3 * (size_t)i + 1] = lam[3 * (size_t)i + 2] = 0ull;
+    if (g != 0.0) {
+        const float4 p = x[i];
+        float gr[3], w[8];
+        int idx[8];
+        size_at(D, G, p.x, p.y, p.z, gr, idx, w);
+        for (int d = 0; d < 3; ++d) {
+            l3[d] += g * (double)gr[d];
+        }
+        for (int k = 0; k < 8; ++k) {
+            fx_add(gG + idx[k], g * (double)w[k]);
+        }
+    }
+    lam_out[i] = make_float4((float)l3[0], (float)l3[1], (float)l3[2], 0.0f);
+}
+
+__global__ void k_fix_to_float(unsigned long long* __restrict__ a, float* __restrict__ out, int m, int clear) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) {
+        out[i] = (float)fx_get(a[i]);
+        if (clear) {
+            a[i] = 0ull;
+        }
+    }
+}
+
+__global__ void k_lists(const int* __restrict__ rowmajor, const int* __restrict__ cnt, int* __restrict__ slot,
+                        uint8_t* __restrict__ nnb, int n) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * V2M_K) {
+        return;
+    }
+    const int i = t / V2M_K, k = t % V2M_K;
+    const int c = cnt[i];
+    slot[(size_t)k * n + i] = k < c ? rowmajor[t] : i;
+    if (k == 0) {
+        nnb[i] = (uint8_t)c;
+    }
+}
+
+}  // namespace v2m_adj
+
+using namespace v2m_adj;
+
+struct v2m_unroll {
+    int device = 0, n = 0, K = 0, ckpt = 10, nck = 0;
+    Dims D{};
+    float fscale = 1.2f, fsurf = 1.0f, dt = 0.2f;
+    cudaStream_t stream = nullptr;
+    int* nbr = nullptr;
+    uint8_t* nnb = nullptr;
+    uint8_t* typ = nullptr;
+    uint32_t* tape = nullptr;        // K x n
+    float4* ck = nullptr;            // nck checkpoints x n
+    float4* seg = nullptr;           // (ckpt + 1) x n segment states
+    float* h = nullptr;
+    float4* lamf = nullptr;
+    unsigned long long* lam = nullptr;
+    unsigned long long* gh = nullptr;
+    unsigned long long* gG = nullptr;
+    double* part = nullptr;
+    int have_tape = 0;
+    float ms_fwd = 0.0f, ms_bwd = 0.0f;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::vector<void*> allocs;
+    template <typename T>
+    T* alloc(size_t count) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, std::max<size_t>(count * sizeof(T), 16)) != cudaSuccess) {
+            throw std::runtime_error("cudaMalloc failed");
+        }
+        allocs.push_back(p);
+        return (T*)p;
+    }
+    ~v2m_unroll() {
+        for (void* p : allocs) {
+            cudaFree(p);
+        }
+        if (e0) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+        }
+        if (stream) {
+            cudaStreamDestroy(stream);
+        }
+    }
+};
+
+namespace {
+
+thread_local std::string g_uerr;
+
+void uck(cudaError_t e, const char* where) {
+    if (e != cudaSuccess) {
+        throw std::runtime_error(std::string(where) + ": CUDA error " + std::to_string((int)e) + " (" +
+                                 cudaGetErrorString(e) + ")");
+    }
+}
+
+template <typename F>
+int uguard(F&& f) {
+    try {
+        f();
+        return V2M_OK;
+    } catch (const std::invalid_argument& e) {
+        g_uerr = e.what();
+        return V2M_ERR_ARG;
+    } catch (const std::exception& e) {
+        g_uerr = e.what();
+        return V2M_ERR_CUDA;
+    }
+}
+
+unsigned blocks(int n) {
+    return (unsigned)((n + kT - 1) / kT);
+}
+
+// forward over steps [t0, t1) from x (float4), writing states to out[t - t0 + 1]
+// (out may be null: only the last state is kept in `last`)
+void run_steps(v2m_unroll* u, const float* G, const float4* x, int t0, int t1, float4* seg, int replay) {
+    const int n = u->n;
+    const float4* cur = x;
+    for (int t = t0; t < t1; ++t) {
+        float4* nxt = seg + (size_t)(t - t0 + 1) * n;
+        k_size<<<blocks(n), kT, 0, u->stream>>>(u->D, G, cur, u->h, n);
+        k_step<<<blocks(n), kT, 0, u->stream>>>(cur, u->h, u->nbr, u->nnb, u->typ, u->fscale, u->fsurf, u->dt,
+                                                u->tape + (size_t)t * n, replay, nxt, n);
+        cur = nxt;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* v2m_unroll_last_error(void) {
+    return g_uerr.c_str();
+}
+
+int v2m_unroll_create(int64_t n, const int32_t* nbr, const int32_t* nnb, const uint8_t* typ, const int32_t* m,
+                      const float* cs, float fscale, float fsurf, float dt, int K, int ckpt, int device,
+                      v2m_unroll** out) {
+    return uguard([&] {
+        if (!out || n < 1 || n > (1 << 30) || !nbr || !nnb || !typ || !m || !cs || K < 1 || ckpt < 1) {
+            throw std::invalid_argument("bad argument");
+        }
+        if (m[0] < 1 || m[1] < 1 || m[2] < 1 || !(cs[0] > 0 && cs[1] > 0 && cs[2] > 0)) {
+            throw std::invalid_argument("bad sizing grid");
+        }
+        for (int64_t i = 0; i < n; ++i) {
+            if (nnb[i] < 0 || nnb[i] > V2M_K || typ[i] > V2M_CORNER) {
+                throw std::invalid_argument("list length or type out of range");
+            }
+            for (int k = 0; k < nnb[i]; ++k) {
+                if (nbr[i * V2M_K + k] < 0 || nbr[i * V2M_K + k] >= n) {
+                    throw std::invalid_argument("neighbour id out of range");
+                }
+            }
+        }
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+            cudaGetLastError();
+            throw std::runtime_error("no CUDA device available");
+        }
+        const int dev = device < 0 ? 0 : device;
+        uck(cudaSetDevice(dev), "cudaSetDevice");
+        v2m_unroll* u = new v2m_unroll();
+        try {
+            u->device = dev;
+            u->n = (int)n;
+            u->K = K;
+            u->ckpt = ckpt;
+            u->nck = (K + ckpt - 1) / ckpt;
+            u->D = Dims{ m[0], m[1], m[2], cs[0], cs[1], cs[2] };
+            u->fscale = fscale;
+            u->fsurf = fsurf;
+            u->dt = dt;
+            uck(cudaStreamCreateWithFlags(&u->stream, cudaStreamNonBlocking), "stream");
+            uck(cudaEventCreate(&u->e0), "event");
+            uck(cudaEventCreate(&u->e1), "event");
+            const size_t nn = (size_t)n;
+            u->nbr = u->alloc<int>(nn * V2M_K);
+            u->nnb = u->alloc<uint8_t>(nn);
+            u->typ = u->alloc<uint8_t>(nn);
+            u->tape = u->alloc<uint32_t>(nn * K);
+            u->ck = u->alloc<float4>(nn * u->nck);
+            u->seg = u->alloc<float4>(nn * (ckpt + 1));
+            u->h = u->alloc<float>(nn);
+            u->lamf = u->alloc<float4>(nn);
+            u->lam = u->alloc<unsigned long long>(3 * nn);
+            u->gh = u->alloc<unsigned long long>(nn);
+            u->gG = u->alloc<unsigned long long>((size_t)m[0] * m[1] * m[2]);
+            u->part = u->alloc<double>(nn / kT + 1);
+            int* tmp = u->alloc<int>(nn * V2M_K + nn);
+            uck(cudaMemcpyAsync(tmp, nbr, 4 * nn * V2M_K, cudaMemcpyHostToDevice, u->stream), "upload");
+            uck(cudaMemcpyAsync(tmp + nn * V2M_K, nnb, 4 * nn, cudaMemcpyHostToDevice, u->stream), "upload");
+            uck(cudaMemcpyAsync(u->typ, typ, nn, cudaMemcpyHostToDevice, u->stream), "upload");
+            k_lists<<<(unsigned)((nn * V2M_K + kT - 1) / kT), kT, 0, u->stream>>>(tmp, tmp + nn * V2M_K, u->nbr, u->nnb,
+                                                                               (int)n);
+            uck(cudaMemsetAsync(u->lam, 0, 8 * 3 * nn, u->stream), "memset");
+            uck(cudaMemsetAsync(u->gh, 0, 8 * nn, u->stream), "memset");
+            uck(cudaMemsetAsync(u->gG, 0, 8 * (size_t)m[0] * m[1] * m[2], u->stream), "memset");
+            uck(cudaGetLastError(), "launch");
+            uck(cudaStreamSynchronize(u->stream), "synchronize");
+        } catch (...) {
+            delete u;
+            throw;
+        }
+        *out = u;
+    });
+}
+
+int v2m_unroll_destroy(v2m_unroll* u) {
+    return uguard([&] {
+        if (u) {
+            cudaSetDevice(u->device);
+            cudaStreamSynchronize(u->stream);
+            delete u;
+        }
+    });
+}
+
+int v2m_unroll_forward(v2m_unroll* u, const float* x0, const float* G, float* xK, int replay) {
+    return uguard([&] {
+        if (!u || !x0 || !G || !xK) {
+            throw std::invalid_argument("bad argument");
+        }
+        if (replay && !u->have_tape) {
+            throw std::invalid_argument("no tape recorded yet");
+        }
+        uck(cudaSetDevice(u->device), "cudaSetDevice");
+        const int n = u->n;
+        uck(cudaEventRecord(u->e0, u->stream), "event");
+        k_pack<<<blocks(n), kT, 0, u->stream>>>(x0, u->seg, n);
+        for (int c = 0; c < u->nck; ++c) {
+            const int t0 = c * u->ckpt, t1 = std::min(u->K, t0 + u->ckpt);
+            uck(cudaMemcpyAsync(u->ck + (size_t)c * n, u->seg, 16 * (size_t)n, cudaMemcpyDeviceToDevice, u->stream),
+                "checkpoint");
+            run_steps(u, G, u->ck + (size_t)c * n, t0, t1, u->seg, replay);
+            uck(cudaMemcpyAsync(u->seg, u->seg + (size_t)(t1 - t0) * n, 16 * (size_t)n, cudaMemcpyDeviceToDevice,
+                                u->stream), "segment");
+        }
+        k_unpack<<<blocks(n), kT, 0, u->stream>>>(u->seg, xK, n);
+        uck(cudaEventRecord(u->e1, u->stream), "event");
+        uck(cudaGetLastError(), "launch");
+        uck(cudaStreamSynchronize(u->stream), "synchronize");
+        uck(cudaEventElapsedTime(&u->ms_fwd, u->e0, u->e1), "elapsed");
+        u->have_tape = 1;
+    });
+}
+
+int v2m_unroll_loss(v2m_unroll* u, const float* x, const float* G, double* loss) {
+    return uguard([&] {
+        if (!u || !x || !G || !loss) {
+            throw std::invalid_argument("bad argument");
+        }
+        uck(cudaSetDevice(u->device), "cudaSetDevice");
+        const int n = u->n;
+        float4* x4 = u->lamf;   // scratch
+        k_pack<<<blocks(n), kT, 0, u->stream>>>(x, x4, n);
+        k_size<<<blocks(n), kT, 0, u->stream>>>(u->D, G, x4, u->h, n);
+        k_loss<<<blocks(n), kT, 0, u->stream>>>(x4, u->h, u->nbr, u->nnb, u->part, n);
+        std::vector<double> part(blocks(n));
+        uck(cudaMemcpyAsync(part.data(), u->part, 8 * part.size(), cudaMemcpyDeviceToHost, u->stream), "read");
+        uck(cudaStreamSynchronize(u->stream), "synchronize");
+        double s = 0.0;
+        for (double p : part) {
+            s += p;
+        }
+        *loss = s;
+    });
+}
+
+// gx = gscale * dLoss/dx at x; gG += gscale * dLoss/dG (gG overwritten when accumulate == 0)
+int v2m_unroll_loss_backward(v2m_unroll* u, const float* x, const float* G, float gscale, float* gx, float* gG,
+                             int accumulate) {
+    return uguard([&] {
+        if (!u || !x || !G || !gx || !gG) {
+            throw std::invalid_argument("bad argument");
+        }
+        uck(cudaSetDevice(u->device), "cudaSetDevice");
+        const int n = u->n, mg = u->D.m0 * u->D.m1 * u->D.m2;
+        float4* x4 = u->seg;
+        k_pack<<<blocks(n), kT, 0, u->stream>>>(x, x4, n);
+        k_size<<<blocks(n), kT, 0, u->stream>>>(u->D, G, x4, u->h, n);
+        if (!accumulate) {
+            uck(cudaMemsetAsync(u->gG, 0, 8 * (size_t)mg, u->stream), "memset");
+        }
+        k_loss_bwd<<<blocks(n), kT, 0, u->stream>>>(x4, u->h, u->nbr, u->nnb, gscale, u->lam, u->gh, n);
+        k_size_bwd<<<blocks(n), kT, 0, u->stream>>>(u->D, G, x4, u->gh, u->lam, u->gG, u->lamf, n);
+        k_unpack<<<blocks(n), kT, 0, u->stream>>>(u->lamf, gx, n);
+        k_fix_to_float<<<blocks(mg), kT, 0, u->stream>>>(u->gG, gG, mg, 0);
+        uck(cudaGetLastError(), "launch");
+        uck(cudaStreamSynchronize(u->stream), "synchronize");
+    });
+}
+
+// reverse of the last forward pass: gxK = dL/dxK in, gx0 = dL/dx0 out,
+// gG (overwritten) = dL/dG through the steps, plus gG_in (may be null) from other terms
+int v2m_unroll_backward(v2m_unroll* u, const float* G, const float* gxK, float* gx0, float* gG, const float* gG_in) {
+    return uguard([&] {
+        if (!u || !G || !gxK || !gx0 || !gG) {
+            throw std::invalid_argument("bad argument");
+        }
+        if (!u->have_tape) {
+            throw std::invalid_argument("backward before forward");
+        }
+        uck(cudaSetDevice(u->device), "cudaSetDevice");
+        const int n = u->n, mg = u->D.m0 * u->D.m1 * u->D.m2;
+        uck(cudaEventRecord(u->e0, u->stream), "event");
+        uck(cudaMemsetAsync(u->gG, 0, 8 * (size_t)mg, u->stream), "memset");
+        k_pack<<<blocks(n), kT, 0, u->stream>>>(gxK, u->lamf, n);
+        for (int c = u->nck - 1; c >= 0; --c) {
+            const int t0 = c * u->ckpt, t1 = std::min(u->K, t0 + u->ckpt);
+            // recompute the segment's states from its checkpoint (replaying the tape)
+            uck(cudaMemcpyAsync(u->seg, u->ck + (size_t)c * n, 16 * (size_t)n, cudaMemcpyDeviceToDevice, u->stream),
+                "segment");
+            run_steps(u, G, u->seg, t0, t1 - 1, u->seg, 1);
+            for (int t = t1 - 1; t >= t0; --t) {
+                const float4* xt = u->seg + (size_t)(t - t0) * n;
+                k_size<<<blocks(n), kT, 0, u->stream>>>(u->D, G, xt, u->h, n);
+                k_step_bwd<<<blocks(n), kT, 0, u->stream>>>(xt, u->h, u->nbr, u->nnb, u->typ, u->fscale, u->fsurf,
+                                                            u->dt, u->tape + (size_t)t * n, u->lamf, u->lam, u->gh, n);
+                k_size_bwd<<<blocks(n), kT, 0, u->stream>>>(u->D, G, xt, u->gh, u->lam, u->gG, u->lamf, n);
+            }
+        }
+        k_unpack<<<blocks(n), kT, 0, u->stream>>>(u->lamf, gx0, n);
+        k_fix_to_float<<<blocks(mg), kT, 0, u->stream>>>(u->gG, gG, mg, 1);
+        uck(cudaEventRecord(u->e1, u->stream), "event");
+        uck(cudaGetLastError(), "launch");
+        uck(cudaStreamSynchronize(u->stream), "synchronize");
+        uck(cudaEventElapsedTime(&u->ms_bwd, u->e0, u->e1), "elapsed");
+        if (gG_in) {
+            std::vector<float> a(mg), b(mg);
+            uck(cudaMemcpy(a.data(), gG, 4 * (size_t)mg, cudaMemcpyDeviceToHost), "read");
+            uck(cudaMemcpy(b.data(), gG_in, 4 * (size_t)mg, cudaMemcpyDeviceToHost), "read");
+            for (int i = 0; i < mg; ++i) {
+                a[i] += b[i];
+            }
+            uck(cudaMemcpy(gG, a.data(), 4 * (size_t)mg, cudaMemcpyHostToDevice), "write");
+        }
+    });
+}
+
+int v2m_unroll_tape(v2m_unroll* u, uint32_t* host, int64_t count) {
+    return uguard([&] {
+        if (!u || !host || count < (int64_t)u->n * u->K) {
+            throw std::invalid_argument("bad argument");
+        }
+        uck(cudaSetDevice(u->device), "cudaSetDevice");
+        uck(cudaMemcpy(host, u->tape, 4 * (size_t)u->n * u->K, cudaMemcpyDeviceToHost), "read tape");
+    });
+}
+
+// device milliseconds of the last forward (all K steps) and backward passes
+int v2m_unroll_timing(v2m_unroll* u, float* ms_forward, float* ms_backward) {
+    return uguard([&] {
+        if (!u) {
+            throw std::invalid_argument("bad argument");
+        }
+        if (ms_forward) {
+            *ms_forward = u->ms_fwd;
+        }
+        if (ms_backward) {
+            *ms_backward = u->ms_bwd;
+        }
+    });
+}
+
+}  // extern "C"

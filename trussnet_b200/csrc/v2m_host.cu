@@ -16,7 +16,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <mutex>
+#include <sys/stat.h>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -50,6 +52,14 @@ int64_t align_up(int64_t x, int64_t a) {
     return (x + a - 1) / a * a;
 }
 
+void mkdir_p(const std::string& dir) {
+    for (size_t i = 1; i <= dir.size(); ++i) {
+        if (i == dir.size() || dir[i] == '/') {
+            mkdir(dir.substr(0, i).c_str(), 0755);
+        }
+    }
+}
+
 int env_int(const char* name, int dflt) {
     const char* e = std::getenv(name);
     return e ? std::atoi(e) : dflt;
@@ -80,6 +90,7 @@ struct v2m_session {
     VolCtl* ctl_init = nullptr;
     int serial_power = 0;
     int force_threads = 256;
+    int nbr_threads = 128;
     int refresh_blocks = 0;
     int max_iters = 0;
     int graph_iters = 10;
@@ -116,6 +127,10 @@ struct v2m_session {
 };
 
 namespace {
+
+bool tune_lookup(v2m_session* s);
+void tune_store(v2m_session* s);
+std::string do_autotune(v2m_session* s, int reps);
 
 void check_kernel_error(v2m_session* s) {
     Global g;
@@ -436,6 +451,14 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
         ck(cudaMemcpyAsync(s->typ0, d.typ, N, cudaMemcpyDeviceToDevice, s->stream), "seed typ");
         ck(cudaMemcpyAsync(s->part0, d.part, 4 * N, cudaMemcpyDeviceToDevice, s->stream), "seed part");
         do_reset(s);
+        s->nbr_threads = env_int("V2M_CUDA_NBR_THREADS", 128);
+        if (s->nbr_threads != 64 && s->nbr_threads != 128 && s->nbr_threads != 256) {
+            s->nbr_threads = 128;
+        }
+        if (env_int("V2M_CUDA_AUTOTUNE", 0) && !tune_lookup(s)) {
+            do_autotune(s, 20);
+            tune_store(s);
+        }
         return s;
     } catch (...) {
         delete s;
@@ -449,7 +472,7 @@ void enqueue_rebuild(v2m_session* s) {
     launch_keys(s->stream, d);
     launch_scan(s->stream, d);
     launch_scatter(s->stream, d);
-    launch_neighbors(s->stream, d);
+    launch_neighbors(s->stream, d, s->nbr_threads);
     s->launches += 8;
 }
 
@@ -1033,6 +1056,156 @@ int v2m_session_write_lists(v2m_session* s, int vol, const int32_t* nbr, const i
         ck(cudaFreeAsync(t, s->stream), "cudaFreeAsync");
         ck(cudaGetLastError(), "launch");
         ck(cudaStreamSynchronize(s->stream), "synchronize");
+    });
+}
+
+}  // extern "C"
+
+// ---- autotuner ---------------------------------------------------------------------
+// Launch shapes that cannot change a result: the force kernel's block (one node
+// per thread, a pure function of the state) and the list kernel's warps per
+// block (one node per warp). The move block is not tuned: it fixes the shape of
+// the FIRE power's summation tree. Each candidate is timed with CUDA events on
+// the session's own lists; the choice is cached per (device, node-count octave,
+// volume count) in V2M_CUDA_TUNE_CACHE (default $HOME/.cache/v2m_cuda_tune.txt).
+namespace {
+
+std::string tune_key(v2m_session* s) {
+    cudaDeviceProp p;
+    cudaGetDeviceProperties(&p, s->device);
+    int oct = 0;
+    while ((int64_t(1) << (oct + 1)) <= s->d.N) {
+        ++oct;
+    }
+    std::string name = p.name;
+    for (char& c : name) {
+        if (c == ' ') {
+            c = '_';
+        }
+    }
+    return name + "|n2^" + std::to_string(oct) + "|v" + std::to_string(s->nvol);
+}
+
+std::string tune_path() {
+    if (const char* e = std::getenv("V2M_CUDA_TUNE_CACHE")) {
+        return e;
+    }
+    const char* home = std::getenv("HOME");
+    return std::string(home ? home : "/tmp") + "/.cache/v2m_cuda_tune.txt";
+}
+
+bool tune_lookup(v2m_session* s) {
+    FILE* f = std::fopen(tune_path().c_str(), "r");
+    if (!f) {
+        return false;
+    }
+    char key[512];
+    int ft = 0, nt = 0;
+    bool hit = false;
+    const std::string want = tune_key(s);
+    while (std::fscanf(f, "%511s %d %d", key, &ft, &nt) == 3) {
+        if (want == key) {
+            s->force_threads = ft;
+            s->nbr_threads = nt;
+            hit = true;
+        }
+    }
+    std::fclose(f);
+    return hit;
+}
+
+void tune_store(v2m_session* s) {
+    const std::string path = tune_path();
+    const size_t slash = path.rfind('/');
+    if (slash != std::string::npos) {
+        std::string dir = path.substr(0, slash);
+        mkdir_p(dir);
+    }
+    FILE* f = std::fopen(path.c_str(), "a");
+    if (f) {
+        std::fprintf(f, "%s %d %d\n", tune_key(s).c_str(), s->force_threads, s->nbr_threads);
+        std::fclose(f);
+    }
+}
+
+float time_launches(v2m_session* s, int reps, const std::function<void()>& launch) {
+    cudaEvent_t e0, e1;
+    ck(cudaEventCreate(&e0), "event");
+    ck(cudaEventCreate(&e1), "event");
+    launch();   // warm
+    ck(cudaEventRecord(e0, s->stream), "event");
+    for (int r = 0; r < reps; ++r) {
+        launch();
+    }
+    ck(cudaEventRecord(e1, s->stream), "event");
+    ck(cudaEventSynchronize(e1), "event sync");
+    float ms = 0.0f;
+    ck(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ck(cudaGetLastError(), "launch");
+    return ms / reps;
+}
+
+std::string do_autotune(v2m_session* s, int reps) {
+    do_reset(s);
+    do_rebuild(s);
+    std::string rep;
+    float best = 1e30f;
+    int bf = s->force_threads;
+    for (int t : { 64, 128, 256, 512 }) {
+        const float ms = time_launches(s, reps, [&] { launch_force(s->stream, s->d, t); });
+        rep += "force " + std::to_string(t) + " " + std::to_string(ms) + " ms\n";
+        if (ms < best) {
+            best = ms;
+            bf = t;
+        }
+    }
+    launch_set_rebuild(s->stream, s->d, 1);
+    best = 1e30f;
+    int bn = s->nbr_threads;
+    for (int t : { 64, 128, 256 }) {
+        const float ms = time_launches(s, reps, [&] { launch_neighbors(s->stream, s->d, t); });
+        rep += "neighbors " + std::to_string(t) + " " + std::to_string(ms) + " ms\n";
+        if (ms < best) {
+            best = ms;
+            bn = t;
+        }
+    }
+    s->force_threads = bf;
+    s->nbr_threads = bn;
+    if (s->gexec) {   // the graph holds the old shapes
+        cudaGraphExecDestroy(s->gexec);
+        s->gexec = nullptr;
+    }
+    do_reset(s);
+    rep += "chosen force " + std::to_string(bf) + " neighbors " + std::to_string(bn) + "\n";
+    return rep;
+}
+
+}  // namespace
+
+extern "C" {
+
+int v2m_session_autotune(v2m_session* s, int reps, char* report, int64_t report_len) {
+    return guard([&] {
+        ck(cudaSetDevice(s->device), "cudaSetDevice");
+        const std::string r = do_autotune(s, reps > 0 ? reps : 20);
+        tune_store(s);
+        if (report && report_len > 0) {
+            std::snprintf(report, (size_t)report_len, "%s", r.c_str());
+        }
+    });
+}
+
+int v2m_session_shapes(v2m_session* s, int32_t* force_threads, int32_t* nbr_threads) {
+    return guard([&] {
+        if (force_threads) {
+            *force_threads = s->force_threads;
+        }
+        if (nbr_threads) {
+            *nbr_threads = s->nbr_threads;
+        }
     });
 }
 

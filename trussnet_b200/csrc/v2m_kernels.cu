@@ -441,15 +441,15 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(kNbrThreads) k_neighbors(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
+__global__ void __launch_bounds__(kNbrMaxThreads) k_neighbors(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
                                                            const uint16_t* __restrict__ nodevol, const float4* __restrict__ Pq,
                                                            const uint8_t* __restrict__ typ, const uint16_t* __restrict__ lab,
                                                            const int* __restrict__ cstart, const int* __restrict__ sorted,
                                                            const float4* __restrict__ Ps, int* __restrict__ nbr,
                                                            uint8_t* __restrict__ nnb, int64_t N) {
-    __shared__ NbrWarpSmem sm[kNbrThreads / 32];
+    __shared__ NbrWarpSmem sm[kNbrMaxThreads / 32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t i = blockIdx.x * (int64_t)(kNbrThreads / 32) + w;
+    const int64_t i = blockIdx.x * (int64_t)(blockDim.x / 32) + w;
     if (i >= N) {
         return;
     }
@@ -462,18 +462,19 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors(const DVol* __restric
 
 // The self-refresh of the nodes past a full skin (list filled by k_move), one
 // warp per entry; the last block to finish empties the list.
-__global__ void __launch_bounds__(kNbrThreads) k_refresh(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
+__global__ void __launch_bounds__(kNbrMaxThreads) k_refresh(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
                                                          const uint16_t* __restrict__ nodevol, const float4* __restrict__ Pq,
                                                          const uint8_t* __restrict__ typ, const uint16_t* __restrict__ lab,
                                                          const int* __restrict__ cstart, const int* __restrict__ sorted,
                                                          const float4* __restrict__ Ps, int* __restrict__ nbr,
                                                          uint8_t* __restrict__ nnb, float4* __restrict__ P0,
                                                          const int* __restrict__ rlist, Global* G, int64_t N) {
-    __shared__ NbrWarpSmem sm[kNbrThreads / 32];
+    __shared__ NbrWarpSmem sm[kNbrMaxThreads / 32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int cnt = *((volatile int*)&G->nrefresh);
-    const int nw = gridDim.x * (kNbrThreads / 32);
-    for (int e = blockIdx.x * (kNbrThreads / 32) + w; e < cnt; e += nw) {
+    const int wpb = blockDim.x / 32;
+    const int nw = gridDim.x * wpb;
+    for (int e = blockIdx.x * wpb + w; e < cnt; e += nw) {
         const int64_t i = rlist[e];
         const int v = nodevol[i];
         if (ctl[v].done) {
@@ -992,8 +993,8 @@ void launch_scatter(cudaStream_t s, const Dev& d) {
     k_binsort<<<nblk(d.KT, 256), 256, 0, s>>>(d.vols, d.ctl, d.tilevol, d.cstart, d.sorted, d.Pq, d.Ps, d.KT);
 }
 
-void launch_neighbors(cudaStream_t s, const Dev& d) {
-    k_neighbors<<<nblk(d.N, kNbrThreads / 32), kNbrThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.typ, d.lab,
+void launch_neighbors(cudaStream_t s, const Dev& d, int threads) {
+    k_neighbors<<<nblk(d.N, threads / 32), threads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.typ, d.lab,
                                                                      d.cstart, d.sorted, d.Ps, d.nbr, d.nnb, d.N);
 }
 
@@ -1014,7 +1015,7 @@ void launch_control(cudaStream_t s, const Dev& d, int serial) {
 }
 
 void launch_refresh(cudaStream_t s, const Dev& d, int blocks) {
-    k_refresh<<<blocks, kNbrThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.typ, d.lab, d.cstart, d.sorted, d.Ps,
+    k_refresh<<<blocks, kNbrMaxThreads / 2, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.typ, d.lab, d.cstart, d.sorted, d.Ps,
                                               d.nbr, d.nnb, d.P0, d.rlist, d.G, d.N);
 }
 

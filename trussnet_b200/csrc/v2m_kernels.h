@@ -11,7 +11,7 @@ namespace v2m {
 
 constexpr int kScanTile = 1024;     // bin entries per scan tile (volume bin ranges are aligned to it)
 constexpr int kScanThreads = 256;
-constexpr int kNbrThreads = 128;    // 4 warps, one node each
+constexpr int kNbrMaxThreads = 256; // k_neighbors: up to 8 warps per block, one node each
 constexpr int kMoveThreads = 256;   // volume node ranges are aligned to it
 constexpr int kCtlThreads = 256;
 constexpr int kNodeAlign = kMoveThreads;
@@ -54,7 +54,7 @@ struct Dev {
 void launch_keys(cudaStream_t s, const Dev& d);
 void launch_scan(cudaStream_t s, const Dev& d);
 void launch_scatter(cudaStream_t s, const Dev& d);
-void launch_neighbors(cudaStream_t s, const Dev& d);
+void launch_neighbors(cudaStream_t s, const Dev& d, int threads);
 void launch_force(cudaStream_t s, const Dev& d, int threads);
 void launch_move(cudaStream_t s, const Dev& d);
 void launch_control(cudaStream_t s, const Dev& d, int serial);

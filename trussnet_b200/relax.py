@@ -163,6 +163,18 @@ class Session:
         _lib.check(self.L.v2m_session_timed_runs(self.h, int(runs), int(graph), int(time_force), C.byref(ms)))
         return ms.value
 
+    def autotune(self, reps: int = 20) -> str:
+        """Time the result-neutral launch shapes, keep the fastest (cached); the
+        session is reset to its seeds."""
+        buf = C.create_string_buffer(4096)
+        _lib.check(self.L.v2m_session_autotune(self.h, int(reps), buf, len(buf)))
+        return buf.value.decode()
+
+    def shapes(self):
+        a, b = C.c_int32(), C.c_int32()
+        _lib.check(self.L.v2m_session_shapes(self.h, C.byref(a), C.byref(b)))
+        return dict(force_threads=a.value, nbr_threads=b.value)
+
     def clear_counters(self):
         _lib.check(self.L.v2m_session_clear_counters(self.h))
 

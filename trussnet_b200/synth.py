@@ -329,3 +329,36 @@ def gray_sphere(dim=48, seed=0, thresholds=(0.3, 0.6), widths=(0.2, 0.2), h=2.0,
     g.gm = int(t.size)
     nd = seed_lattice(L, hf, rng, density=h / spacing, hmin=h, hmax=h)
     return g, nd
+
+
+def sizing_grid(shape=(64, 64, 64), lo=1.5, hi=4.0, seed=0):
+    """A seeded smooth sizing grid G [m2, m1, m0] (x fastest) with values in [lo, hi]."""
+    rng = np.random.default_rng(seed)
+    nz = value_noise(tuple(shape[::-1]), 2, 3, rng)
+    nz = (nz - nz.min()) / max(1e-12, float(nz.max() - nz.min()))
+    return (lo + (hi - lo) * nz).astype(np.float32)
+
+
+def sample_sizing(G: np.ndarray, cs, dims) -> np.ndarray:
+    """G interpolated trilinearly at every voxel centre of a (nx, ny, nz) grid (x fastest)."""
+    nx, ny, nz = dims
+    m = G.shape[::-1]
+    coords = []
+    for n, c, mm in zip((nz, ny, nx), (cs[2], cs[1], cs[0]), (m[2], m[1], m[0])):
+        coords.append(np.clip(np.arange(n) / c, 0, mm - 1))
+    zz, yy, xx = np.meshgrid(*coords, indexing="ij")
+    return ndimage.map_coordinates(G.astype(np.float64), [zz, yy, xx], order=1, mode="nearest").astype(np.float32)
+
+
+def ellipsoids_adjoint(dim=128, m=64, nlab=4, lo=1.5, hi=4.0, density=1.66, seed=0):
+    """The adjoint workload: nested ellipsoids (nlab labels) in a dim^3 volume,
+    a seeded m^3 sizing grid in [lo, hi] spanning the volume (cell (dim-1)/(m-1)),
+    the per-voxel h sampled from it, and lattice seeds graded by it."""
+    rng = np.random.default_rng(seed)
+    L = nested_shells(dim, nlab - 1, 0.22 * dim, 0.44 * dim, 0.04 * dim, rng)
+    G = sizing_grid((m, m, m), lo, hi, seed + 1)
+    cs = ((dim - 1) / (m - 1),) * 3
+    hf = sample_sizing(G, cs, (dim, dim, dim))
+    g = build_grid(L, hf, lo, hi)
+    nd = seed_lattice(L, hf, rng, density=density, hmin=lo, hmax=hi)
+    return g, nd, G, cs
