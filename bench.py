@@ -267,6 +267,11 @@ def run_cuda(args):
                 "bytes_per_launch": force_bytes, "mean_nnb": float(nnb.mean()) if n else 0.0,
                 "force_ms_per_launch": force_avg_ms, "force_share_of_step": cnt["force_ms"] / ms if ms else None}
     st = sess.stats()
+    # where an iteration's time goes: one more run from the seeds, its first 100
+    # iterations profiled stage by stage (plain launches, outside the timed region)
+    sess.reset()
+    sess.rebuild()
+    stages = sess.profile_stages(min(100, iters))
     sess.close()
     # end to end through the public call (tn::relax_cl's C ABI) with pinned host buffers
     e2e = None
@@ -285,7 +290,7 @@ def run_cuda(args):
                            "rebuilds_per_step": st.rebuilds, "final_types": [st.n_interior, st.n_interface,
                                                                              st.n_junction, st.n_corner]},
                 "clocks": clocks, "e2e": e2e, "gpu_launches": int(cnt["launches"]), "roofline": roofline,
-                "cpu_baseline": cb}
+                "stage_ms_first100": stages, "cpu_baseline": cb}
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()

@@ -218,6 +218,12 @@ int v2m_session_timed_runs(v2m_session* s, int runs, int graph, int time_force, 
 int v2m_session_autotune(v2m_session* s, int reps, char* report, int64_t report_len);
 int v2m_session_shapes(v2m_session* s, int32_t* force_threads, int32_t* nbr_threads);
 int v2m_session_clear_counters(v2m_session* s);
+/*
+ * Per-stage device milliseconds over `iters` iterations from the current state,
+ * plain launches with CUDA events between the stages: ms[0] force, ms[1] move,
+ * ms[2] control + self-refresh, ms[3] the rebuild stages, ms[4] the iterations.
+ */
+int v2m_session_profile_stages(v2m_session* s, int iters, double* ms);
 
 /*
  * The differentiable relaxation unroll and its adjoint (no counterpart in the

@@ -344,6 +344,8 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
         d.nbr = s->alloc<int>((size_t)N * V2M_K);
         d.nnb = s->alloc<uint8_t>(N);
         d.rlist = s->alloc<int>(N);
+        d.S = s->alloc<float4>(N);
+        d.queue = s->alloc<int>(N);
         d.cnt = s->alloc<int>(KT);
         d.cstart = s->alloc<int>(KT);
         d.cursor = s->alloc<int>(KT);
@@ -473,7 +475,7 @@ void enqueue_rebuild(v2m_session* s) {
     launch_scan(s->stream, d);
     launch_scatter(s->stream, d);
     launch_neighbors(s->stream, d, s->nbr_threads);
-    s->launches += 8;
+    s->launches += 7;
 }
 
 // (inside a stream capture an event record only becomes a graph node with
@@ -503,7 +505,7 @@ void enqueue_tail(v2m_session* s) {
     launch_move(s->stream, d);
     launch_control(s->stream, d, s->serial_power);
     launch_refresh(s->stream, d, s->refresh_blocks);
-    s->launches += 3 + (s->serial_power ? 1 : 0);
+    s->launches += 4 + (s->serial_power ? 1 : 0);
     enqueue_rebuild(s);
 }
 
@@ -567,7 +569,7 @@ void do_iterate(v2m_session* s, int iters, int graph) {
         const int G = s->graph_iters;
         int done_it = 0;
         // per-iteration launches inside the graph: force + tail
-        const int per_it = 1 + 3 + (s->serial_power ? 1 : 0) + 8;
+        const int per_it = 1 + 4 + (s->serial_power ? 1 : 0) + 7;
         while (done_it < iters) {
             ck(cudaGraphLaunch(s->gexec, s->stream), "cudaGraphLaunch");
             s->launches += (int64_t)G * per_it;
@@ -1206,6 +1208,52 @@ int v2m_session_shapes(v2m_session* s, int32_t* force_threads, int32_t* nbr_thre
         if (nbr_threads) {
             *nbr_threads = s->nbr_threads;
         }
+    });
+}
+
+// Per-stage device time over `iters` iterations run as plain launches with
+// CUDA events between the stages: ms[0] force, [1] move (pre + main),
+// [2] control + refresh, [3] rebuild stages (keys, scan, scatter, in-bin order,
+// lists; no-ops unless a volume rebuilds), [4] whole iterations.
+int v2m_session_profile_stages(v2m_session* s, int iters, double* ms) {
+    return guard([&] {
+        if (iters < 1 || !ms) {
+            throw ArgError("bad argument");
+        }
+        ck(cudaSetDevice(s->device), "cudaSetDevice");
+        cudaEvent_t ev[6];
+        for (auto& e : ev) {
+            ck(cudaEventCreate(&e), "event");
+        }
+        for (int k = 0; k < 5; ++k) {
+            ms[k] = 0.0;
+        }
+        const Dev& d = s->d;
+        for (int it = 0; it < iters; ++it) {
+            ck(cudaEventRecord(ev[0], s->stream), "event");
+            launch_force(s->stream, d, s->force_threads);
+            ck(cudaEventRecord(ev[1], s->stream), "event");
+            launch_move(s->stream, d);
+            ck(cudaEventRecord(ev[2], s->stream), "event");
+            launch_control(s->stream, d, s->serial_power);
+            launch_refresh(s->stream, d, s->refresh_blocks);
+            ck(cudaEventRecord(ev[3], s->stream), "event");
+            enqueue_rebuild(s);
+            ck(cudaEventRecord(ev[4], s->stream), "event");
+            ck(cudaEventSynchronize(ev[4]), "event sync");
+            for (int k = 0; k < 4; ++k) {
+                float t = 0.0f;
+                ck(cudaEventElapsedTime(&t, ev[k], ev[k + 1]), "elapsed");
+                ms[k] += t;
+            }
+            float t = 0.0f;
+            ck(cudaEventElapsedTime(&t, ev[0], ev[4]), "elapsed");
+            ms[4] += t;
+        }
+        for (auto& e : ev) {
+            cudaEventDestroy(e);
+        }
+        check_kernel_error(s);
     });
 }
 

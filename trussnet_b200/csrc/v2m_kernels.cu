@@ -492,6 +492,8 @@ __global__ void __launch_bounds__(kNbrMaxThreads) k_refresh(const DVol* __restri
         const int d = atomicAdd(&G->blocks_done, 1);
         if (d == (int)gridDim.x - 1) {
             G->nrefresh = 0;
+            G->qtrap = 0;
+            G->qint = 0;
             G->blocks_done = 0;
             __threadfence();
         }
@@ -557,34 +559,107 @@ __device__ __forceinline__ int hist_bin(float m) {
     return b < 0 ? 0 : (b > 31 ? 31 : b);
 }
 
-__global__ void __launch_bounds__(kMoveThreads) k_move(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl,
-                                                      const uint16_t* __restrict__ nodevol, float4* __restrict__ Pq,
-                                                      const float4* __restrict__ F, float4* __restrict__ Vel,
-                                                      uint8_t* __restrict__ typ, const uint16_t* __restrict__ lab,
-                                                      uint32_t* __restrict__ part, float* __restrict__ mvout,
-                                                      float* __restrict__ pwout, const float4* __restrict__ P0,
-                                                      double* __restrict__ psum, int* __restrict__ rlist, Global* G,
-                                                      int64_t N) {
-    __shared__ int sh_hist[32];
-    __shared__ unsigned sh_max, sh_maxd;
-    __shared__ int sh_half, sh_vol;
-    __shared__ double sh_pw[kMoveThreads / 32];
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+// The iteration's reductions of one finished node (its |dp|/h, position, size):
+// log2 histogram, max, Verlet half-skin count or self-refresh request
+// (src/v2m_particles.cpp:874-937; src/opencl/v2m_kernels.cl:196-249). `shared`
+// accumulates into the block's counters when every node of the block belongs to
+// volume `v` (then flushed once), else straight into the volume's counters.
+struct TailAcc {
+    int hist[32];
+    unsigned maxbits, maxd;
+    int half;
+};
+
+__device__ __forceinline__ void node_tail(const DVol& Vd, VolCtl* ctl, int v, int64_t i, float m, float px, float py,
+                                          float pz, float hh, const float4* __restrict__ P0, int* __restrict__ rlist,
+                                          Global* G, TailAcc* sh) {
+    const float4 q0 = P0[i];
+    const float ex = px - q0.x, ey = py - q0.y, ez = pz - q0.z;
+    const float m2 = ex * ex + ey * ey + ez * ez, s2 = Vd.skin * Vd.skin * hh * hh;
+    const int b = hist_bin(m);
+    VolCtl* cv = ctl + v;
+    if (sh) {
+        atomicAdd(&sh->hist[b], 1);
+        atomicMax(&sh->maxbits, __float_as_uint(m));
+        if (Vd.policy == 1) {
+            atomicMax(&sh->maxd, __float_as_uint(sqrtf(m2) / hh));
+        }
+    } else {
+        atomicAdd(&cv->hist[b], 1);
+        atomicMax(&cv->maxbits, __float_as_uint(m));
+        if (Vd.policy == 1) {
+            atomicMax(reinterpret_cast<unsigned*>(&cv->pad1), __float_as_uint(sqrtf(m2) / hh));
+        }
+    }
+    if (m2 > s2) {
+        const int e = atomicAdd(&G->nrefresh, 1);
+        rlist[e] = (int)i;
+        atomicAdd(&cv->nrefresh, 1);
+    } else if (m2 > 0.25f * s2) {
+        if (sh) {
+            atomicAdd(&sh->half, 1);
+        } else {
+            atomicAdd(&cv->nhalf, 1);
+        }
+    }
+}
+
+__device__ __forceinline__ void tail_init(TailAcc& a) {
     if (threadIdx.x < 32) {
-        sh_hist[threadIdx.x] = 0;
+        a.hist[threadIdx.x] = 0;
     }
     if (threadIdx.x == 0) {
-        sh_max = 0u;
-        sh_maxd = 0u;
-        sh_half = 0;
+        a.maxbits = 0u;
+        a.maxd = 0u;
+        a.half = 0;
+    }
+}
+
+__device__ __forceinline__ void tail_flush(TailAcc& a, VolCtl* cv) {
+    if (threadIdx.x < 32 && a.hist[threadIdx.x]) {
+        atomicAdd(&cv->hist[threadIdx.x], a.hist[threadIdx.x]);
+    }
+    if (threadIdx.x == 0) {
+        if (a.maxbits) {
+            atomicMax(&cv->maxbits, a.maxbits);
+        }
+        if (a.maxd) {
+            atomicMax(reinterpret_cast<unsigned*>(&cv->pad1), a.maxd);
+        }
+        if (a.half) {
+            atomicAdd(&cv->nhalf, a.half);
+        }
+    }
+}
+
+// First half of v2m_move (src/opencl/v2m_particle_body.cl:844-921), every node in
+// node order: FIRE velocity update and power, the step, the settle test and the
+// step cap. Corners and settled nodes finish here; the others are queued with
+// their step (S = s, h) for k_move_main -- trapped (non-INTERIOR) nodes at the
+// front of the queue, INTERIOR ones at the back, so that a warp of k_move_main
+// holds nodes of one kind. The FIRE power of the block is summed here, in node
+// order (a fixed-shape double tree: deterministic whatever the queue order).
+__global__ void __launch_bounds__(kMoveThreads) k_move_pre(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl,
+                                                          const uint16_t* __restrict__ nodevol,
+                                                          const float4* __restrict__ Pq, const float4* __restrict__ F,
+                                                          float4* __restrict__ Vel, const uint8_t* __restrict__ typ,
+                                                          float* __restrict__ mvout, float* __restrict__ pwout,
+                                                          const float4* __restrict__ P0, float4* __restrict__ S,
+                                                          int* __restrict__ queue, double* __restrict__ psum,
+                                                          int* __restrict__ rlist, Global* G, int64_t N) {
+    __shared__ TailAcc acc;
+    __shared__ int sh_vol;
+    __shared__ double sh_pw[kMoveThreads / 32];
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    tail_init(acc);
+    if (threadIdx.x == 0) {
         sh_vol = -1;
     }
     __syncthreads();
-    // every node of a block lies in one volume (node ranges are kMoveThreads-aligned;
-    // padding sits at the end of a range)
     const int v = i < N ? nodevol[i] : 0xFFFF;
     bool active = v != 0xFFFF;
     float pwv = 0.0f;
+    int qkind = -1;   // 0: trapped queue, 1: interior queue
     if (active) {
         const DVol& Vd = vols[v];
         const VolCtl& c = ctl[v];
@@ -594,31 +669,17 @@ __global__ void __launch_bounds__(kMoveThreads) k_move(const DVol* __restrict__ 
             if (threadIdx.x == 0) {
                 sh_vol = v;
             }
-            const DGrid& g = Vd.g;
             const int fire = Vd.fire;
             const float fdt = c.fdt, falpha = c.falpha;
             const float4 pq = Pq[i];
-            NodeState st;
-            st.p[0] = pq.x;
-            st.p[1] = pq.y;
-            st.p[2] = pq.z;
-            st.hn = fabsf(pq.w);
-            st.a = lab[i];
-            st.ty = typ[i];
-            const uint32_t pp = part[i];
-            st.pb = (int)(pp & 0xFFFFu);
-            st.pc = (int)(pp >> 16);
-            const int ty0 = st.ty;
-            const float p0 = pq.x, p1 = pq.y, p2 = pq.z;
-            const float h = size_at(g, Vd.hmode, p0, p1, p2);
-            float m = 0.0f;
-            float4 vnew = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            const int ty0 = typ[i];
+            const float h = size_at(Vd.g, Vd.hmode, pq.x, pq.y, pq.z);
+            bool finished = true;
             if (ty0 != V2M_CORNER) {
                 const float4 f4 = F[i];
                 const float stiff = f4.w > 1.0f ? f4.w : 1.0f;
-                float ac[3] = { f4.x / stiff, f4.y / stiff, f4.z / stiff };
+                const float ac[3] = { f4.x / stiff, f4.y / stiff, f4.z / stiff };
                 float s[3];
-                bool go = true;
                 if (fire) {
                     float vv[3] = { 0.0f, 0.0f, 0.0f };
                     if (!c.vzero) {
@@ -650,54 +711,51 @@ __global__ void __launch_bounds__(kMoveThreads) k_move(const DVol* __restrict__ 
                     }
                 }
                 const float sl = sqrtf(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
-                if (sl < 5e-4f * h) {
-                    go = false;
-                }
-                if (go) {
+                if (!(sl < 5e-4f * h)) {
                     if (sl > Vd.maxstep * h) {
                         for (int k = 0; k < 3; ++k) {
                             s[k] *= Vd.maxstep * h / sl;
                         }
                     }
-                    m = move_step(g, Vd.hmode, h, s, Vd.maxstep, Vd.snap, Vd.voxmode, st);
-                    if (fire && m > 0.0f && st.ty == ty0) {
-                        vnew = make_float4((st.p[0] - p0) / fdt, (st.p[1] - p1) / fdt, (st.p[2] - p2) / fdt, 0.0f);
-                    }
+                    S[i] = make_float4(s[0], s[1], s[2], h);
+                    finished = false;
+                    qkind = ty0 == V2M_INTERIOR ? 1 : 0;
                 }
             }
             if (fire) {
-                Vel[i] = vnew;
                 pwout[i] = pwv;
             }
-            mvout[i] = m;
-            Pq[i] = make_float4(st.p[0], st.p[1], st.p[2], pack_h(st.hn, st.ty));
-            typ[i] = (uint8_t)st.ty;
-            part[i] = (uint32_t)(st.pb & 0xFFFF) | ((uint32_t)(st.pc & 0xFFFF) << 16);
-            // the iteration's reductions
-            atomicAdd(&sh_hist[hist_bin(m)], 1);
-            atomicMax(&sh_max, __float_as_uint(m));
-            const float4 q0 = P0[i];
-            const float ex = st.p[0] - q0.x, ey = st.p[1] - q0.y, ez = st.p[2] - q0.z;
-            const float hh = st.hn;
-            const float m2 = ex * ex + ey * ey + ez * ez, s2 = Vd.skin * Vd.skin * hh * hh;
-            if (Vd.policy == 1) {
-                atomicMax(&sh_maxd, __float_as_uint(sqrtf(m2) / hh));
-            }
-            if (m2 > s2) {
-                const int e = atomicAdd(&G->nrefresh, 1);
-                rlist[e] = (int)i;
-                atomicAdd(&ctl[v].nrefresh, 1);
-            } else if (m2 > 0.25f * s2) {
-                atomicAdd(&sh_half, 1);
+            if (finished) {
+                if (fire) {
+                    Vel[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                }
+                mvout[i] = 0.0f;
+                node_tail(Vd, ctl, v, i, 0.0f, pq.x, pq.y, pq.z, fabsf(pq.w), P0, rlist, G, &acc);
             }
         }
     }
-    // FIRE power of the block, fixed-shape double tree (deterministic)
+    // queue the moving nodes: one atomic per warp and kind
+    const unsigned lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int kind = 0; kind < 2; ++kind) {
+        const unsigned m = __ballot_sync(0xffffffffu, qkind == kind);
+        if (m) {
+            int base = 0;
+            if (lane == (unsigned)(__ffs(m) - 1)) {
+                base = atomicAdd(kind == 0 ? &G->qtrap : &G->qint, __popc(m));
+            }
+            base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+            if (qkind == kind) {
+                const int slot = base + __popc(m & ((1u << lane) - 1u));
+                queue[kind == 0 ? slot : (int)(N - 1 - slot)] = (int)i;
+            }
+        }
+    }
     double pd = active ? (double)pwv : 0.0;
     for (int o = 16; o > 0; o >>= 1) {
         pd += __shfl_down_sync(0xffffffffu, pd, o);
     }
-    if ((threadIdx.x & 31) == 0) {
+    if (lane == 0) {
         sh_pw[threadIdx.x >> 5] = pd;
     }
     __syncthreads();
@@ -711,19 +769,77 @@ __global__ void __launch_bounds__(kMoveThreads) k_move(const DVol* __restrict__ 
             t += sh_pw[w];
         }
         psum[blockIdx.x] = t;
-        VolCtl* cv = ctl + bv;
-        if (sh_max) {
-            atomicMax(&cv->maxbits, sh_max);
-        }
-        if (sh_half) {
-            atomicAdd(&cv->nhalf, sh_half);
-        }
-        if (sh_maxd) {
-            atomicMax(reinterpret_cast<unsigned*>(&cv->pad1), sh_maxd);
-        }
     }
-    if (threadIdx.x < 32 && sh_hist[threadIdx.x]) {
-        atomicAdd(&ctl[bv].hist[threadIdx.x], sh_hist[threadIdx.x]);
+    tail_flush(acc, ctl + bv);
+}
+
+// Second half of v2m_move: the trapped move (v2m_move_step) of every queued
+// node, then its velocity, |dp|/h and the iteration's reductions.
+__global__ void __launch_bounds__(kMoveThreads) k_move_main(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl,
+                                                           const uint16_t* __restrict__ nodevol, float4* __restrict__ Pq,
+                                                           float4* __restrict__ Vel, uint8_t* __restrict__ typ,
+                                                           const uint16_t* __restrict__ lab, uint32_t* __restrict__ part,
+                                                           float* __restrict__ mvout, const float4* __restrict__ P0,
+                                                           const float4* __restrict__ S, const int* __restrict__ queue,
+                                                           int* __restrict__ rlist, Global* G, int64_t N) {
+    __shared__ TailAcc acc;
+    __shared__ int sh_v0, sh_mixed;
+    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int qa = *((volatile int*)&G->qtrap), qb = *((volatile int*)&G->qint);
+    int64_t i = -1;
+    if (q < N && (q < qa || q >= N - qb)) {
+        i = queue[q];
+    }
+    tail_init(acc);
+    if (threadIdx.x == 0) {
+        sh_v0 = -1;
+        sh_mixed = 0;
+    }
+    __syncthreads();
+    const int v = i >= 0 ? nodevol[i] : -1;
+    if (v >= 0) {
+        atomicCAS(&sh_v0, -1, v);
+    }
+    __syncthreads();
+    if (v >= 0 && v != sh_v0) {
+        sh_mixed = 1;
+    }
+    __syncthreads();
+    const bool uniform = !sh_mixed;
+    if (v >= 0) {
+        const DVol& Vd = vols[v];
+        const VolCtl& c = ctl[v];
+        const DGrid& g = Vd.g;
+        const float4 pq = Pq[i];
+        const float4 s4 = S[i];
+        NodeState st;
+        st.p[0] = pq.x;
+        st.p[1] = pq.y;
+        st.p[2] = pq.z;
+        st.hn = fabsf(pq.w);
+        st.a = lab[i];
+        st.ty = typ[i];
+        const uint32_t pp = part[i];
+        st.pb = (int)(pp & 0xFFFFu);
+        st.pc = (int)(pp >> 16);
+        const int ty0 = st.ty;
+        float s[3] = { s4.x, s4.y, s4.z };
+        const float m = move_step(g, Vd.hmode, s4.w, s, Vd.maxstep, Vd.snap, Vd.voxmode, st);
+        if (Vd.fire) {
+            const float fdt = c.fdt;
+            Vel[i] = (m > 0.0f && st.ty == ty0)
+                         ? make_float4((st.p[0] - pq.x) / fdt, (st.p[1] - pq.y) / fdt, (st.p[2] - pq.z) / fdt, 0.0f)
+                         : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        mvout[i] = m;
+        Pq[i] = make_float4(st.p[0], st.p[1], st.p[2], pack_h(st.hn, st.ty));
+        typ[i] = (uint8_t)st.ty;
+        part[i] = (uint32_t)(st.pb & 0xFFFF) | ((uint32_t)(st.pc & 0xFFFF) << 16);
+        node_tail(Vd, ctl, v, i, m, st.p[0], st.p[1], st.p[2], st.hn, P0, rlist, G, uniform ? &acc : nullptr);
+    }
+    __syncthreads();
+    if (uniform && sh_v0 >= 0) {
+        tail_flush(acc, ctl + sh_v0);
     }
 }
 
@@ -1003,8 +1119,11 @@ void launch_force(cudaStream_t s, const Dev& d, int threads) {
 }
 
 void launch_move(cudaStream_t s, const Dev& d) {
-    k_move<<<nblk(d.N, kMoveThreads), kMoveThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.F, d.Vel, d.typ, d.lab,
-                                                            d.part, d.mv, d.pw, d.P0, d.psum, d.rlist, d.G, d.N);
+    k_move_pre<<<nblk(d.N, kMoveThreads), kMoveThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.F, d.Vel, d.typ,
+                                                                d.mv, d.pw, d.P0, d.S, d.queue, d.psum, d.rlist, d.G,
+                                                                d.N);
+    k_move_main<<<nblk(d.N, kMoveThreads), kMoveThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.Vel, d.typ, d.lab,
+                                                                 d.part, d.mv, d.P0, d.S, d.queue, d.rlist, d.G, d.N);
 }
 
 void launch_control(cudaStream_t s, const Dev& d, int serial) {

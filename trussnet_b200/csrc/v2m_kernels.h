@@ -42,6 +42,8 @@ struct Dev {
     int* nbr = nullptr;            // slot-major: nbr[k*N + i]
     uint8_t* nnb = nullptr;
     int* rlist = nullptr;
+    float4* S = nullptr;           // queued nodes' capped step and h
+    int* queue = nullptr;          // move queue: trapped from the front, interior from the back
     int* cnt = nullptr;
     int* cstart = nullptr;
     int* cursor = nullptr;

@@ -89,6 +89,7 @@ struct Global {
     int blocks_done;     // last-block-done counter of the refresh kernel
     int err;             // kernel error flag (first error code)
     int err_info;
+    int qtrap, qint;     // move queue lengths: trapped nodes (front), interior nodes (back)
 };
 
 constexpr int kMaxVol = 1024;

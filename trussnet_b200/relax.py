@@ -175,6 +175,12 @@ class Session:
         _lib.check(self.L.v2m_session_shapes(self.h, C.byref(a), C.byref(b)))
         return dict(force_threads=a.value, nbr_threads=b.value)
 
+    def profile_stages(self, iters: int) -> dict:
+        """Device ms per stage over `iters` plain-launch iterations from the current state."""
+        ms = np.zeros(5, np.float64)
+        _lib.check(self.L.v2m_session_profile_stages(self.h, int(iters), ms.ctypes.data))
+        return dict(zip(("force", "move", "control_refresh", "rebuild", "total"), ms.tolist()))
+
     def clear_counters(self):
         _lib.check(self.L.v2m_session_clear_counters(self.h))
 
