@@ -50,28 +50,32 @@ __device__ __forceinline__ LabList load_labels(const DGrid& g, int b) {
 }
 
 // Slot of label l in brick b (-1: uniform brick or l not listed); *has = listed.
-// (src/opencl/v2m_grid_body.cl:122-134)
+// (src/opencl/v2m_grid_body.cl:122-134) The 16 labels are compared two at a
+// time with 16-bit SIMD compares; the first listed match wins, as in the loop.
 __device__ __forceinline__ int slot_lookup(const DGrid& g, int b, int l, int* has) {
     const int n = __ldg(g.bl_cnt + b);
     const LabList ll = load_labels(g, b);
-    *has = 0;
-    int idx = -1;
+    const unsigned pat = (unsigned)(l & 0xFFFF) * 0x00010001u;
+    unsigned bits = 0u;
 #pragma unroll
-    for (int s = 0; s < V2M_BL; ++s) {
-        if (idx < 0 && s < n && ll.get(s) == l) {
-            idx = s;
-        }
+    for (int w = 0; w < 8; ++w) {
+        const unsigned m = __vcmpeq2(ll.w[w], pat);
+        bits |= ((m & 1u) | ((m >> 15) & 2u)) << (2 * w);
     }
-    if (idx < 0) {
+    const int nn = n < V2M_BL ? n : V2M_BL;
+    bits &= nn >= 32 ? 0xFFFFFFFFu : ((1u << nn) - 1u);
+    if (!bits) {
+        *has = 0;
         return -1;
     }
     *has = 1;
+    const int idx = __ffs(bits) - 1;
     const int first = __ldg(g.bl_slot + b);
     return first < 0 ? -1 : first + idx;
 }
 
 // phi_l at voxel (i,j,k) (src/opencl/v2m_grid_body.cl:137-153)
-__device__ __forceinline__ float phi_voxel(const DGrid& g, int l, int i, int j, int k) {
+__device__ __noinline__ float phi_voxel(const DGrid& g, int l, int i, int j, int k) {
     if (i < 0 || j < 0 || k < 0 || i >= g.nx || j >= g.ny || k >= g.nz) {
         return l == 0 ? 1.0f : 0.0f;
     }
@@ -120,7 +124,7 @@ __device__ __forceinline__ float trilerp8(const float* c, float fx, float fy, fl
 }
 
 // phi_l trilinear at p (src/opencl/v2m_grid_body.cl:189-200)
-__device__ __forceinline__ float phi_point(const DGrid& g, int l, float px, float py, float pz) {
+__device__ __noinline__ float phi_point(const DGrid& g, int l, float px, float py, float pz) {
     const float u = px / g.vx, v = py / g.vy, w = pz / g.vz;
     const int i0 = (int)floorf(u), j0 = (int)floorf(v), k0 = (int)floorf(w);
     const float fx = u - i0, fy = v - j0, fz = w - k0;
@@ -237,7 +241,7 @@ __device__ __forceinline__ int owner_label(const DGrid& g, int voxmode, float px
 }
 
 // psi_ab = phi_a - phi_b at p (src/opencl/v2m_seed_body.cl:179-205)
-__device__ __forceinline__ float psi(const DGrid& g, int a, int b, float px, float py, float pz) {
+__device__ __noinline__ float psi(const DGrid& g, int a, int b, float px, float py, float pz) {
     float gv;
     if (gray_psi(g, a, b, px, py, pz, &gv, nullptr)) {
         return gv;
@@ -256,10 +260,11 @@ __device__ __forceinline__ float psi(const DGrid& g, int a, int b, float px, flo
 }
 
 // psi_ab and its cell-analytic gradient (src/opencl/v2m_seed_body.cl:211-247)
-__device__ __forceinline__ float psi_grad(const DGrid& g, int a, int b, float px, float py, float pz, float* gr) {
-    float gv;
+// (one out-of-line copy returning (gradient, value); psi_grad below unpacks it)
+__device__ __noinline__ float4 psi_grad4(const DGrid& g, int a, int b, float px, float py, float pz) {
+    float gv, gr[3];
     if (gray_psi(g, a, b, px, py, pz, &gv, gr)) {
-        return gv;
+        return make_float4(gr[0], gr[1], gr[2], gv);
     }
     const float u = px / g.vx, v = py / g.vy, w = pz / g.vz;
     const int i0 = (int)floorf(u), j0 = (int)floorf(v), k0 = (int)floorf(w);
@@ -279,7 +284,15 @@ __device__ __forceinline__ float psi_grad(const DGrid& g, int a, int b, float px
     gr[0] = (dx0 + fz * (dx1 - dx0)) / g.vx;
     gr[1] = ((x10 - x00) + fz * ((x11 - x01) - (x10 - x00))) / g.vy;
     gr[2] = (y1 - y0) / g.vz;
-    return y0 + fz * (y1 - y0);
+    return make_float4(gr[0], gr[1], gr[2], y0 + fz * (y1 - y0));
+}
+
+__device__ __forceinline__ float psi_grad(const DGrid& g, int a, int b, float px, float py, float pz, float* gr) {
+    const float4 r = psi_grad4(g, a, b, px, py, pz);
+    gr[0] = r.x;
+    gr[1] = r.y;
+    gr[2] = r.z;
+    return r.w;
 }
 
 // Bracketed root of psi_ab along unit direction u from p, within rad: doubling

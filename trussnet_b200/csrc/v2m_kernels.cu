@@ -774,72 +774,96 @@ __global__ void __launch_bounds__(kMoveThreads) k_move_pre(const DVol* __restric
 }
 
 // Second half of v2m_move: the trapped move (v2m_move_step) of every queued
-// node, then its velocity, |dp|/h and the iteration's reductions.
-__global__ void __launch_bounds__(kMoveThreads) k_move_main(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl,
+// node, then its velocity, |dp|/h and the iteration's reductions. Blocks of
+// kMainThreads with no block-wide barrier: a warp's statistics are combined
+// with warp votes and flushed by one lane per (volume, bin), so a finished warp
+// never waits for a slower one.
+__global__ void __launch_bounds__(kMainThreads) k_move_main(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl,
                                                            const uint16_t* __restrict__ nodevol, float4* __restrict__ Pq,
                                                            float4* __restrict__ Vel, uint8_t* __restrict__ typ,
                                                            const uint16_t* __restrict__ lab, uint32_t* __restrict__ part,
                                                            float* __restrict__ mvout, const float4* __restrict__ P0,
                                                            const float4* __restrict__ S, const int* __restrict__ queue,
                                                            int* __restrict__ rlist, Global* G, int64_t N) {
-    __shared__ TailAcc acc;
-    __shared__ int sh_v0, sh_mixed;
     const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int qa = *((volatile int*)&G->qtrap), qb = *((volatile int*)&G->qint);
+    if (blockIdx.x * (int64_t)blockDim.x >= qa && (blockIdx.x + 1) * (int64_t)blockDim.x <= N - qb) {
+        return;   // the whole block lies between the two queues
+    }
     int64_t i = -1;
     if (q < N && (q < qa || q >= N - qb)) {
         i = queue[q];
     }
-    tail_init(acc);
-    if (threadIdx.x == 0) {
-        sh_v0 = -1;
-        sh_mixed = 0;
-    }
-    __syncthreads();
     const int v = i >= 0 ? nodevol[i] : -1;
-    if (v >= 0) {
-        atomicCAS(&sh_v0, -1, v);
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned act = __ballot_sync(0xffffffffu, v >= 0);
+    if (v < 0) {
+        return;
     }
-    __syncthreads();
-    if (v >= 0 && v != sh_v0) {
-        sh_mixed = 1;
+    const DVol& Vd = vols[v];
+    const VolCtl& c = ctl[v];
+    const DGrid& g = Vd.g;
+    const float4 pq = Pq[i];
+    const float4 s4 = S[i];
+    NodeState st;
+    st.p[0] = pq.x;
+    st.p[1] = pq.y;
+    st.p[2] = pq.z;
+    st.hn = fabsf(pq.w);
+    st.a = lab[i];
+    st.ty = typ[i];
+    const uint32_t pp = part[i];
+    st.pb = (int)(pp & 0xFFFFu);
+    st.pc = (int)(pp >> 16);
+    const int ty0 = st.ty;
+    float s[3] = { s4.x, s4.y, s4.z };
+    const float m = move_step(g, Vd.hmode, s4.w, s, Vd.maxstep, Vd.snap, Vd.voxmode, st);
+    if (Vd.fire) {
+        const float fdt = c.fdt;
+        Vel[i] = (m > 0.0f && st.ty == ty0)
+                     ? make_float4((st.p[0] - pq.x) / fdt, (st.p[1] - pq.y) / fdt, (st.p[2] - pq.z) / fdt, 0.0f)
+                     : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
-    __syncthreads();
-    const bool uniform = !sh_mixed;
-    if (v >= 0) {
-        const DVol& Vd = vols[v];
-        const VolCtl& c = ctl[v];
-        const DGrid& g = Vd.g;
-        const float4 pq = Pq[i];
-        const float4 s4 = S[i];
-        NodeState st;
-        st.p[0] = pq.x;
-        st.p[1] = pq.y;
-        st.p[2] = pq.z;
-        st.hn = fabsf(pq.w);
-        st.a = lab[i];
-        st.ty = typ[i];
-        const uint32_t pp = part[i];
-        st.pb = (int)(pp & 0xFFFFu);
-        st.pc = (int)(pp >> 16);
-        const int ty0 = st.ty;
-        float s[3] = { s4.x, s4.y, s4.z };
-        const float m = move_step(g, Vd.hmode, s4.w, s, Vd.maxstep, Vd.snap, Vd.voxmode, st);
-        if (Vd.fire) {
-            const float fdt = c.fdt;
-            Vel[i] = (m > 0.0f && st.ty == ty0)
-                         ? make_float4((st.p[0] - pq.x) / fdt, (st.p[1] - pq.y) / fdt, (st.p[2] - pq.z) / fdt, 0.0f)
-                         : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    mvout[i] = m;
+    Pq[i] = make_float4(st.p[0], st.p[1], st.p[2], pack_h(st.hn, st.ty));
+    typ[i] = (uint8_t)st.ty;
+    part[i] = (uint32_t)(st.pb & 0xFFFF) | ((uint32_t)(st.pc & 0xFFFF) << 16);
+    // the iteration's reductions, combined per warp
+    const float4 q0 = P0[i];
+    const float ex = st.p[0] - q0.x, ey = st.p[1] - q0.y, ez = st.p[2] - q0.z;
+    const float hh = st.hn;
+    const float m2 = ex * ex + ey * ey + ez * ez, s2 = Vd.skin * Vd.skin * hh * hh;
+    const int b = hist_bin(m);
+    VolCtl* cv = ctl + v;
+    const unsigned gb = __match_any_sync(act, (unsigned)(v << 5) | (unsigned)b);
+    if (lane == (unsigned)(__ffs(gb) - 1)) {
+        atomicAdd(&cv->hist[b], __popc(gb));
+    }
+    const unsigned gvol = __match_any_sync(act, (unsigned)v);
+    const unsigned leader = (unsigned)(__ffs(gvol) - 1);
+    const unsigned mx = __reduce_max_sync(gvol, __float_as_uint(m));
+    const bool refresh = m2 > s2;
+    const bool half = !refresh && m2 > 0.25f * s2;
+    const unsigned nh = __popc(__ballot_sync(act, half) & gvol);
+    unsigned md = 0u;
+    if (Vd.policy == 1) {
+        md = __reduce_max_sync(gvol, __float_as_uint(sqrtf(m2) / hh));
+    }
+    if (lane == leader) {
+        if (mx) {
+            atomicMax(&cv->maxbits, mx);
         }
-        mvout[i] = m;
-        Pq[i] = make_float4(st.p[0], st.p[1], st.p[2], pack_h(st.hn, st.ty));
-        typ[i] = (uint8_t)st.ty;
-        part[i] = (uint32_t)(st.pb & 0xFFFF) | ((uint32_t)(st.pc & 0xFFFF) << 16);
-        node_tail(Vd, ctl, v, i, m, st.p[0], st.p[1], st.p[2], st.hn, P0, rlist, G, uniform ? &acc : nullptr);
+        if (nh) {
+            atomicAdd(&cv->nhalf, (int)nh);
+        }
+        if (md) {
+            atomicMax(reinterpret_cast<unsigned*>(&cv->pad1), md);
+        }
     }
-    __syncthreads();
-    if (uniform && sh_v0 >= 0) {
-        tail_flush(acc, ctl + sh_v0);
+    if (refresh) {
+        const int e = atomicAdd(&G->nrefresh, 1);
+        rlist[e] = (int)i;
+        atomicAdd(&cv->nrefresh, 1);
     }
 }
 
@@ -1122,7 +1146,7 @@ void launch_move(cudaStream_t s, const Dev& d) {
     k_move_pre<<<nblk(d.N, kMoveThreads), kMoveThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.F, d.Vel, d.typ,
                                                                 d.mv, d.pw, d.P0, d.S, d.queue, d.psum, d.rlist, d.G,
                                                                 d.N);
-    k_move_main<<<nblk(d.N, kMoveThreads), kMoveThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.Vel, d.typ, d.lab,
+    k_move_main<<<nblk(d.N, kMainThreads), kMainThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.Vel, d.typ, d.lab,
                                                                  d.part, d.mv, d.P0, d.S, d.queue, d.rlist, d.G, d.N);
 }
 

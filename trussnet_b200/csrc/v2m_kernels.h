@@ -12,7 +12,8 @@ namespace v2m {
 constexpr int kScanTile = 1024;     // bin entries per scan tile (volume bin ranges are aligned to it)
 constexpr int kScanThreads = 256;
 constexpr int kNbrMaxThreads = 256; // k_neighbors: up to 8 warps per block, one node each
-constexpr int kMoveThreads = 256;   // volume node ranges are aligned to it
+constexpr int kMoveThreads = 256;   // k_move_pre's block; volume node ranges are aligned to it
+constexpr int kMainThreads = 128;   // k_move_main's block
 constexpr int kCtlThreads = 256;
 constexpr int kNodeAlign = kMoveThreads;
 
