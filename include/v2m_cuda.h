@@ -256,6 +256,31 @@ int v2m_unroll_tape(v2m_unroll* u, uint32_t* host, int64_t count);
 int v2m_unroll_timing(v2m_unroll* u, float* ms_forward, float* ms_backward);
 const char* v2m_unroll_last_error(void);
 
+/*
+ * The hash's stable counting sort with no device allocation, for callers that
+ * cannot call cudaMalloc: a process whose GPU memory belongs to its own pool (a
+ * framework's caching allocator, a host application that reserved most of the
+ * device), where a library allocation can fail or fragment the pool and
+ * cudaFree would synchronize the whole device. No counterpart in the
+ * reference.
+ *
+ * key: DEVICE int32[n], each in [0, nbins); outputs, DEVICE buffers of the
+ * caller: sorted int32[n] (node ids by (key, id)) and cstart int32[nbins + 1]
+ * (bin starts) -- what the hash build produces (v2m_session_read_array's
+ * V2M_ARR_SORTED / V2M_ARR_CSTART). stream: a cudaStream_t, NULL for the legacy
+ * default stream; the call returns when the sort is done.
+ *
+ * Scratch is a fixed array in the library's device memory (about 8 MB, on every
+ * GPU that loads the library, until exit): nbins is limited to
+ * V2M_NOALLOC_MAX_BINS, larger requests return V2M_ERR_ARG. Its device address
+ * is looked up on the first call made on each device (call once before any
+ * stream capture). Calls share the array: calls that overlap on the GPU race.
+ */
+#define V2M_NOALLOC_MAX_BINS (1 << 20)
+int v2m_bin_sort_noalloc(const int32_t* key, int64_t n, int64_t nbins, int32_t* sorted, int32_t* cstart,
+                         void* stream);
+const char* v2m_bin_sort_noalloc_error(void);
+
 #ifdef __cplusplus
 }
 #endif
