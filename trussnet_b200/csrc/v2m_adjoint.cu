@@ -17,10 +17,12 @@
 // Loss: sum over every list entry (i, j) of (l_ij / hm_ij - 1)^2, hm = (h_i+h_j)/2.
 //
 // Reverse mode with checkpoints every `ckpt` steps: the backward pass recomputes
-// each segment's states from its checkpoint, then walks it backwards. Gradient
-// contributions that scatter (to a neighbour j, to the 8 corners of G) are
-// added as 64-bit fixed point (2^-32) with integer atomics, which are exact
-// and associative: the gradients are bit-identical run to run.
+// each segment's states (and sizes) from its checkpoint, then walks it
+// backwards. Each node gathers the reverse terms of its own bars and of the bars
+// pointing at it (the lists' transpose, built once), in a fixed order, in
+// double; the sizing grid's 8-corner contributions are added as 64-bit fixed
+// point (2^-32) with integer atomics, exact and associative. The gradients are
+// bit-identical run to run.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -221,110 +223,154 @@ __global__ void k_loss(const float4* __restrict__ x, const float* __restrict__ h
     }
 }
 
-__global__ void k_loss_bwd(const float4* __restrict__ x, const float* __restrict__ h, const int* __restrict__ nbr,
-                           const uint8_t* __restrict__ nnb, float gscale, unsigned long long* __restrict__ lam,
-                           unsigned long long* __restrict__ gh, int n) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) {
+// ---- gather form of the reverse passes --------------------------------------------
+// The lists are frozen, so their transpose (for every node j, the entries
+// (i, k) with nbr[i][k] = j, by ascending i then k) is built once. Each node then
+// sums, in a fixed order and in double, the terms of its own bars and of the
+// bars that point at it: no atomics, and the same bits on every run. Only the
+// sizing grid's 8-corner scatter (k_size_bwd_g) stays on fixed-point atomics.
+
+// d(loss)/dx and d(loss)/dh at x (loss = sum over list entries of (l/hm - 1)^2)
+__global__ void k_loss_bwd_g(const float4* __restrict__ x, const float* __restrict__ h, const int* __restrict__ nbr,
+                             const uint8_t* __restrict__ nnb, const int* __restrict__ tofs,
+                             const int* __restrict__ tsrc, float gscale, float4* __restrict__ lam,
+                             float* __restrict__ gh, int n) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) {
         return;
     }
-    const float4 p = x[i];
-    const float hi = h[i];
-    double li[3] = { 0.0, 0.0, 0.0 }, ghi = 0.0;
-    for (int k = 0; k < nnb[i]; ++k) {
-        const int j = __ldg(nbr + (size_t)k * n + i);
-        const float4 q = __ldg(x + j);
-        const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
-        const float l = sqrtf(ex * ex + ey * ey + ez * ez);
-        const float hm = 0.5f * (hi + __ldg(h + j));
+    const float4 pj = x[j];
+    const float hj = h[j];
+    double l3[3] = { 0.0, 0.0, 0.0 }, g = 0.0;
+    // own entries (j -> k): + dl e/l
+    for (int k = 0; k < nnb[j]; ++k) {
+        const int m = __ldg(nbr + (size_t)k * n + j);
+        const float4 q = __ldg(x + m);
+        const float e[3] = { pj.x - q.x, pj.y - q.y, pj.z - q.z };
+        const float l = sqrtf(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+        const float hm = 0.5f * (hj + __ldg(h + m));
         const float r = l / hm - 1.0f;
         const float dl = gscale * 2.0f * r / hm, dhm = -gscale * 2.0f * r * l / (hm * hm);
-        const float e[3] = { ex / l, ey / l, ez / l };
         for (int d = 0; d < 3; ++d) {
-            li[d] += (double)(dl * e[d]);
-            fx_add(lam + 3 * (size_t)j + d, -(double)(dl * e[d]));
+            l3[d] += (double)(dl * (e[d] / l));
         }
-        ghi += 0.5 * (double)dhm;
-        fx_add(gh + j, 0.5 * (double)dhm);
+        g += 0.5 * (double)dhm;
     }
-    for (int d = 0; d < 3; ++d) {
-        fx_add(lam + 3 * (size_t)i + d, li[d]);
+    // entries pointing at j (i -> j): - dl e/l
+    for (int t = tofs[j]; t < tofs[j + 1]; ++t) {
+        const int i = __ldg(tsrc + t);
+        const float4 pi = __ldg(x + i);
+        const float e[3] = { pi.x - pj.x, pi.y - pj.y, pi.z - pj.z };
+        const float l = sqrtf(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+        const float hm = 0.5f * (__ldg(h + i) + hj);
+        const float r = l / hm - 1.0f;
+        const float dl = gscale * 2.0f * r / hm, dhm = -gscale * 2.0f * r * l / (hm * hm);
+        for (int d = 0; d < 3; ++d) {
+            l3[d] -= (double)(dl * (e[d] / l));
+        }
+        g += 0.5 * (double)dhm;
     }
-    fx_add(gh + i, ghi);
+    lam[j] = make_float4((float)l3[0], (float)l3[1], (float)l3[2], 0.0f);
+    gh[j] = (float)g;
 }
 
-// reverse of one step: lam_in = dL/dx_{t+1}; accumulates dL/dx_t and dL/dh_t
-__global__ void k_step_bwd(const float4* __restrict__ x, const float* __restrict__ h, const int* __restrict__ nbr,
-                           const uint8_t* __restrict__ nnb, const uint8_t* __restrict__ typ, float fscale, float fsurf,
-                           float dt, const uint32_t* __restrict__ mask, const float4* __restrict__ lam_in,
-                           unsigned long long* __restrict__ lam, unsigned long long* __restrict__ gh, int n) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) {
+// one bar's reverse terms: v = (d phi / d e)^T mu and s = (e . mu) / l
+__device__ __forceinline__ void bar_vjp(const float* e, float l0, float a, const float* mu, float* v, float* sa) {
+    const float l = sqrtf(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+    const float f = (l0 - l) / l, dfl = -l0 / (l * l);
+    const float em = e[0] * mu[0] + e[1] * mu[1] + e[2] * mu[2];
+    for (int d = 0; d < 3; ++d) {
+        v[d] = f * mu[d] + e[d] / l * dfl * em;
+    }
+    *sa = a * (em / l);
+}
+
+// reverse of one step: lam_in = dL/dx_{t+1} -> lam_out (before the size term), gh = dL/dh_t
+__global__ void k_step_bwd_g(const float4* __restrict__ x, const float* __restrict__ h, const int* __restrict__ nbr,
+                             const uint8_t* __restrict__ nnb, const uint8_t* __restrict__ typ, float fscale,
+                             float fsurf, float dt, const uint32_t* __restrict__ mask, const float4* __restrict__ lam_in,
+                             const int* __restrict__ tofs, const int* __restrict__ tsrc,
+                             const uint8_t* __restrict__ tslot, float4* __restrict__ lam_out, float* __restrict__ gh,
+                             int n) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) {
         return;
     }
-    const float4 li4 = lam_in[i];
-    double li[3] = { (double)li4.x, (double)li4.y, (double)li4.z }, ghi = 0.0;
-    const int ti = typ[i];
-    if (ti != V2M_CORNER) {
-        const float4 p = x[i];
-        const float hi = h[i];
-        const uint32_t bits = mask[i];
+    const float4 lj = lam_in[j];
+    double l3[3] = { (double)lj.x, (double)lj.y, (double)lj.z }, g = 0.0;
+    const float4 pj = x[j];
+    const float hj = h[j];
+    const int tj = typ[j];
+    if (tj != V2M_CORNER) {
+        const uint32_t bits = mask[j];
         const int act = __popc(bits);
         const float s = dt / (float)(act > 1 ? act : 1);
-        const float mu[3] = { s * li4.x, s * li4.y, s * li4.z };
-        for (int k = 0; k < nnb[i]; ++k) {
+        const float mu[3] = { s * lj.x, s * lj.y, s * lj.z };
+        for (int k = 0; k < nnb[j]; ++k) {
             if (!((bits >> k) & 1u)) {
                 continue;
             }
-            const int j = __ldg(nbr + (size_t)k * n + i);
-            const float4 q = __ldg(x + j);
-            const float e[3] = { p.x - q.x, p.y - q.y, p.z - q.z };
-            const float l = sqrtf(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
-            const float a = ((ti != V2M_INTERIOR && typ[j] != V2M_INTERIOR) ? fsurf : fscale) * 0.5f;
-            const float l0 = a * (hi + __ldg(h + j));
-            const float f = (l0 - l) / l, dfl = -l0 / (l * l);
-            const float em = e[0] * mu[0] + e[1] * mu[1] + e[2] * mu[2];
+            const int m = __ldg(nbr + (size_t)k * n + j);
+            const float4 q = __ldg(x + m);
+            const float e[3] = { pj.x - q.x, pj.y - q.y, pj.z - q.z };
+            const float a = ((tj != V2M_INTERIOR && typ[m] != V2M_INTERIOR) ? fsurf : fscale) * 0.5f;
+            const float l0 = a * (hj + __ldg(h + m));
+            float v[3], sa;
+            bar_vjp(e, l0, a, mu, v, &sa);
             for (int d = 0; d < 3; ++d) {
-                const float v = f * mu[d] + e[d] / l * dfl * em;
-                li[d] += (double)v;
-                fx_add(lam + 3 * (size_t)j + d, -(double)v);
+                l3[d] += (double)v[d];
             }
-            const double sa = (double)(a * (em / l));
-            ghi += sa;
-            fx_add(gh + j, sa);
+            g += (double)sa;
         }
     }
-    for (int d = 0; d < 3; ++d) {
-        fx_add(lam + 3 * (size_t)i + d, li[d]);
+    for (int t = tofs[j]; t < tofs[j + 1]; ++t) {
+        const int i = __ldg(tsrc + t);
+        const int k = __ldg(tslot + t);
+        const int ti = typ[i];
+        const uint32_t bi = __ldg(mask + i);
+        if (ti == V2M_CORNER || !((bi >> k) & 1u)) {
+            continue;
+        }
+        const float4 li = __ldg(lam_in + i);
+        const int act = __popc(bi);
+        const float s = dt / (float)(act > 1 ? act : 1);
+        const float mu[3] = { s * li.x, s * li.y, s * li.z };
+        const float4 pi = __ldg(x + i);
+        const float e[3] = { pi.x - pj.x, pi.y - pj.y, pi.z - pj.z };
+        const float a = ((ti != V2M_INTERIOR && tj != V2M_INTERIOR) ? fsurf : fscale) * 0.5f;
+        const float l0 = a * (__ldg(h + i) + hj);
+        float v[3], sa;
+        bar_vjp(e, l0, a, mu, v, &sa);
+        for (int d = 0; d < 3; ++d) {
+            l3[d] -= (double)v[d];
+        }
+        g += (double)sa;
     }
-    fx_add(gh + i, ghi);
+    lam_out[j] = make_float4((float)l3[0], (float)l3[1], (float)l3[2], 0.0f);
+    gh[j] = (float)g;
 }
 
-// dL/dh into dL/dx (own) and dL/dG (8 corners), then the float adjoint, buffers cleared
-__global__ void k_size_bwd(Dims D, const float* __restrict__ G, const float4* __restrict__ x,
-                           unsigned long long* __restrict__ gh, unsigned long long* __restrict__ lam,
-                           unsigned long long* __restrict__ gG, float4* __restrict__ lam_out, int n) {
+// lam += gh dH/dx (own node), gG += gh w (8 corners, fixed-point atomics)
+__global__ void k_size_bwd_g(Dims D, const float* __restrict__ G, const float4* __restrict__ x,
+                             const float* __restrict__ gh, float4* __restrict__ lam,
+                             unsigned long long* __restrict__ gG, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) {
         return;
     }
-    const double g = fx_get(gh[i]);
-    gh[i] = 0ull;
-    double l3[3] = { fx_get(lam[3 * (size_t)i]), fx_get(lam[3 * (size_t)i + 1]), fx_get(lam[3 * (size_t)i + 2]) };
-    lam[3 * (size_t)i] = lam[3 * (size_t)i + 1] = lam[3 * (size_t)i + 2] = 0ull;
-    if (g != 0.0) {
-        const float4 p = x[i];
-        float gr[3], w[8];
-        int idx[8];
-        size_at(D, G, p.x, p.y, p.z, gr, idx, w);
-        for (int d = 0; d < 3; ++d) {
-            l3[d] += g * (double)gr[d];
-        }
-        for (int k = 0; k < 8; ++k) {
-            fx_add(gG + idx[k], g * (double)w[k]);
-        }
+    const float g = gh[i];
+    if (g == 0.0f) {
+        return;
     }
-    lam_out[i] = make_float4((float)l3[0], (float)l3[1], (float)l3[2], 0.0f);
+    const float4 p = x[i];
+    float gr[3], w[8];
+    int idx[8];
+    size_at(D, G, p.x, p.y, p.z, gr, idx, w);
+    const float4 l = lam[i];
+    lam[i] = make_float4(l.x + g * gr[0], l.y + g * gr[1], l.z + g * gr[2], 0.0f);
+    for (int k = 0; k < 8; ++k) {
+        fx_add(gG + idx[k], (double)g * (double)w[k]);
+    }
 }
 
 __global__ void k_fix_to_float(unsigned long long* __restrict__ a, float* __restrict__ out, int m, int clear) {
@@ -368,10 +414,14 @@ struct v2m_unroll {
     float4* seg = nullptr;           // (ckpt + 1) x n segment states
     float* h = nullptr;
     float4* lamf = nullptr;
-    unsigned long long* lam = nullptr;
-    unsigned long long* gh = nullptr;
     unsigned long long* gG = nullptr;
     double* part = nullptr;
+    int* tofs = nullptr;             // transpose of the lists: n + 1 offsets
+    int* tsrc = nullptr;             // source node i of each incoming entry
+    uint8_t* tslot = nullptr;        // its slot k in i's list
+    float4* lamb = nullptr;          // second adjoint buffer
+    float* ghf = nullptr;            // dL/dh per node
+    float* hseg = nullptr;           // h of each state of a segment
     int have_tape = 0;
     float ms_fwd = 0.0f, ms_bwd = 0.0f;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -430,13 +480,16 @@ unsigned blocks(int n) {
 
 // forward over steps [t0, t1) from x (float4), writing states to out[t - t0 + 1]
 // (out may be null: only the last state is kept in `last`)
-void run_steps(v2m_unroll* u, const float* G, const float4* x, int t0, int t1, float4* seg, int replay) {
+// (the size of every state goes to hseg[t - t0] when hseg is given, else to u->h)
+void run_steps(v2m_unroll* u, const float* G, const float4* x, int t0, int t1, float4* seg, int replay,
+               float* hseg = nullptr) {
     const int n = u->n;
     const float4* cur = x;
     for (int t = t0; t < t1; ++t) {
         float4* nxt = seg + (size_t)(t - t0 + 1) * n;
-        k_size<<<blocks(n), kT, 0, u->stream>>>(u->D, G, cur, u->h, n);
-        k_step<<<blocks(n), kT, 0, u->stream>>>(cur, u->h, u->nbr, u->nnb, u->typ, u->fscale, u->fsurf, u->dt,
+        float* h = hseg ? hseg + (size_t)(t - t0) * n : u->h;
+        k_size<<<blocks(n), kT, 0, u->stream>>>(u->D, G, cur, h, n);
+        k_step<<<blocks(n), kT, 0, u->stream>>>(cur, h, u->nbr, u->nnb, u->typ, u->fscale, u->fsurf, u->dt,
                                                 u->tape + (size_t)t * n, replay, nxt, n);
         cur = nxt;
     }
@@ -500,18 +553,43 @@ int v2m_unroll_create(int64_t n, const int32_t* nbr, const int32_t* nnb, const u
             u->seg = u->alloc<float4>(nn * (ckpt + 1));
             u->h = u->alloc<float>(nn);
             u->lamf = u->alloc<float4>(nn);
-            u->lam = u->alloc<unsigned long long>(3 * nn);
-            u->gh = u->alloc<unsigned long long>(nn);
             u->gG = u->alloc<unsigned long long>((size_t)m[0] * m[1] * m[2]);
             u->part = u->alloc<double>(nn / kT + 1);
+            u->lamb = u->alloc<float4>(nn);
+            u->ghf = u->alloc<float>(nn);
+            u->hseg = u->alloc<float>(nn * (ckpt + 1));
+            // the transpose of the lists: incoming entries of every node, by (i, k)
+            std::vector<int> tofs(nn + 1, 0);
+            for (int64_t i = 0; i < n; ++i) {
+                for (int k = 0; k < nnb[i]; ++k) {
+                    ++tofs[nbr[i * V2M_K + k] + 1];
+                }
+            }
+            for (size_t j = 0; j < nn; ++j) {
+                tofs[j + 1] += tofs[j];
+            }
+            std::vector<int> cur(tofs.begin(), tofs.end() - 1), tsrc(std::max(tofs[nn], 1));
+            std::vector<uint8_t> tslot(std::max(tofs[nn], 1));
+            for (int64_t i = 0; i < n; ++i) {
+                for (int k = 0; k < nnb[i]; ++k) {
+                    const int j = nbr[i * V2M_K + k];
+                    tsrc[cur[j]] = (int)i;
+                    tslot[cur[j]] = (uint8_t)k;
+                    ++cur[j];
+                }
+            }
+            u->tofs = u->alloc<int>(nn + 1);
+            u->tsrc = u->alloc<int>(tsrc.size());
+            u->tslot = u->alloc<uint8_t>(tslot.size());
+            uck(cudaMemcpy(u->tofs, tofs.data(), 4 * (nn + 1), cudaMemcpyHostToDevice), "upload");
+            uck(cudaMemcpy(u->tsrc, tsrc.data(), 4 * tsrc.size(), cudaMemcpyHostToDevice), "upload");
+            uck(cudaMemcpy(u->tslot, tslot.data(), tslot.size(), cudaMemcpyHostToDevice), "upload");
             int* tmp = u->alloc<int>(nn * V2M_K + nn);
             uck(cudaMemcpyAsync(tmp, nbr, 4 * nn * V2M_K, cudaMemcpyHostToDevice, u->stream), "upload");
             uck(cudaMemcpyAsync(tmp + nn * V2M_K, nnb, 4 * nn, cudaMemcpyHostToDevice, u->stream), "upload");
             uck(cudaMemcpyAsync(u->typ, typ, nn, cudaMemcpyHostToDevice, u->stream), "upload");
             k_lists<<<(unsigned)((nn * V2M_K + kT - 1) / kT), kT, 0, u->stream>>>(tmp, tmp + nn * V2M_K, u->nbr, u->nnb,
                                                                                (int)n);
-            uck(cudaMemsetAsync(u->lam, 0, 8 * 3 * nn, u->stream), "memset");
-            uck(cudaMemsetAsync(u->gh, 0, 8 * nn, u->stream), "memset");
             uck(cudaMemsetAsync(u->gG, 0, 8 * (size_t)m[0] * m[1] * m[2], u->stream), "memset");
             uck(cudaGetLastError(), "launch");
             uck(cudaStreamSynchronize(u->stream), "synchronize");
@@ -599,8 +677,9 @@ int v2m_unroll_loss_backward(v2m_unroll* u, const float* x, const float* G, floa
         if (!accumulate) {
             uck(cudaMemsetAsync(u->gG, 0, 8 * (size_t)mg, u->stream), "memset");
         }
-        k_loss_bwd<<<blocks(n), kT, 0, u->stream>>>(x4, u->h, u->nbr, u->nnb, gscale, u->lam, u->gh, n);
-        k_size_bwd<<<blocks(n), kT, 0, u->stream>>>(u->D, G, x4, u->gh, u->lam, u->gG, u->lamf, n);
+        k_loss_bwd_g<<<blocks(n), kT, 0, u->stream>>>(x4, u->h, u->nbr, u->nnb, u->tofs, u->tsrc, gscale, u->lamf,
+                                                      u->ghf, n);
+        k_size_bwd_g<<<blocks(n), kT, 0, u->stream>>>(u->D, G, x4, u->ghf, u->lamf, u->gG, n);
         k_unpack<<<blocks(n), kT, 0, u->stream>>>(u->lamf, gx, n);
         k_fix_to_float<<<blocks(mg), kT, 0, u->stream>>>(u->gG, gG, mg, 0);
         uck(cudaGetLastError(), "launch");
@@ -628,13 +707,18 @@ int v2m_unroll_backward(v2m_unroll* u, const float* G, const float* gxK, float* 
             // recompute the segment's states from its checkpoint (replaying the tape)
             uck(cudaMemcpyAsync(u->seg, u->ck + (size_t)c * n, 16 * (size_t)n, cudaMemcpyDeviceToDevice, u->stream),
                 "segment");
-            run_steps(u, G, u->seg, t0, t1 - 1, u->seg, 1);
+            run_steps(u, G, u->seg, t0, t1 - 1, u->seg, 1, u->hseg);
+            // the last state's size (run_steps stops before its step)
+            k_size<<<blocks(n), kT, 0, u->stream>>>(u->D, G, u->seg + (size_t)(t1 - 1 - t0) * n,
+                                                    u->hseg + (size_t)(t1 - 1 - t0) * n, n);
             for (int t = t1 - 1; t >= t0; --t) {
                 const float4* xt = u->seg + (size_t)(t - t0) * n;
-                k_size<<<blocks(n), kT, 0, u->stream>>>(u->D, G, xt, u->h, n);
-                k_step_bwd<<<blocks(n), kT, 0, u->stream>>>(xt, u->h, u->nbr, u->nnb, u->typ, u->fscale, u->fsurf,
-                                                            u->dt, u->tape + (size_t)t * n, u->lamf, u->lam, u->gh, n);
-                k_size_bwd<<<blocks(n), kT, 0, u->stream>>>(u->D, G, xt, u->gh, u->lam, u->gG, u->lamf, n);
+                const float* ht = u->hseg + (size_t)(t - t0) * n;
+                k_step_bwd_g<<<blocks(n), kT, 0, u->stream>>>(xt, ht, u->nbr, u->nnb, u->typ, u->fscale, u->fsurf,
+                                                              u->dt, u->tape + (size_t)t * n, u->lamf, u->tofs,
+                                                              u->tsrc, u->tslot, u->lamb, u->ghf, n);
+                k_size_bwd_g<<<blocks(n), kT, 0, u->stream>>>(u->D, G, xt, u->ghf, u->lamb, u->gG, n);
+                std::swap(u->lamf, u->lamb);
             }
         }
         k_unpack<<<blocks(n), kT, 0, u->stream>>>(u->lamf, gx0, n);
