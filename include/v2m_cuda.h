@@ -224,6 +224,8 @@ int v2m_session_clear_counters(v2m_session* s);
  * ms[2] control + self-refresh, ms[3] the rebuild stages, ms[4] the iterations.
  */
 int v2m_session_profile_stages(v2m_session* s, int iters, double* ms);
+/* Nodes the last iteration's move handed to the trapped-move stage: non-INTERIOR and INTERIOR ones. */
+int v2m_session_queue_sizes(v2m_session* s, int32_t* trapped, int32_t* interior);
 
 /*
  * The differentiable relaxation unroll and its adjoint (no counterpart in the

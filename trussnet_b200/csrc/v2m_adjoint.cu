@@ -230,11 +230,30 @@ __global__ void k_loss(const float4* __restrict__ x, const float* __restrict__ h
 // bars that point at it: no atomics, and the same bits on every run. Only the
 // sizing grid's 8-corner scatter (k_size_bwd_g) stays on fixed-point atomics.
 
+// the size term of node j, in the same thread that summed dL/dh_j: lam_j +=
+// dL/dh_j dH/dx_j, and the grid's 8 corners get dL/dh_j w (fixed-point atomics)
+__device__ __forceinline__ void size_tail(const Dims& D, const float* __restrict__ G, const float4& p, double gh,
+                                          double* l3, unsigned long long* __restrict__ gG) {
+    const float g = (float)gh;
+    if (g == 0.0f) {
+        return;
+    }
+    float gr[3], w[8];
+    int idx[8];
+    size_at(D, G, p.x, p.y, p.z, gr, idx, w);
+    for (int d = 0; d < 3; ++d) {
+        l3[d] += (double)(g * gr[d]);
+    }
+    for (int k = 0; k < 8; ++k) {
+        fx_add(gG + idx[k], (double)g * (double)w[k]);
+    }
+}
+
 // d(loss)/dx and d(loss)/dh at x (loss = sum over list entries of (l/hm - 1)^2)
-__global__ void k_loss_bwd_g(const float4* __restrict__ x, const float* __restrict__ h, const int* __restrict__ nbr,
-                             const uint8_t* __restrict__ nnb, const int* __restrict__ tofs,
-                             const int* __restrict__ tsrc, float gscale, float4* __restrict__ lam,
-                             float* __restrict__ gh, int n) {
+__global__ void k_loss_bwd_g(Dims D, const float* __restrict__ G, const float4* __restrict__ x,
+                             const float* __restrict__ h, const int* __restrict__ nbr, const uint8_t* __restrict__ nnb,
+                             const int* __restrict__ tofs, const int* __restrict__ tsrc, float gscale,
+                             float4* __restrict__ lam, unsigned long long* __restrict__ gG, int n) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) {
         return;
@@ -270,8 +289,8 @@ __global__ void k_loss_bwd_g(const float4* __restrict__ x, const float* __restri
         }
         g += 0.5 * (double)dhm;
     }
+    size_tail(D, G, pj, g, l3, gG);
     lam[j] = make_float4((float)l3[0], (float)l3[1], (float)l3[2], 0.0f);
-    gh[j] = (float)g;
 }
 
 // one bar's reverse terms: v = (d phi / d e)^T mu and s = (e . mu) / l
@@ -286,12 +305,13 @@ __device__ __forceinline__ void bar_vjp(const float* e, float l0, float a, const
 }
 
 // reverse of one step: lam_in = dL/dx_{t+1} -> lam_out (before the size term), gh = dL/dh_t
-__global__ void k_step_bwd_g(const float4* __restrict__ x, const float* __restrict__ h, const int* __restrict__ nbr,
-                             const uint8_t* __restrict__ nnb, const uint8_t* __restrict__ typ, float fscale,
-                             float fsurf, float dt, const uint32_t* __restrict__ mask, const float4* __restrict__ lam_in,
+__global__ void k_step_bwd_g(Dims D, const float* __restrict__ G, const float4* __restrict__ x,
+                             const float* __restrict__ h, const int* __restrict__ nbr, const uint8_t* __restrict__ nnb,
+                             const uint8_t* __restrict__ typ, float fscale, float fsurf, float dt,
+                             const uint32_t* __restrict__ mask, const float4* __restrict__ lam_in,
                              const int* __restrict__ tofs, const int* __restrict__ tsrc,
-                             const uint8_t* __restrict__ tslot, float4* __restrict__ lam_out, float* __restrict__ gh,
-                             int n) {
+                             const uint8_t* __restrict__ tslot, float4* __restrict__ lam_out,
+                             unsigned long long* __restrict__ gG, int n) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) {
         return;
@@ -346,31 +366,8 @@ __global__ void k_step_bwd_g(const float4* __restrict__ x, const float* __restri
         }
         g += (double)sa;
     }
+    size_tail(D, G, pj, g, l3, gG);
     lam_out[j] = make_float4((float)l3[0], (float)l3[1], (float)l3[2], 0.0f);
-    gh[j] = (float)g;
-}
-
-// lam += gh dH/dx (own node), gG += gh w (8 corners, fixed-point atomics)
-__global__ void k_size_bwd_g(Dims D, const float* __restrict__ G, const float4* __restrict__ x,
-                             const float* __restrict__ gh, float4* __restrict__ lam,
-                             unsigned long long* __restrict__ gG, int n) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) {
-        return;
-    }
-    const float g = gh[i];
-    if (g == 0.0f) {
-        return;
-    }
-    const float4 p = x[i];
-    float gr[3], w[8];
-    int idx[8];
-    size_at(D, G, p.x, p.y, p.z, gr, idx, w);
-    const float4 l = lam[i];
-    lam[i] = make_float4(l.x + g * gr[0], l.y + g * gr[1], l.z + g * gr[2], 0.0f);
-    for (int k = 0; k < 8; ++k) {
-        fx_add(gG + idx[k], (double)g * (double)w[k]);
-    }
 }
 
 __global__ void k_fix_to_float(unsigned long long* __restrict__ a, float* __restrict__ out, int m, int clear) {
@@ -420,7 +417,6 @@ struct v2m_unroll {
     int* tsrc = nullptr;             // source node i of each incoming entry
     uint8_t* tslot = nullptr;        // its slot k in i's list
     float4* lamb = nullptr;          // second adjoint buffer
-    float* ghf = nullptr;            // dL/dh per node
     float* hseg = nullptr;           // h of each state of a segment
     int have_tape = 0;
     float ms_fwd = 0.0f, ms_bwd = 0.0f;
@@ -556,7 +552,6 @@ int v2m_unroll_create(int64_t n, const int32_t* nbr, const int32_t* nnb, const u
             u->gG = u->alloc<unsigned long long>((size_t)m[0] * m[1] * m[2]);
             u->part = u->alloc<double>(nn / kT + 1);
             u->lamb = u->alloc<float4>(nn);
-            u->ghf = u->alloc<float>(nn);
             u->hseg = u->alloc<float>(nn * (ckpt + 1));
             // the transpose of the lists: incoming entries of every node, by (i, k)
             std::vector<int> tofs(nn + 1, 0);
@@ -677,9 +672,8 @@ int v2m_unroll_loss_backward(v2m_unroll* u, const float* x, const float* G, floa
         if (!accumulate) {
             uck(cudaMemsetAsync(u->gG, 0, 8 * (size_t)mg, u->stream), "memset");
         }
-        k_loss_bwd_g<<<blocks(n), kT, 0, u->stream>>>(x4, u->h, u->nbr, u->nnb, u->tofs, u->tsrc, gscale, u->lamf,
-                                                      u->ghf, n);
-        k_size_bwd_g<<<blocks(n), kT, 0, u->stream>>>(u->D, G, x4, u->ghf, u->lamf, u->gG, n);
+        k_loss_bwd_g<<<blocks(n), kT, 0, u->stream>>>(u->D, G, x4, u->h, u->nbr, u->nnb, u->tofs, u->tsrc, gscale,
+                                                      u->lamf, u->gG, n);
         k_unpack<<<blocks(n), kT, 0, u->stream>>>(u->lamf, gx, n);
         k_fix_to_float<<<blocks(mg), kT, 0, u->stream>>>(u->gG, gG, mg, 0);
         uck(cudaGetLastError(), "launch");
@@ -714,10 +708,9 @@ int v2m_unroll_backward(v2m_unroll* u, const float* G, const float* gxK, float* 
             for (int t = t1 - 1; t >= t0; --t) {
                 const float4* xt = u->seg + (size_t)(t - t0) * n;
                 const float* ht = u->hseg + (size_t)(t - t0) * n;
-                k_step_bwd_g<<<blocks(n), kT, 0, u->stream>>>(xt, ht, u->nbr, u->nnb, u->typ, u->fscale, u->fsurf,
-                                                              u->dt, u->tape + (size_t)t * n, u->lamf, u->tofs,
-                                                              u->tsrc, u->tslot, u->lamb, u->ghf, n);
-                k_size_bwd_g<<<blocks(n), kT, 0, u->stream>>>(u->D, G, xt, u->ghf, u->lamb, u->gG, n);
+                k_step_bwd_g<<<blocks(n), kT, 0, u->stream>>>(u->D, G, xt, ht, u->nbr, u->nnb, u->typ, u->fscale,
+                                                              u->fsurf, u->dt, u->tape + (size_t)t * n, u->lamf,
+                                                              u->tofs, u->tsrc, u->tslot, u->lamb, u->gG, n);
                 std::swap(u->lamf, u->lamb);
             }
         }

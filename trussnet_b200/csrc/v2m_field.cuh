@@ -123,14 +123,92 @@ __device__ __forceinline__ float trilerp8(const float* c, float fx, float fy, fl
     return y0 + fz * (y1 - y0);
 }
 
+// The trilinear cell under a point, computed once and shared by every label
+// evaluated there: corner voxel, fractions and -- when the cell lies inside one
+// brick (v2m_phi_cell's fast case) -- that brick's label count, labels and
+// first slot. cell_phi gives exactly the corners v2m_phi_cell gives
+// (src/opencl/v2m_grid_body.cl:159-186), so the values are the reference's.
+struct Cell {
+    int i0, j0, k0;
+    float fx, fy, fz;
+    int fast;
+    int n, first;
+    LabList ll;
+};
+
+__device__ __forceinline__ void cell_at(const DGrid& g, float px, float py, float pz, Cell& c) {
+    const float u = px / g.vx, v = py / g.vy, w = pz / g.vz;
+    c.i0 = (int)floorf(u);
+    c.j0 = (int)floorf(v);
+    c.k0 = (int)floorf(w);
+    c.fx = u - c.i0;
+    c.fy = v - c.j0;
+    c.fz = w - c.k0;
+    c.fast = c.i0 >= 0 && c.j0 >= 0 && c.k0 >= 0 && c.i0 + 1 < g.nx && c.j0 + 1 < g.ny && c.k0 + 1 < g.nz &&
+             (c.i0 & 7) != 7 && (c.j0 & 7) != 7 && (c.k0 & 7) != 7;
+    if (c.fast) {
+        const int b = brick_index(g, c.i0, c.j0, c.k0);
+        c.n = __ldg(g.bl_cnt + b);
+        c.ll = load_labels(g, b);
+        c.first = __ldg(g.bl_slot + b);
+    } else {
+        c.n = 0;
+        c.first = -1;
+    }
+}
+
+// index of label l among the first n of a brick's labels, -1 if absent
+__device__ __forceinline__ int lab_index(const LabList& ll, int n, int l) {
+    const unsigned pat = (unsigned)(l & 0xFFFF) * 0x00010001u;
+    unsigned bits = 0u;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+        const unsigned m = __vcmpeq2(ll.w[w], pat);
+        bits |= ((m & 1u) | ((m >> 15) & 2u)) << (2 * w);
+    }
+    const int nn = n < V2M_BL ? n : V2M_BL;
+    bits &= (1u << nn) - 1u;
+    return bits ? __ffs(bits) - 1 : -1;
+}
+
+// the 8 corners of phi_l in the cell
+__device__ __forceinline__ void cell_corners(const DGrid& g, const Cell& c, int l, float* out) {
+    if (c.fast) {
+        const int idx = lab_index(c.ll, c.n, l);
+        if (idx >= 0 && c.first >= 0) {
+            const float* base = g.phi + (size_t)(c.first + idx) * V2M_SLOT + (c.i0 & 7) +
+                                V2M_BS * ((c.j0 & 7) + V2M_BS * (c.k0 & 7));
+#pragma unroll
+            for (int n = 0; n < 8; ++n) {
+                out[n] = __ldg(base + (n & 1) + V2M_BS * ((n >> 1) & 1) + V2M_BS * V2M_BS * (n >> 2));
+            }
+        } else {
+#pragma unroll
+            for (int n = 0; n < 8; ++n) {
+                out[n] = (idx >= 0 && g.L[(c.i0 + (n & 1)) + (size_t)g.nx * ((c.j0 + ((n >> 1) & 1)) +
+                                                                          (size_t)g.ny * (c.k0 + (n >> 2)))] == l)
+                             ? 1.0f : 0.0f;
+            }
+        }
+        return;
+    }
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+        out[n] = phi_voxel(g, l, c.i0 + (n & 1), c.j0 + ((n >> 1) & 1), c.k0 + ((n >> 2) & 1));
+    }
+}
+
+__device__ __forceinline__ float cell_phi(const DGrid& g, const Cell& c, int l) {
+    float v[8];
+    cell_corners(g, c, l, v);
+    return trilerp8(v, c.fx, c.fy, c.fz);
+}
+
 // phi_l trilinear at p (src/opencl/v2m_grid_body.cl:189-200)
 __device__ __noinline__ float phi_point(const DGrid& g, int l, float px, float py, float pz) {
-    const float u = px / g.vx, v = py / g.vy, w = pz / g.vz;
-    const int i0 = (int)floorf(u), j0 = (int)floorf(v), k0 = (int)floorf(w);
-    const float fx = u - i0, fy = v - j0, fz = w - k0;
-    float c[8];
-    phi_corners(g, l, i0, j0, k0, c);
-    return trilerp8(c, fx, fy, fz);
+    Cell c;
+    cell_at(g, px, py, pz, c);
+    return cell_phi(g, c, l);
 }
 
 // The labels that may appear at p: its brick's list (src/opencl/v2m_seed_body.cl:42-59).
@@ -218,10 +296,12 @@ __device__ __forceinline__ int owner_label(const DGrid& g, int voxmode, float px
         *margin = 1.0f;
         return best;
     }
+    Cell cl;
+    cell_at(g, px, py, pz, cl);
 #pragma unroll 1
     for (int s = 0; s < n; ++s) {
         const int ls = ll.get(s);
-        const float v = phi_point(g, ls, px, py, pz);
+        const float v = cell_phi(g, cl, ls);
         if (v > pb) {
             ps = pb;
             sec = best;
@@ -246,17 +326,16 @@ __device__ __noinline__ float psi(const DGrid& g, int a, int b, float px, float 
     if (gray_psi(g, a, b, px, py, pz, &gv, nullptr)) {
         return gv;
     }
-    const float u = px / g.vx, v = py / g.vy, w = pz / g.vz;
-    const int i0 = (int)floorf(u), j0 = (int)floorf(v), k0 = (int)floorf(w);
-    const float fx = u - i0, fy = v - j0, fz = w - k0;
+    Cell cl;
+    cell_at(g, px, py, pz, cl);
     float c[8], e[8];
-    phi_corners(g, a, i0, j0, k0, c);
-    phi_corners(g, b, i0, j0, k0, e);
+    cell_corners(g, cl, a, c);
+    cell_corners(g, cl, b, e);
 #pragma unroll
     for (int n = 0; n < 8; ++n) {
         c[n] -= e[n];
     }
-    return trilerp8(c, fx, fy, fz);
+    return trilerp8(c, cl.fx, cl.fy, cl.fz);
 }
 
 // psi_ab and its cell-analytic gradient (src/opencl/v2m_seed_body.cl:211-247)
@@ -266,12 +345,12 @@ __device__ __noinline__ float4 psi_grad4(const DGrid& g, int a, int b, float px,
     if (gray_psi(g, a, b, px, py, pz, &gv, gr)) {
         return make_float4(gr[0], gr[1], gr[2], gv);
     }
-    const float u = px / g.vx, v = py / g.vy, w = pz / g.vz;
-    const int i0 = (int)floorf(u), j0 = (int)floorf(v), k0 = (int)floorf(w);
-    const float fx = u - i0, fy = v - j0, fz = w - k0;
+    Cell cl;
+    cell_at(g, px, py, pz, cl);
+    const float fx = cl.fx, fy = cl.fy, fz = cl.fz;
     float c[8], e[8];
-    phi_corners(g, a, i0, j0, k0, c);
-    phi_corners(g, b, i0, j0, k0, e);
+    cell_corners(g, cl, a, c);
+    cell_corners(g, cl, b, e);
 #pragma unroll
     for (int n = 0; n < 8; ++n) {
         c[n] -= e[n];
@@ -452,14 +531,16 @@ __device__ __noinline__ int third_label(const DGrid& g, int a, int b, const floa
     if (!other) {
         return V2M_NOLAB;
     }
-    const float pa = phi_point(g, a, q[0], q[1], q[2]);
+    Cell cl;
+    cell_at(g, q[0], q[1], q[2], cl);
+    const float pa = cell_phi(g, cl, a);
     int c = V2M_NOLAB;
     float pc = 0.5f * pa;
 #pragma unroll 1
     for (int s = 0; s < n; ++s) {
         const int l = ll.get(s);
         if (l != a && l != b) {
-            const float w = phi_point(g, l, q[0], q[1], q[2]);
+            const float w = cell_phi(g, cl, l);
             if (w > pc) {
                 pc = w;
                 c = l;
@@ -484,14 +565,16 @@ __device__ __noinline__ int valid_on(const DGrid& g, int a, int b, int c, const 
     if (!other) {
         return 1;
     }
-    float mine = fminf(phi_point(g, a, q[0], q[1], q[2]), phi_point(g, b, q[0], q[1], q[2]));
+    Cell cl;
+    cell_at(g, q[0], q[1], q[2], cl);
+    float mine = fminf(cell_phi(g, cl, a), cell_phi(g, cl, b));
     if (c != V2M_NOLAB) {
-        mine = fminf(mine, phi_point(g, c, q[0], q[1], q[2]));
+        mine = fminf(mine, cell_phi(g, cl, c));
     }
 #pragma unroll 1
     for (int s = 0; s < n; ++s) {
         const int l = ll.get(s);
-        if (l != a && l != b && l != c && phi_point(g, l, q[0], q[1], q[2]) > mine + 0.02f) {
+        if (l != a && l != b && l != c && cell_phi(g, cl, l) > mine + 0.02f) {
             return 0;
         }
     }

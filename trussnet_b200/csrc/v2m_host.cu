@@ -1257,6 +1257,20 @@ int v2m_session_profile_stages(v2m_session* s, int iters, double* ms) {
     });
 }
 
+int v2m_session_queue_sizes(v2m_session* s, int32_t* trapped, int32_t* interior) {
+    return guard([&] {
+        Global g;
+        ck(cudaMemcpyAsync(&g, s->d.G, sizeof(Global), cudaMemcpyDeviceToHost, s->stream), "read");
+        ck(cudaStreamSynchronize(s->stream), "synchronize");
+        if (trapped) {
+            *trapped = g.qtrap_last;
+        }
+        if (interior) {
+            *interior = g.qint_last;
+        }
+    });
+}
+
 int v2m_session_timed_runs(v2m_session* s, int runs, int graph, int time_force, float* ms) {
     return guard([&] {
         if (runs < 1 || !ms) {

@@ -351,82 +351,100 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
     const int li = lab[i];
     const int Li = level_of(H, Ri);
     const int* cs = cstart + V.kofs;
-    int m = 0;
-    for (int L = Li - 1; L <= Li + 1; ++L) {
-        if (L < 0 || L >= H.nlev) {
-            continue;
-        }
-        const float bL = H.b0 * (float)(1 << L);
-        const float r = 0.5f * (Ri + bL);
-        const int x0 = bin_coord(H, L, px - r, H.ox, 0), x1 = bin_coord(H, L, px + r, H.ox, 0);
-        const int y0 = bin_coord(H, L, py - r, H.oy, 1), y1 = bin_coord(H, L, py + r, H.oy, 1);
-        const int z0 = bin_coord(H, L, pz - r, H.oz, 2), z1 = bin_coord(H, L, pz + r, H.oz, 2);
-        const int nbx = x1 - x0 + 1, nby = y1 - y0 + 1;
-        const int nbins = nbx * nby * (z1 - z0 + 1);
-        for (int bb = 0; bb < nbins; bb += 32) {
-            const int b = bb + lane;
-            int s0 = 0, c = 0;
-            if (b < nbins) {
-                const int cx = x0 + b % nbx, cy = y0 + (b / nbx) % nby, cz = z0 + b / (nbx * nby);
-                const int key = H.off[L] + cx + H.dim[L][0] * (cy + H.dim[L][1] * cz);
-                s0 = cs[key];
-                c = cs[key + 1] - s0;
-            }
-            int incl = c;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) {
-                    incl += y;
-                }
-            }
-            const int total = __shfl_sync(0xffffffffu, incl, 31);
-            for (int cb = 0; cb < total; cb += 32) {
-                const int q = cb + lane;
-                // bin of candidate q: the first lane whose inclusive count exceeds q
-                int lo = 0, hi2 = 31;
+    // The bins of a level inside the search box form rows along x with
+    // consecutive keys, so a row's candidates are one contiguous range of the
+    // sorted ids: the lanes take rows (of all three levels), not bins.
+    int lx0[3], lx1[3], ly0[3], lz0[3], lny[3], lrow[4], lkey[3];
+    lrow[0] = 0;
 #pragma unroll
-                for (int st = 0; st < 5; ++st) {
-                    const int mid = (lo + hi2) >> 1;
-                    const int vm = __shfl_sync(0xffffffffu, incl, mid);
-                    if (q < vm) {
-                        hi2 = mid;
-                    } else {
-                        lo = mid + 1;
+    for (int q = 0; q < 3; ++q) {
+        const int L = Li - 1 + q;
+        int nrows = 0;
+        lx0[q] = lx1[q] = ly0[q] = lz0[q] = lny[q] = lkey[q] = 0;
+        if (L >= 0 && L < H.nlev) {
+            const float bL = H.b0 * (float)(1 << L);
+            const float r = 0.5f * (Ri + bL);
+            lx0[q] = bin_coord(H, L, px - r, H.ox, 0);
+            lx1[q] = bin_coord(H, L, px + r, H.ox, 0);
+            ly0[q] = bin_coord(H, L, py - r, H.oy, 1);
+            const int y1 = bin_coord(H, L, py + r, H.oy, 1);
+            lz0[q] = bin_coord(H, L, pz - r, H.oz, 2);
+            const int z1 = bin_coord(H, L, pz + r, H.oz, 2);
+            lny[q] = y1 - ly0[q] + 1;
+            nrows = lny[q] * (z1 - lz0[q] + 1);
+            lkey[q] = H.off[L] + lx0[q];
+        }
+        lrow[q + 1] = lrow[q] + nrows;
+    }
+    const int nrows = lrow[3];
+    int m = 0;
+    for (int rb = 0; rb < nrows; rb += 32) {
+        const int r = rb + lane;
+        int s0 = 0, c = 0;
+        if (r < nrows) {
+            const int q = r < lrow[1] ? 0 : (r < lrow[2] ? 1 : 2);
+            const int L = Li - 1 + q;
+            const int rr = r - lrow[q];
+            const int zz = rr / lny[q];
+            const int cy = ly0[q] + (rr - zz * lny[q]), cz = lz0[q] + zz;
+            const int key0 = lkey[q] + H.dim[L][0] * (cy + H.dim[L][1] * cz);
+            s0 = cs[key0];
+            c = cs[key0 + (lx1[q] - lx0[q]) + 1] - s0;
+        }
+        int incl = c;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) {
+                incl += y;
+            }
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        for (int cb = 0; cb < total; cb += 32) {
+            const int q = cb + lane;
+            // row of candidate q: the first lane whose inclusive count exceeds q
+            int lo = 0, hi2 = 31;
+#pragma unroll
+            for (int st = 0; st < 5; ++st) {
+                const int mid = (lo + hi2) >> 1;
+                const int vm = __shfl_sync(0xffffffffu, incl, mid);
+                if (q < vm) {
+                    hi2 = mid;
+                } else {
+                    lo = mid + 1;
+                }
+            }
+            const int bs0 = __shfl_sync(0xffffffffu, s0, lo);
+            const int bexc = __shfl_sync(0xffffffffu, incl - c, lo);
+            bool ok = false;
+            float dist = 0.0f;
+            int j = -1;
+            if (q < total) {
+                const int sidx = bs0 + (q - bexc);
+                j = sorted[sidx];
+                if (j != (int)i) {
+                    const float4 ps = Ps[sidx];
+                    const float ex = ps.x - px, ey = ps.y - py, ez = ps.z - pz;
+                    const float d2 = ex * ex + ey * ey + ez * ez;
+                    const float rj = ts * 0.5f * (hi + ps.w);
+                    ok = !(d2 >= rj * rj);
+                    if (ok && ti_int && typ[j] == V2M_INTERIOR && lab[j] != li) {
+                        ok = false;
+                    }
+                    if (ok) {
+                        dist = sqrtf(d2);
                     }
                 }
-                const int bs0 = __shfl_sync(0xffffffffu, s0, lo);
-                const int bexc = __shfl_sync(0xffffffffu, incl - c, lo);
-                bool ok = false;
-                float dist = 0.0f;
-                int j = -1;
-                if (q < total) {
-                    const int s = bs0 + (q - bexc);
-                    j = sorted[s];
-                    if (j != (int)i) {
-                        const float4 ps = Ps[s];
-                        const float ex = ps.x - px, ey = ps.y - py, ez = ps.z - pz;
-                        const float d2 = ex * ex + ey * ey + ez * ez;
-                        const float rj = ts * 0.5f * (hi + ps.w);
-                        ok = !(d2 >= rj * rj);
-                        if (ok && ti_int && typ[j] == V2M_INTERIOR && lab[j] != li) {
-                            ok = false;
-                        }
-                        if (ok) {
-                            dist = sqrtf(d2);
-                        }
-                    }
-                }
-                const unsigned mask = __ballot_sync(0xffffffffu, ok);
-                if (ok) {
-                    const int slot = m + __popc(mask & ((1u << lane) - 1u));
-                    sm.d[slot] = dist;
-                    sm.id[slot] = j;
-                }
-                m += __popc(mask);
-                __syncwarp();
-                if (m > kCap - 32) {
-                    m = warp_prune(sm, m, lane);
-                }
+            }
+            const unsigned mask = __ballot_sync(0xffffffffu, ok);
+            if (ok) {
+                const int slot = m + __popc(mask & ((1u << lane) - 1u));
+                sm.d[slot] = dist;
+                sm.id[slot] = j;
+            }
+            m += __popc(mask);
+            __syncwarp();
+            if (m > kCap - 32) {
+                m = warp_prune(sm, m, lane);
             }
         }
     }
@@ -492,6 +510,8 @@ __global__ void __launch_bounds__(kNbrMaxThreads) k_refresh(const DVol* __restri
         const int d = atomicAdd(&G->blocks_done, 1);
         if (d == (int)gridDim.x - 1) {
             G->nrefresh = 0;
+            G->qtrap_last = G->qtrap;
+            G->qint_last = G->qint;
             G->qtrap = 0;
             G->qint = 0;
             G->blocks_done = 0;

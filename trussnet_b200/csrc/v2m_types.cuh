@@ -90,6 +90,7 @@ struct Global {
     int err;             // kernel error flag (first error code)
     int err_info;
     int qtrap, qint;     // move queue lengths: trapped nodes (front), interior nodes (back)
+    int qtrap_last, qint_last;   // the last iteration's queue lengths
 };
 
 constexpr int kMaxVol = 1024;

@@ -181,6 +181,12 @@ class Session:
         _lib.check(self.L.v2m_session_profile_stages(self.h, int(iters), ms.ctypes.data))
         return dict(zip(("force", "move", "control_refresh", "rebuild", "total"), ms.tolist()))
 
+    def queue_sizes(self):
+        """(trapped, interior) nodes the last iteration's move sent to the trapped-move stage."""
+        a, b = C.c_int32(), C.c_int32()
+        _lib.check(self.L.v2m_session_queue_sizes(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def clear_counters(self):
         _lib.check(self.L.v2m_session_clear_counters(self.h))
 
