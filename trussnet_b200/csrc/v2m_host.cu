@@ -296,6 +296,7 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         s->refresh_blocks = sms * 4;
+        s->d.sms = sms;
         static const int env_div = std::getenv("V2M_REBUILD_DIV") ? std::atoi(std::getenv("V2M_REBUILD_DIV")) : 300;
         // layout
         int64_t N = 0, KT = 0;

@@ -20,6 +20,7 @@
 //                 half-skin count, FIRE power per block)
 //   k_control     FIRE update, p99, stop test, rebuild trigger [src/v2m_particles.cpp:849-946; FireCtl src/v2m_particles.h:47-76]
 //   k_refresh     lists of nodes past a full skin rebuilt     [src/v2m_particles.cpp:917-937]
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 
@@ -63,25 +64,26 @@ __device__ __forceinline__ float pack_h(float h, int ty) {
 __global__ void k_keys(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl, const uint16_t* __restrict__ nodevol,
                        const float4* __restrict__ Pq, int* __restrict__ key, int* __restrict__ cnt,
                        float4* __restrict__ P0, int64_t N, Global* G) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= N) {
+    if (!*((volatile int*)&G->rebuild_any)) {
         return;
     }
-    const int v = nodevol[i];
-    if (v == 0xFFFF || !ctl[v].rebuild) {
-        return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const int v = nodevol[i];
+        if (v == 0xFFFF || !ctl[v].rebuild) {
+            continue;
+        }
+        const DVol& V = vols[v];
+        const float4 p = Pq[i];
+        const float hh = size_at(V.g, V.hmode, p.x, p.y, p.z);
+        const int k = bin_key(V.H, level_of(V.H, (V.t + V.skin) * hh), p.x, p.y, p.z);
+        if (k < 0 || k >= V.nkeys) {
+            raise_error(G, 1, (int)i);
+            continue;
+        }
+        key[i] = k;
+        atomicAdd(cnt + V.kofs + k, 1);
+        P0[i] = make_float4(p.x, p.y, p.z, 0.0f);
     }
-    const DVol& V = vols[v];
-    const float4 p = Pq[i];
-    const float hh = size_at(V.g, V.hmode, p.x, p.y, p.z);
-    const int k = bin_key(V.H, level_of(V.H, (V.t + V.skin) * hh), p.x, p.y, p.z);
-    if (k < 0 || k >= V.nkeys) {
-        raise_error(G, 1, (int)i);
-        return;
-    }
-    key[i] = k;
-    atomicAdd(cnt + V.kofs + k, 1);
-    P0[i] = make_float4(p.x, p.y, p.z, 0.0f);
 }
 
 // ---- exclusive scan of the bin counts, per volume, based at the volume's first node --
@@ -240,40 +242,27 @@ __global__ void k_scan_apply(const DVol* __restrict__ vols, const VolCtl* __rest
 __global__ void k_scatter(const VolCtl* __restrict__ ctl, const DVol* __restrict__ vols, const uint16_t* __restrict__ nodevol,
                           const int* __restrict__ key, int* __restrict__ cursor, int* __restrict__ sorted, int64_t N,
                           Global* G) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= N) {
+    if (!*((volatile int*)&G->rebuild_any)) {
         return;
     }
-    const int v = nodevol[i];
-    if (v == 0xFFFF || !ctl[v].rebuild) {
-        return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const int v = nodevol[i];
+        if (v == 0xFFFF || !ctl[v].rebuild) {
+            continue;
+        }
+        const DVol& V = vols[v];
+        const int pos = atomicAdd(cursor + V.kofs + key[i], 1);
+        if (pos < V.nofs || pos >= V.nofs + V.n) {
+            raise_error(G, 2, (int)i);
+            continue;
+        }
+        sorted[pos] = (int)i;
     }
-    const DVol& V = vols[v];
-    const int pos = atomicAdd(cursor + V.kofs + key[i], 1);
-    if (pos < V.nofs || pos >= V.nofs + V.n) {
-        raise_error(G, 2, (int)i);
-        return;
-    }
-    sorted[pos] = (int)i;
 }
 
-// One thread per bin: the bin's ids ascending (the CPU's stable counting sort,
-// src/v2m_particles.cpp:791-795), then their positions and sizes in bin order.
-__global__ void k_binsort(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl, const int16_t* __restrict__ tilevol,
-                          const int* __restrict__ cstart, int* __restrict__ sorted, const float4* __restrict__ Pq,
-                          float4* __restrict__ Ps, int64_t KT) {
-    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (e >= KT) {
-        return;
-    }
-    const int v = tilevol[e / kScanTile];
-    if (v < 0 || !ctl[v].rebuild) {
-        return;
-    }
-    const DVol& V = vols[v];
-    if (e < V.kofs || e >= V.kofs + V.nkeys) {
-        return;
-    }
+// ascending ids within bin e, then the bin's positions and sizes
+__device__ __forceinline__ void bin_order(const int* __restrict__ cstart, int* __restrict__ sorted,
+                                          const float4* __restrict__ Pq, float4* __restrict__ Ps, int64_t e) {
     const int s0 = cstart[e], s1 = cstart[e + 1];
     for (int a = s0 + 1; a < s1; ++a) {
         const int x = sorted[a];
@@ -289,6 +278,28 @@ __global__ void k_binsort(const DVol* __restrict__ vols, const VolCtl* __restric
         Ps[s] = make_float4(p.x, p.y, p.z, fabsf(p.w));
     }
 }
+
+// One thread per bin: the bin's ids ascending (the CPU's stable counting sort,
+// src/v2m_particles.cpp:791-795), then their positions and sizes in bin order.
+__global__ void k_binsort(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl, const int16_t* __restrict__ tilevol,
+                          const int* __restrict__ cstart, int* __restrict__ sorted, const float4* __restrict__ Pq,
+                          float4* __restrict__ Ps, int64_t KT, const Global* G) {
+    if (!*((volatile const int*)&G->rebuild_any)) {
+        return;
+    }
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < KT; e += (int64_t)gridDim.x * blockDim.x) {
+        const int v = tilevol[e / kScanTile];
+        if (v < 0 || !ctl[v].rebuild) {
+            continue;
+        }
+        const DVol& V = vols[v];
+        if (e < V.kofs || e >= V.kofs + V.nkeys) {
+            continue;
+        }
+        bin_order(cstart, sorted, Pq, Ps, e);
+    }
+}
+
 
 // ---- K-nearest truss lists ----------------------------------------------------------
 // One warp per node. The accepted candidates (distance and label tests of
@@ -464,18 +475,20 @@ __global__ void __launch_bounds__(kNbrMaxThreads) k_neighbors(const DVol* __rest
                                                            const uint8_t* __restrict__ typ, const uint16_t* __restrict__ lab,
                                                            const int* __restrict__ cstart, const int* __restrict__ sorted,
                                                            const float4* __restrict__ Ps, int* __restrict__ nbr,
-                                                           uint8_t* __restrict__ nnb, int64_t N) {
+                                                           uint8_t* __restrict__ nnb, int64_t N, const Global* G) {
     __shared__ NbrWarpSmem sm[kNbrMaxThreads / 32];
+    if (!*((volatile const int*)&G->rebuild_any)) {
+        return;
+    }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t i = blockIdx.x * (int64_t)(blockDim.x / 32) + w;
-    if (i >= N) {
-        return;
+    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x / 32);
+    for (int64_t i = blockIdx.x * (int64_t)(blockDim.x / 32) + w; i < N; i += nwarps) {
+        const int v = nodevol[i];
+        if (v == 0xFFFF || !ctl[v].rebuild) {
+            continue;
+        }
+        warp_neighbors(vols[v], i, lane, sm[w], Pq, typ, lab, cstart, sorted, Ps, nbr, nnb, N);
     }
-    const int v = nodevol[i];
-    if (v == 0xFFFF || !ctl[v].rebuild) {
-        return;
-    }
-    warp_neighbors(vols[v], i, lane, sm[w], Pq, typ, lab, cstart, sorted, Ps, nbr, nnb, N);
 }
 
 // The self-refresh of the nodes past a full skin (list filled by k_move), one
@@ -521,6 +534,8 @@ __global__ void __launch_bounds__(kNbrMaxThreads) k_refresh(const DVol* __restri
 }
 
 // ---- bar forces ----------------------------------------------------------------
+constexpr int kForceBatch = 8;
+
 // One thread per node; the lists are slot-major (nbr[k*N + i]) so a warp's k-th
 // entries are one coalesced 128-byte row; neighbour position + signed size is
 // one 16-byte gather. Bars are added in list order, as v2m_force does.
@@ -548,21 +563,38 @@ __global__ void __launch_bounds__(256) k_force(const DVol* __restrict__ vols, co
     const int n = nnb[i];
     float fx = 0.0f, fy = 0.0f, fz = 0.0f, fa = 0.0f;
     const int* row = nbr + i;
-    for (int k = 0; k < n; ++k) {
-        const int j = __ldg(row + (int64_t)k * N);
-        const float4 q = __ldg(Pq + j);
-        const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
-        const float l = sqrtf(ex * ex + ey * ey + ez * ez);
-        const float hj = fabsf(q.w);
-        const float l0 = ((ni && signbit(q.w)) ? fsurf : fscale) * 0.5f * (hi + hj);
-        if (l >= l0 || l <= 0.0f) {
-            continue;
+    // loads in batches of kForceBatch (ids, then positions) so that many gathers
+    // are in flight per thread; the bars are still added one by one in list order
+    for (int k0 = 0; k0 < n; k0 += kForceBatch) {
+        int jj[kForceBatch];
+        float4 qq[kForceBatch];
+#pragma unroll
+        for (int u = 0; u < kForceBatch; ++u) {
+            jj[u] = k0 + u < n ? __ldg(row + (int64_t)(k0 + u) * N) : (int)i;
         }
-        const float f = (l0 - l) / l;
-        fx += f * ex;
-        fy += f * ey;
-        fz += f * ez;
-        fa += 1.0f;
+#pragma unroll
+        for (int u = 0; u < kForceBatch; ++u) {
+            qq[u] = __ldg(Pq + jj[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < kForceBatch; ++u) {
+            if (k0 + u >= n) {
+                break;
+            }
+            const float4 q = qq[u];
+            const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
+            const float l = sqrtf(ex * ex + ey * ey + ez * ez);
+            const float hj = fabsf(q.w);
+            const float l0 = ((ni && signbit(q.w)) ? fsurf : fscale) * 0.5f * (hi + hj);
+            if (l >= l0 || l <= 0.0f) {
+                continue;
+            }
+            const float f = (l0 - l) / l;
+            fx += f * ex;
+            fy += f * ey;
+            fz += f * ez;
+            fa += 1.0f;
+        }
     }
     F[i] = make_float4(fx, fy, fz, fa);
 }
@@ -674,6 +706,9 @@ __global__ void __launch_bounds__(kMoveThreads) k_move_pre(const DVol* __restric
     tail_init(acc);
     if (threadIdx.x == 0) {
         sh_vol = -1;
+        if (blockIdx.x == 0) {
+            G->rebuild_any = 0;   // the last iteration's rebuild stages are done
+        }
     }
     __syncthreads();
     const int v = i < N ? nodevol[i] : 0xFFFF;
@@ -908,7 +943,7 @@ __global__ void k_power_serial(const DVol* __restrict__ vols, const VolCtl* __re
 
 // ---- the loop's control (one block per volume) ---------------------------------------
 __global__ void k_control(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl, const double* __restrict__ psum,
-                          const double* __restrict__ pser, int serial, int move_threads) {
+                          const double* __restrict__ pser, int serial, int move_threads, Global* G) {
     const int v = blockIdx.x;
     const DVol& V = vols[v];
     VolCtl& c = ctl[v];
@@ -1004,12 +1039,16 @@ __global__ void k_control(const DVol* __restrict__ vols, VolCtl* __restrict__ ct
     c.rebuild = reb;
     if (reb) {
         ++c.rebuilds;
+        G->rebuild_any = 1;
     }
 }
 
 // ---- small utilities -----------------------------------------------------------------
-__global__ void k_set_rebuild(VolCtl* ctl, int nvol, int val) {
+__global__ void k_set_rebuild(VolCtl* ctl, int nvol, int val, Global* G) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v == 0) {
+        G->rebuild_any = val;
+    }
     if (v < nvol && !ctl[v].done) {
         ctl[v].rebuild = val;
         if (val) {
@@ -1138,8 +1177,15 @@ static inline unsigned nblk(int64_t n, int b) {
     return (unsigned)((n + b - 1) / b);
 }
 
+// grid of a grid-stride kernel: enough blocks to fill the GPU, no more
+static inline unsigned gsblocks(const Dev& d, int64_t items, int per_block) {
+    const int64_t need = (items + per_block - 1) / per_block;
+    const int64_t cap = (int64_t)d.sms * 8;
+    return (unsigned)std::max<int64_t>(1, std::min(need, cap));
+}
+
 void launch_keys(cudaStream_t s, const Dev& d) {
-    k_keys<<<nblk(d.N, 256), 256, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.key, d.cnt, d.P0, d.N, d.G);
+    k_keys<<<gsblocks(d, d.N, 256), 256, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.key, d.cnt, d.P0, d.N, d.G);
 }
 
 void launch_scan(cudaStream_t s, const Dev& d) {
@@ -1149,13 +1195,15 @@ void launch_scan(cudaStream_t s, const Dev& d) {
 }
 
 void launch_scatter(cudaStream_t s, const Dev& d) {
-    k_scatter<<<nblk(d.N, 256), 256, 0, s>>>(d.ctl, d.vols, d.nodevol, d.key, d.cursor, d.sorted, d.N, d.G);
-    k_binsort<<<nblk(d.KT, 256), 256, 0, s>>>(d.vols, d.ctl, d.tilevol, d.cstart, d.sorted, d.Pq, d.Ps, d.KT);
+    k_scatter<<<gsblocks(d, d.N, 256), 256, 0, s>>>(d.ctl, d.vols, d.nodevol, d.key, d.cursor, d.sorted, d.N, d.G);
+    k_binsort<<<gsblocks(d, d.KT, 256), 256, 0, s>>>(d.vols, d.ctl, d.tilevol, d.cstart, d.sorted, d.Pq, d.Ps, d.KT,
+                                                     d.G);
 }
 
 void launch_neighbors(cudaStream_t s, const Dev& d, int threads) {
-    k_neighbors<<<nblk(d.N, threads / 32), threads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.typ, d.lab,
-                                                                     d.cstart, d.sorted, d.Ps, d.nbr, d.nnb, d.N);
+    k_neighbors<<<gsblocks(d, d.N, threads / 32) * 2, threads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.typ, d.lab,
+                                                                        d.cstart, d.sorted, d.Ps, d.nbr, d.nnb, d.N,
+                                                                        d.G);
 }
 
 void launch_force(cudaStream_t s, const Dev& d, int threads) {
@@ -1174,7 +1222,7 @@ void launch_control(cudaStream_t s, const Dev& d, int serial) {
     if (serial) {
         k_power_serial<<<nblk(d.nvol, 32), 32, 0, s>>>(d.vols, d.ctl, d.pw, d.pser, d.nvol);
     }
-    k_control<<<d.nvol, kCtlThreads, 0, s>>>(d.vols, d.ctl, d.psum, d.pser, serial, kMoveThreads);
+    k_control<<<d.nvol, kCtlThreads, 0, s>>>(d.vols, d.ctl, d.psum, d.pser, serial, kMoveThreads, d.G);
 }
 
 void launch_refresh(cudaStream_t s, const Dev& d, int blocks) {
@@ -1183,7 +1231,7 @@ void launch_refresh(cudaStream_t s, const Dev& d, int blocks) {
 }
 
 void launch_set_rebuild(cudaStream_t s, const Dev& d, int val) {
-    k_set_rebuild<<<nblk(d.nvol, 128), 128, 0, s>>>(d.ctl, d.nvol, val);
+    k_set_rebuild<<<nblk(d.nvol, 128), 128, 0, s>>>(d.ctl, d.nvol, val, d.G);
 }
 
 void launch_lists_rowmajor(cudaStream_t s, const Dev& d, int64_t nofs, int n, int* out, int* nout) {

@@ -20,6 +20,7 @@ constexpr int kNodeAlign = kMoveThreads;
 // Every device array of a session (flat over its volumes).
 struct Dev {
     int nvol = 0;
+    int sms = 148;       // multiprocessors: the grid of the grid-stride kernels
     int64_t N = 0;       // nodes incl. per-volume padding
     int64_t KT = 0;      // bin-start entries incl. padding
     int ntile_key = 0;

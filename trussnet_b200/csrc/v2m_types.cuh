@@ -91,6 +91,7 @@ struct Global {
     int err_info;
     int qtrap, qint;     // move queue lengths: trapped nodes (front), interior nodes (back)
     int qtrap_last, qint_last;   // the last iteration's queue lengths
+    int rebuild_any;     // some volume rebuilds this iteration (the rebuild stages return at once otherwise)
 };
 
 constexpr int kMaxVol = 1024;

@@ -264,7 +264,7 @@ def ellipsoids(dim=128, nlab=4, h=(1.5, 4.0), density=1.0, seed=0):
     return g, nd
 
 
-def batch(nvol=64, seed=0, dmin=32, dmax=160, lmin=2, lmax=18, scale=1.0):
+def batch(nvol=64, seed=0, dmin=32, dmax=160, lmin=2, lmax=18, scale=1.55):
     """`nvol` independent volumes of seeded sizes dmin^3..dmax^3 with lmin..lmax
     nested-shell labels; shells at least 2R+8 voxels apart where they fit."""
     rng = np.random.default_rng(seed)
