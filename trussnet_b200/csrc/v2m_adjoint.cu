@@ -116,6 +116,26 @@ __device__ __forceinline__ float size_at(const Dims& D, const float* __restrict_
     return h;
 }
 
+// ---- packed node records ---------------------------------------------------------
+// A state is float4 xh[i] = (x_i, h_i): one 16-byte load brings a neighbour's
+// position and size. List entries carry the neighbour's "not INTERIOR" flag in
+// bit 31 (ids are below 2^30), so no type byte is gathered per bar.
+
+constexpr int kIdMask = 0x7FFFFFFF;
+
+__device__ __forceinline__ float4 with_size(const Dims& D, const float* __restrict__ G, float x, float y, float z) {
+    return make_float4(x, y, z, size_at(D, G, x, y, z, nullptr, nullptr, nullptr));
+}
+
+// xh = (x, H(x)) from [n, 3] positions
+__global__ void k_pack_size(Dims D, const float* __restrict__ G, const float* __restrict__ x3, float4* __restrict__ xh,
+                            int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        xh[i] = with_size(D, G, x3[3 * i], x3[3 * i + 1], x3[3 * i + 2]);
+    }
+}
+
 __global__ void k_pack(const float* __restrict__ x3, float4* __restrict__ x4, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
@@ -133,77 +153,81 @@ __global__ void k_unpack(const float4* __restrict__ x4, float* __restrict__ x3, 
     }
 }
 
-__global__ void k_size(Dims D, const float* __restrict__ G, const float4* __restrict__ x, float* __restrict__ h, int n) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) {
-        const float4 p = x[i];
-        h[i] = size_at(D, G, p.x, p.y, p.z, nullptr, nullptr, nullptr);
-    }
-}
-
-// one step; records (replay = 0) or replays the active-bar masks
-__global__ void k_step(const float4* __restrict__ x, const float* __restrict__ h, const int* __restrict__ nbr,
-                       const uint8_t* __restrict__ nnb, const uint8_t* __restrict__ typ, float fscale, float fsurf,
-                       float dt, uint32_t* __restrict__ mask, int replay, float4* __restrict__ y, int n) {
+// one step xh -> yh (the new state's sizes included); records (replay = 0) or
+// replays the active-bar masks. A replay visits only the taped bars, in the same
+// ascending slot order as the recording.
+__global__ void k_step(Dims D, const float* __restrict__ G, const float4* __restrict__ xh,
+                       const int* __restrict__ nbrf, const uint8_t* __restrict__ nnb, const uint8_t* __restrict__ typ,
+                       float fscale, float fsurf, float dt, uint32_t* __restrict__ mask, int replay,
+                       float4* __restrict__ yh, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) {
         return;
     }
-    const float4 p = x[i];
+    const float4 p = xh[i];
     const int ti = typ[i];
     if (ti == V2M_CORNER) {
-        y[i] = p;
+        yh[i] = p;   // y = x, so H(y) = H(x)
         if (!replay) {
             mask[i] = 0u;
         }
         return;
     }
-    const float hi = h[i];
-    const int c = nnb[i];
-    uint32_t bits = replay ? mask[i] : 0u;
+    const bool ni = ti != V2M_INTERIOR;
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
     int act = 0;
-    for (int k = 0; k < c; ++k) {
-        const int j = __ldg(nbr + (size_t)k * n + i);
-        const float4 q = __ldg(x + j);
-        const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
-        const float l = sqrtf(ex * ex + ey * ey + ez * ez);
-        const float a = ((ti != V2M_INTERIOR && typ[j] != V2M_INTERIOR) ? fsurf : fscale) * 0.5f;
-        const float l0 = a * (hi + __ldg(h + j));
-        const bool on = replay ? ((bits >> k) & 1u) != 0u : (l < l0 && l > 0.0f);
-        if (!on) {
-            continue;
+    if (replay) {
+        for (uint32_t b = mask[i]; b; b &= b - 1u) {
+            const int k = __ffs(b) - 1;
+            const int e = __ldg(nbrf + (size_t)k * n + i);
+            const float4 q = __ldg(xh + (e & kIdMask));
+            const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
+            const float l = sqrtf(ex * ex + ey * ey + ez * ez);
+            const float l0 = ((ni && e < 0) ? fsurf : fscale) * 0.5f * (p.w + q.w);
+            const float f = (l0 - l) / l;
+            fx += f * ex;
+            fy += f * ey;
+            fz += f * ez;
+            ++act;
         }
-        if (!replay) {
+    } else {
+        uint32_t bits = 0u;
+        const int c = nnb[i];
+        for (int k = 0; k < c; ++k) {
+            const int e = __ldg(nbrf + (size_t)k * n + i);
+            const float4 q = __ldg(xh + (e & kIdMask));
+            const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
+            const float l = sqrtf(ex * ex + ey * ey + ez * ez);
+            const float l0 = ((ni && e < 0) ? fsurf : fscale) * 0.5f * (p.w + q.w);
+            if (!(l < l0 && l > 0.0f)) {
+                continue;
+            }
             bits |= 1u << k;
+            const float f = (l0 - l) / l;
+            fx += f * ex;
+            fy += f * ey;
+            fz += f * ez;
+            ++act;
         }
-        const float f = (l0 - l) / l;
-        fx += f * ex;
-        fy += f * ey;
-        fz += f * ez;
-        ++act;
-    }
-    if (!replay) {
         mask[i] = bits;
     }
     const float s = dt / (float)(act > 1 ? act : 1);
-    y[i] = make_float4(p.x + s * fx, p.y + s * fy, p.z + s * fz, 0.0f);
+    yh[i] = with_size(D, G, p.x + s * fx, p.y + s * fy, p.z + s * fz);
 }
 
-__global__ void k_loss(const float4* __restrict__ x, const float* __restrict__ h, const int* __restrict__ nbr,
-                       const uint8_t* __restrict__ nnb, double* __restrict__ part, int n) {
+__global__ void k_loss(const float4* __restrict__ xh, const int* __restrict__ nbrf, const uint8_t* __restrict__ nnb,
+                       double* __restrict__ part, int n) {
     __shared__ double red[kT / 32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double s = 0.0;
     if (i < n) {
-        const float4 p = x[i];
-        const float hi = h[i];
+        const float4 p = xh[i];
         for (int k = 0; k < nnb[i]; ++k) {
-            const int j = __ldg(nbr + (size_t)k * n + i);
-            const float4 q = __ldg(x + j);
+            const int j = __ldg(nbrf + (size_t)k * n + i) & kIdMask;
+            const float4 q = __ldg(xh + j);
             const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
             const float l = sqrtf(ex * ex + ey * ey + ez * ez);
-            const float r = l / (0.5f * (hi + __ldg(h + j))) - 1.0f;
+            const float r = l / (0.5f * (p.w + q.w)) - 1.0f;
             s += (double)r * (double)r;
         }
     }
@@ -228,7 +252,33 @@ __global__ void k_loss(const float4* __restrict__ x, const float* __restrict__ h
 // (i, k) with nbr[i][k] = j, by ascending i then k) is built once. Each node then
 // sums, in a fixed order and in double, the terms of its own bars and of the
 // bars that point at it: no atomics, and the same bits on every run. Only the
-// sizing grid's 8-corner scatter (k_size_bwd_g) stays on fixed-point atomics.
+// sizing grid's 8-corner scatter stays on fixed-point atomics.
+//
+// The reverse of step t reads, for every node, one 32-byte record: the state
+// (x_t, h_t), mu = s_t lam_{t+1} (s_t = dt / max(c_t, 1), the node's step scale)
+// and the step's taped mask. A bar pointing at j then costs one load of its
+// source's record.
+struct __align__(32) Rec {
+    float4 xh;    // x_t, h_t
+    float4 mub;   // mu (3 floats), the taped mask (bits)
+};
+
+__device__ __forceinline__ Rec make_rec(const float4& xh, const float4& lam, uint32_t bits, float dt) {
+    const int act = __popc(bits);
+    const float s = dt / (float)(act > 1 ? act : 1);
+    Rec r;
+    r.xh = xh;
+    r.mub = make_float4(s * lam.x, s * lam.y, s * lam.z, __uint_as_float(bits));
+    return r;
+}
+
+__global__ void k_rec(const float4* __restrict__ xh, const float4* __restrict__ lam, const uint32_t* __restrict__ mask,
+                      float dt, Rec* __restrict__ rec, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        rec[i] = make_rec(xh[i], lam[i], mask[i], dt);
+    }
+}
 
 // the size term of node j, in the same thread that summed dL/dh_j: lam_j +=
 // dL/dh_j dH/dx_j, and the grid's 8 corners get dL/dh_j w (fixed-point atomics)
@@ -250,24 +300,22 @@ __device__ __forceinline__ void size_tail(const Dims& D, const float* __restrict
 }
 
 // d(loss)/dx and d(loss)/dh at x (loss = sum over list entries of (l/hm - 1)^2)
-__global__ void k_loss_bwd_g(Dims D, const float* __restrict__ G, const float4* __restrict__ x,
-                             const float* __restrict__ h, const int* __restrict__ nbr, const uint8_t* __restrict__ nnb,
-                             const int* __restrict__ tofs, const int* __restrict__ tsrc, float gscale,
+__global__ void k_loss_bwd_g(Dims D, const float* __restrict__ G, const float4* __restrict__ xh,
+                             const int* __restrict__ nbrf, const uint8_t* __restrict__ nnb,
+                             const int* __restrict__ tofs, const int* __restrict__ tsrcf, float gscale,
                              float4* __restrict__ lam, unsigned long long* __restrict__ gG, int n) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) {
         return;
     }
-    const float4 pj = x[j];
-    const float hj = h[j];
+    const float4 pj = xh[j];
     double l3[3] = { 0.0, 0.0, 0.0 }, g = 0.0;
     // own entries (j -> k): + dl e/l
     for (int k = 0; k < nnb[j]; ++k) {
-        const int m = __ldg(nbr + (size_t)k * n + j);
-        const float4 q = __ldg(x + m);
+        const float4 q = __ldg(xh + (__ldg(nbrf + (size_t)k * n + j) & kIdMask));
         const float e[3] = { pj.x - q.x, pj.y - q.y, pj.z - q.z };
         const float l = sqrtf(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
-        const float hm = 0.5f * (hj + __ldg(h + m));
+        const float hm = 0.5f * (pj.w + q.w);
         const float r = l / hm - 1.0f;
         const float dl = gscale * 2.0f * r / hm, dhm = -gscale * 2.0f * r * l / (hm * hm);
         for (int d = 0; d < 3; ++d) {
@@ -277,11 +325,10 @@ __global__ void k_loss_bwd_g(Dims D, const float* __restrict__ G, const float4* 
     }
     // entries pointing at j (i -> j): - dl e/l
     for (int t = tofs[j]; t < tofs[j + 1]; ++t) {
-        const int i = __ldg(tsrc + t);
-        const float4 pi = __ldg(x + i);
+        const float4 pi = __ldg(xh + (__ldg(tsrcf + t) & kIdMask));
         const float e[3] = { pi.x - pj.x, pi.y - pj.y, pi.z - pj.z };
         const float l = sqrtf(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
-        const float hm = 0.5f * (__ldg(h + i) + hj);
+        const float hm = 0.5f * (pi.w + pj.w);
         const float r = l / hm - 1.0f;
         const float dl = gscale * 2.0f * r / hm, dhm = -gscale * 2.0f * r * l / (hm * hm);
         for (int d = 0; d < 3; ++d) {
@@ -304,37 +351,35 @@ __device__ __forceinline__ void bar_vjp(const float* e, float l0, float a, const
     *sa = a * (em / l);
 }
 
-// reverse of one step: lam_in = dL/dx_{t+1} -> lam_out (before the size term), gh = dL/dh_t
-__global__ void k_step_bwd_g(Dims D, const float* __restrict__ G, const float4* __restrict__ x,
-                             const float* __restrict__ h, const int* __restrict__ nbr, const uint8_t* __restrict__ nnb,
+// reverse of step t: lam_in = dL/dx_{t+1} -> lam_out = dL/dx_t (with the size
+// term). When step t - 1 follows in the same segment, the thread also writes
+// node j's record for it (state x_{t-1}, mask_{t-1}, mu from lam_out).
+__global__ void k_step_bwd_g(Dims D, const float* __restrict__ G, const Rec* __restrict__ rec,
+                             const float4* __restrict__ lam_in, const int* __restrict__ nbrf,
                              const uint8_t* __restrict__ typ, float fscale, float fsurf, float dt,
-                             const uint32_t* __restrict__ mask, const float4* __restrict__ lam_in,
-                             const int* __restrict__ tofs, const int* __restrict__ tsrc,
+                             const int* __restrict__ tofs, const int* __restrict__ tsrcf,
                              const uint8_t* __restrict__ tslot, float4* __restrict__ lam_out,
-                             unsigned long long* __restrict__ gG, int n) {
+                             const float4* __restrict__ xh_prev, const uint32_t* __restrict__ mask_prev,
+                             Rec* __restrict__ rec_prev, unsigned long long* __restrict__ gG, int n) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) {
         return;
     }
     const float4 lj = lam_in[j];
     double l3[3] = { (double)lj.x, (double)lj.y, (double)lj.z }, g = 0.0;
-    const float4 pj = x[j];
-    const float hj = h[j];
-    const int tj = typ[j];
-    if (tj != V2M_CORNER) {
-        const uint32_t bits = mask[j];
-        const int act = __popc(bits);
-        const float s = dt / (float)(act > 1 ? act : 1);
-        const float mu[3] = { s * lj.x, s * lj.y, s * lj.z };
-        for (int k = 0; k < nnb[j]; ++k) {
-            if (!((bits >> k) & 1u)) {
-                continue;
-            }
-            const int m = __ldg(nbr + (size_t)k * n + j);
-            const float4 q = __ldg(x + m);
+    const Rec rj = rec[j];
+    const float4 pj = rj.xh;
+    const bool nj = typ[j] != V2M_INTERIOR;
+    {
+        // own bars (a CORNER's mask is empty)
+        const float mu[3] = { rj.mub.x, rj.mub.y, rj.mub.z };
+        for (uint32_t b = __float_as_uint(rj.mub.w); b; b &= b - 1u) {
+            const int k = __ffs(b) - 1;
+            const int em = __ldg(nbrf + (size_t)k * n + j);
+            const float4 q = __ldg(&rec[em & kIdMask].xh);
             const float e[3] = { pj.x - q.x, pj.y - q.y, pj.z - q.z };
-            const float a = ((tj != V2M_INTERIOR && typ[m] != V2M_INTERIOR) ? fsurf : fscale) * 0.5f;
-            const float l0 = a * (hj + __ldg(h + m));
+            const float a = ((nj && em < 0) ? fsurf : fscale) * 0.5f;
+            const float l0 = a * (pj.w + q.w);
             float v[3], sa;
             bar_vjp(e, l0, a, mu, v, &sa);
             for (int d = 0; d < 3; ++d) {
@@ -344,21 +389,18 @@ __global__ void k_step_bwd_g(Dims D, const float* __restrict__ G, const float4* 
         }
     }
     for (int t = tofs[j]; t < tofs[j + 1]; ++t) {
-        const int i = __ldg(tsrc + t);
+        const int ei = __ldg(tsrcf + t);
         const int k = __ldg(tslot + t);
-        const int ti = typ[i];
-        const uint32_t bi = __ldg(mask + i);
-        if (ti == V2M_CORNER || !((bi >> k) & 1u)) {
+        const float4* ri = reinterpret_cast<const float4*>(rec + (ei & kIdMask));
+        const float4 mb = __ldg(ri + 1);
+        if (!((__float_as_uint(mb.w) >> k) & 1u)) {
             continue;
         }
-        const float4 li = __ldg(lam_in + i);
-        const int act = __popc(bi);
-        const float s = dt / (float)(act > 1 ? act : 1);
-        const float mu[3] = { s * li.x, s * li.y, s * li.z };
-        const float4 pi = __ldg(x + i);
+        const float4 pi = __ldg(ri);
+        const float mu[3] = { mb.x, mb.y, mb.z };
         const float e[3] = { pi.x - pj.x, pi.y - pj.y, pi.z - pj.z };
-        const float a = ((ti != V2M_INTERIOR && tj != V2M_INTERIOR) ? fsurf : fscale) * 0.5f;
-        const float l0 = a * (__ldg(h + i) + hj);
+        const float a = ((ei < 0 && nj) ? fsurf : fscale) * 0.5f;
+        const float l0 = a * (pi.w + pj.w);
         float v[3], sa;
         bar_vjp(e, l0, a, mu, v, &sa);
         for (int d = 0; d < 3; ++d) {
@@ -367,7 +409,11 @@ __global__ void k_step_bwd_g(Dims D, const float* __restrict__ G, const float4* 
         g += (double)sa;
     }
     size_tail(D, G, pj, g, l3, gG);
-    lam_out[j] = make_float4((float)l3[0], (float)l3[1], (float)l3[2], 0.0f);
+    const float4 lo = make_float4((float)l3[0], (float)l3[1], (float)l3[2], 0.0f);
+    lam_out[j] = lo;
+    if (rec_prev) {
+        rec_prev[j] = make_rec(xh_prev[j], lo, mask_prev[j], dt);
+    }
 }
 
 __global__ void k_fix_to_float(unsigned long long* __restrict__ a, float* __restrict__ out, int m, int clear) {
@@ -380,15 +426,17 @@ __global__ void k_fix_to_float(unsigned long long* __restrict__ a, float* __rest
     }
 }
 
-__global__ void k_lists(const int* __restrict__ rowmajor, const int* __restrict__ cnt, int* __restrict__ slot,
-                        uint8_t* __restrict__ nnb, int n) {
+// row-major [n][K] lists -> slot-major, each entry flagged (bit 31) when its node is not INTERIOR
+__global__ void k_lists(const int* __restrict__ rowmajor, const int* __restrict__ cnt, const uint8_t* __restrict__ typ,
+                        int* __restrict__ slot, uint8_t* __restrict__ nnb, int n) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n * V2M_K) {
         return;
     }
     const int i = t / V2M_K, k = t % V2M_K;
     const int c = cnt[i];
-    slot[(size_t)k * n + i] = k < c ? rowmajor[t] : i;
+    const int j = k < c ? rowmajor[t] : i;
+    slot[(size_t)k * n + i] = j | (typ[j] != V2M_INTERIOR ? (int)0x80000000u : 0);
     if (k == 0) {
         nnb[i] = (uint8_t)c;
     }
@@ -403,21 +451,20 @@ struct v2m_unroll {
     Dims D{};
     float fscale = 1.2f, fsurf = 1.0f, dt = 0.2f;
     cudaStream_t stream = nullptr;
-    int* nbr = nullptr;
+    int* nbr = nullptr;              // slot-major lists, bit 31 = the neighbour is not INTERIOR
     uint8_t* nnb = nullptr;
     uint8_t* typ = nullptr;
     uint32_t* tape = nullptr;        // K x n
     float4* ck = nullptr;            // nck checkpoints x n
-    float4* seg = nullptr;           // (ckpt + 1) x n segment states
-    float* h = nullptr;
+    float4* seg = nullptr;           // (ckpt + 1) x n segment states (x, h)
     float4* lamf = nullptr;
     unsigned long long* gG = nullptr;
     double* part = nullptr;
     int* tofs = nullptr;             // transpose of the lists: n + 1 offsets
-    int* tsrc = nullptr;             // source node i of each incoming entry
+    int* tsrc = nullptr;             // source node i of each incoming entry (bit 31: i is not INTERIOR)
     uint8_t* tslot = nullptr;        // its slot k in i's list
     float4* lamb = nullptr;          // second adjoint buffer
-    float* hseg = nullptr;           // h of each state of a segment
+    Rec* rec = nullptr;              // 2 x n reverse-step records (double buffer)
     int have_tape = 0;
     float ms_fwd = 0.0f, ms_bwd = 0.0f;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -474,18 +521,13 @@ unsigned blocks(int n) {
     return (unsigned)((n + kT - 1) / kT);
 }
 
-// forward over steps [t0, t1) from x (float4), writing states to out[t - t0 + 1]
-// (out may be null: only the last state is kept in `last`)
-// (the size of every state goes to hseg[t - t0] when hseg is given, else to u->h)
-void run_steps(v2m_unroll* u, const float* G, const float4* x, int t0, int t1, float4* seg, int replay,
-               float* hseg = nullptr) {
+// forward over steps [t0, t1) from the state xh, writing state t + 1 to seg[t - t0 + 1]
+void run_steps(v2m_unroll* u, const float* G, const float4* xh, int t0, int t1, float4* seg, int replay) {
     const int n = u->n;
-    const float4* cur = x;
+    const float4* cur = xh;
     for (int t = t0; t < t1; ++t) {
         float4* nxt = seg + (size_t)(t - t0 + 1) * n;
-        float* h = hseg ? hseg + (size_t)(t - t0) * n : u->h;
-        k_size<<<blocks(n), kT, 0, u->stream>>>(u->D, G, cur, h, n);
-        k_step<<<blocks(n), kT, 0, u->stream>>>(cur, h, u->nbr, u->nnb, u->typ, u->fscale, u->fsurf, u->dt,
+        k_step<<<blocks(n), kT, 0, u->stream>>>(u->D, G, cur, u->nbr, u->nnb, u->typ, u->fscale, u->fsurf, u->dt,
                                                 u->tape + (size_t)t * n, replay, nxt, n);
         cur = nxt;
     }
@@ -547,12 +589,11 @@ int v2m_unroll_create(int64_t n, const int32_t* nbr, const int32_t* nnb, const u
             u->tape = u->alloc<uint32_t>(nn * K);
             u->ck = u->alloc<float4>(nn * u->nck);
             u->seg = u->alloc<float4>(nn * (ckpt + 1));
-            u->h = u->alloc<float>(nn);
             u->lamf = u->alloc<float4>(nn);
             u->gG = u->alloc<unsigned long long>((size_t)m[0] * m[1] * m[2]);
             u->part = u->alloc<double>(nn / kT + 1);
             u->lamb = u->alloc<float4>(nn);
-            u->hseg = u->alloc<float>(nn * (ckpt + 1));
+            u->rec = u->alloc<Rec>(2 * nn);
             // the transpose of the lists: incoming entries of every node, by (i, k)
             std::vector<int> tofs(nn + 1, 0);
             for (int64_t i = 0; i < n; ++i) {
@@ -568,7 +609,7 @@ int v2m_unroll_create(int64_t n, const int32_t* nbr, const int32_t* nnb, const u
             for (int64_t i = 0; i < n; ++i) {
                 for (int k = 0; k < nnb[i]; ++k) {
                     const int j = nbr[i * V2M_K + k];
-                    tsrc[cur[j]] = (int)i;
+                    tsrc[cur[j]] = (int)i | (typ[i] != V2M_INTERIOR ? (int)0x80000000u : 0);
                     tslot[cur[j]] = (uint8_t)k;
                     ++cur[j];
                 }
@@ -583,8 +624,8 @@ int v2m_unroll_create(int64_t n, const int32_t* nbr, const int32_t* nnb, const u
             uck(cudaMemcpyAsync(tmp, nbr, 4 * nn * V2M_K, cudaMemcpyHostToDevice, u->stream), "upload");
             uck(cudaMemcpyAsync(tmp + nn * V2M_K, nnb, 4 * nn, cudaMemcpyHostToDevice, u->stream), "upload");
             uck(cudaMemcpyAsync(u->typ, typ, nn, cudaMemcpyHostToDevice, u->stream), "upload");
-            k_lists<<<(unsigned)((nn * V2M_K + kT - 1) / kT), kT, 0, u->stream>>>(tmp, tmp + nn * V2M_K, u->nbr, u->nnb,
-                                                                               (int)n);
+            k_lists<<<(unsigned)((nn * V2M_K + kT - 1) / kT), kT, 0, u->stream>>>(tmp, tmp + nn * V2M_K, u->typ, u->nbr,
+                                                                               u->nnb, (int)n);
             uck(cudaMemsetAsync(u->gG, 0, 8 * (size_t)m[0] * m[1] * m[2], u->stream), "memset");
             uck(cudaGetLastError(), "launch");
             uck(cudaStreamSynchronize(u->stream), "synchronize");
@@ -617,7 +658,7 @@ int v2m_unroll_forward(v2m_unroll* u, const float* x0, const float* G, float* xK
         uck(cudaSetDevice(u->device), "cudaSetDevice");
         const int n = u->n;
         uck(cudaEventRecord(u->e0, u->stream), "event");
-        k_pack<<<blocks(n), kT, 0, u->stream>>>(x0, u->seg, n);
+        k_pack_size<<<blocks(n), kT, 0, u->stream>>>(u->D, G, x0, u->seg, n);
         for (int c = 0; c < u->nck; ++c) {
             const int t0 = c * u->ckpt, t1 = std::min(u->K, t0 + u->ckpt);
             uck(cudaMemcpyAsync(u->ck + (size_t)c * n, u->seg, 16 * (size_t)n, cudaMemcpyDeviceToDevice, u->stream),
@@ -642,10 +683,9 @@ int v2m_unroll_loss(v2m_unroll* u, const float* x, const float* G, double* loss)
         }
         uck(cudaSetDevice(u->device), "cudaSetDevice");
         const int n = u->n;
-        float4* x4 = u->lamf;   // scratch
-        k_pack<<<blocks(n), kT, 0, u->stream>>>(x, x4, n);
-        k_size<<<blocks(n), kT, 0, u->stream>>>(u->D, G, x4, u->h, n);
-        k_loss<<<blocks(n), kT, 0, u->stream>>>(x4, u->h, u->nbr, u->nnb, u->part, n);
+        float4* xh = u->lamf;   // scratch
+        k_pack_size<<<blocks(n), kT, 0, u->stream>>>(u->D, G, x, xh, n);
+        k_loss<<<blocks(n), kT, 0, u->stream>>>(xh, u->nbr, u->nnb, u->part, n);
         std::vector<double> part(blocks(n));
         uck(cudaMemcpyAsync(part.data(), u->part, 8 * part.size(), cudaMemcpyDeviceToHost, u->stream), "read");
         uck(cudaStreamSynchronize(u->stream), "synchronize");
@@ -666,13 +706,12 @@ int v2m_unroll_loss_backward(v2m_unroll* u, const float* x, const float* G, floa
         }
         uck(cudaSetDevice(u->device), "cudaSetDevice");
         const int n = u->n, mg = u->D.m0 * u->D.m1 * u->D.m2;
-        float4* x4 = u->seg;
-        k_pack<<<blocks(n), kT, 0, u->stream>>>(x, x4, n);
-        k_size<<<blocks(n), kT, 0, u->stream>>>(u->D, G, x4, u->h, n);
+        float4* xh = u->seg;
+        k_pack_size<<<blocks(n), kT, 0, u->stream>>>(u->D, G, x, xh, n);
         if (!accumulate) {
             uck(cudaMemsetAsync(u->gG, 0, 8 * (size_t)mg, u->stream), "memset");
         }
-        k_loss_bwd_g<<<blocks(n), kT, 0, u->stream>>>(u->D, G, x4, u->h, u->nbr, u->nnb, u->tofs, u->tsrc, gscale,
+        k_loss_bwd_g<<<blocks(n), kT, 0, u->stream>>>(u->D, G, xh, u->nbr, u->nnb, u->tofs, u->tsrc, gscale,
                                                       u->lamf, u->gG, n);
         k_unpack<<<blocks(n), kT, 0, u->stream>>>(u->lamf, gx, n);
         k_fix_to_float<<<blocks(mg), kT, 0, u->stream>>>(u->gG, gG, mg, 0);
@@ -701,17 +740,19 @@ int v2m_unroll_backward(v2m_unroll* u, const float* G, const float* gxK, float* 
             // recompute the segment's states from its checkpoint (replaying the tape)
             uck(cudaMemcpyAsync(u->seg, u->ck + (size_t)c * n, 16 * (size_t)n, cudaMemcpyDeviceToDevice, u->stream),
                 "segment");
-            run_steps(u, G, u->seg, t0, t1 - 1, u->seg, 1, u->hseg);
-            // the last state's size (run_steps stops before its step)
-            k_size<<<blocks(n), kT, 0, u->stream>>>(u->D, G, u->seg + (size_t)(t1 - 1 - t0) * n,
-                                                    u->hseg + (size_t)(t1 - 1 - t0) * n, n);
+            run_steps(u, G, u->seg, t0, t1 - 1, u->seg, 1);
+            Rec* rc = u->rec;
+            Rec* rp = u->rec + n;
+            k_rec<<<blocks(n), kT, 0, u->stream>>>(u->seg + (size_t)(t1 - 1 - t0) * n, u->lamf,
+                                                   u->tape + (size_t)(t1 - 1) * n, u->dt, rc, n);
             for (int t = t1 - 1; t >= t0; --t) {
-                const float4* xt = u->seg + (size_t)(t - t0) * n;
-                const float* ht = u->hseg + (size_t)(t - t0) * n;
-                k_step_bwd_g<<<blocks(n), kT, 0, u->stream>>>(u->D, G, xt, ht, u->nbr, u->nnb, u->typ, u->fscale,
-                                                              u->fsurf, u->dt, u->tape + (size_t)t * n, u->lamf,
-                                                              u->tofs, u->tsrc, u->tslot, u->lamb, u->gG, n);
+                const bool more = t > t0;
+                k_step_bwd_g<<<blocks(n), kT, 0, u->stream>>>(
+                    u->D, G, rc, u->lamf, u->nbr, u->typ, u->fscale, u->fsurf, u->dt, u->tofs, u->tsrc, u->tslot,
+                    u->lamb, more ? u->seg + (size_t)(t - 1 - t0) * n : nullptr,
+                    more ? u->tape + (size_t)(t - 1) * n : nullptr, more ? rp : nullptr, u->gG, n);
                 std::swap(u->lamf, u->lamb);
+                std::swap(rc, rp);
             }
         }
         k_unpack<<<blocks(n), kT, 0, u->stream>>>(u->lamf, gx0, n);

@@ -87,34 +87,6 @@ __device__ __noinline__ float phi_voxel(const DGrid& g, int l, int i, int j, int
     return __ldg(g.phi + (size_t)s * V2M_SLOT + (i & 7) + V2M_BS * ((j & 7) + V2M_BS * (k & 7)));
 }
 
-// The 8 corners of phi_l's trilinear cell at (i0,j0,k0); corner bit 0 -> +i,
-// bit 1 -> +j, bit 2 -> +k (src/opencl/v2m_grid_body.cl:159-186).
-__device__ __forceinline__ void phi_corners(const DGrid& g, int l, int i0, int j0, int k0, float* c) {
-    if (i0 >= 0 && j0 >= 0 && k0 >= 0 && i0 + 1 < g.nx && j0 + 1 < g.ny && k0 + 1 < g.nz && (i0 & 7) != 7 &&
-        (j0 & 7) != 7 && (k0 & 7) != 7) {
-        int has;
-        const int s = slot_lookup(g, brick_index(g, i0, j0, k0), l, &has);
-        if (s >= 0) {
-            const float* base = g.phi + (size_t)s * V2M_SLOT + (i0 & 7) + V2M_BS * ((j0 & 7) + V2M_BS * (k0 & 7));
-#pragma unroll
-            for (int n = 0; n < 8; ++n) {
-                c[n] = __ldg(base + (n & 1) + V2M_BS * ((n >> 1) & 1) + V2M_BS * V2M_BS * (n >> 2));
-            }
-        } else {
-#pragma unroll
-            for (int n = 0; n < 8; ++n) {
-                c[n] = (has && g.L[(i0 + (n & 1)) + (size_t)g.nx * ((j0 + ((n >> 1) & 1)) + (size_t)g.ny * (k0 + (n >> 2)))] == l)
-                           ? 1.0f : 0.0f;
-            }
-        }
-        return;
-    }
-#pragma unroll
-    for (int n = 0; n < 8; ++n) {
-        c[n] = phi_voxel(g, l, i0 + (n & 1), j0 + ((n >> 1) & 1), k0 + ((n >> 2) & 1));
-    }
-}
-
 // Trilinear blend of 8 corners at fractions (fx,fy,fz), the reference's order.
 __device__ __forceinline__ float trilerp8(const float* c, float fx, float fy, float fz) {
     const float x00 = c[0] + fx * (c[1] - c[0]), x10 = c[2] + fx * (c[3] - c[2]);
@@ -124,10 +96,12 @@ __device__ __forceinline__ float trilerp8(const float* c, float fx, float fy, fl
 }
 
 // The trilinear cell under a point, computed once and shared by every label
-// evaluated there: corner voxel, fractions and -- when the cell lies inside one
-// brick (v2m_phi_cell's fast case) -- that brick's label count, labels and
-// first slot. cell_phi gives exactly the corners v2m_phi_cell gives
-// (src/opencl/v2m_grid_body.cl:159-186), so the values are the reference's.
+// evaluated there: corner voxel, fractions and -- when the cell's base voxel
+// lies inside the grid -- its brick's corner-table list (labels, count, first
+// table). cell_corners reads the table, whose values are the reference's
+// per-voxel phi (v2m_phi_cell, src/opencl/v2m_grid_body.cl:159-186, corner by
+// corner), so the corners equal the reference's in both its one-brick case and
+// its per-corner case.
 struct Cell {
     int i0, j0, k0;
     float fx, fy, fz;
@@ -144,16 +118,21 @@ __device__ __forceinline__ void cell_at(const DGrid& g, float px, float py, floa
     c.fx = u - c.i0;
     c.fy = v - c.j0;
     c.fz = w - c.k0;
-    c.fast = c.i0 >= 0 && c.j0 >= 0 && c.k0 >= 0 && c.i0 + 1 < g.nx && c.j0 + 1 < g.ny && c.k0 + 1 < g.nz &&
-             (c.i0 & 7) != 7 && (c.j0 & 7) != 7 && (c.k0 & 7) != 7;
-    if (c.fast) {
+    c.fast = 0;
+    c.n = 0;
+    c.first = -1;
+    if (c.i0 >= 0 && c.j0 >= 0 && c.k0 >= 0 && c.i0 < g.nx && c.j0 < g.ny && c.k0 < g.nz) {
         const int b = brick_index(g, c.i0, c.j0, c.k0);
-        c.n = __ldg(g.bl_cnt + b);
-        c.ll = load_labels(g, b);
-        c.first = __ldg(g.bl_slot + b);
-    } else {
-        c.n = 0;
-        c.first = -1;
+        const int n = __ldg(g.xcnt + b);
+        if (n >= 0) {
+            c.fast = 1;
+            c.n = n;
+            const uint4* p = reinterpret_cast<const uint4*>(g.xlab + (size_t)b * V2M_BL);
+            const uint4 a = __ldg(p), e = __ldg(p + 1);
+            c.ll.w[0] = a.x; c.ll.w[1] = a.y; c.ll.w[2] = a.z; c.ll.w[3] = a.w;
+            c.ll.w[4] = e.x; c.ll.w[5] = e.y; c.ll.w[6] = e.z; c.ll.w[7] = e.w;
+            c.first = __ldg(g.xfirst + b);
+        }
     }
 }
 
@@ -176,18 +155,16 @@ __device__ __forceinline__ void cell_corners(const DGrid& g, const Cell& c, int 
     if (c.fast) {
         const int idx = lab_index(c.ll, c.n, l);
         if (idx >= 0 && c.first >= 0) {
-            const float* base = g.phi + (size_t)(c.first + idx) * V2M_SLOT + (c.i0 & 7) +
-                                V2M_BS * ((c.j0 & 7) + V2M_BS * (c.k0 & 7));
+            const float* base = g.xphi + (size_t)(c.first + idx) * 729 + (c.i0 & 7) + 9 * ((c.j0 & 7) + 9 * (c.k0 & 7));
 #pragma unroll
             for (int n = 0; n < 8; ++n) {
-                out[n] = __ldg(base + (n & 1) + V2M_BS * ((n >> 1) & 1) + V2M_BS * V2M_BS * (n >> 2));
+                out[n] = __ldg(base + (n & 1) + 9 * ((n >> 1) & 1) + 81 * (n >> 2));
             }
         } else {
+            const float f = idx >= 0 ? 1.0f : 0.0f;   // uniform table: its label everywhere; absent label: 0
 #pragma unroll
             for (int n = 0; n < 8; ++n) {
-                out[n] = (idx >= 0 && g.L[(c.i0 + (n & 1)) + (size_t)g.nx * ((c.j0 + ((n >> 1) & 1)) +
-                                                                          (size_t)g.ny * (c.k0 + (n >> 2)))] == l)
-                             ? 1.0f : 0.0f;
+                out[n] = f;
             }
         }
         return;

@@ -238,6 +238,46 @@ T* upload(v2m_session* s, const T* host, size_t count) {
     return d;
 }
 
+// The corner tables of one volume's grid (DGrid::xcnt .. xphi), built on the
+// device from the uploaded grid; the table list is laid out on the host.
+void build_corner_tables(v2m_session* s, DGrid& g, size_t nb) {
+    int* xcnt = s->alloc<int>(nb);
+    uint16_t* xlab = s->alloc<uint16_t>(nb * V2M_BL);
+    int* xfirst = s->alloc<int>(nb);
+    int* xn = nullptr;
+    ck(cudaMallocAsync((void**)&xn, 4 * std::max<size_t>(nb, 1), s->stream), "cudaMallocAsync");
+    launch_xcount(s->stream, g, xcnt, xlab, xn, (int)nb);
+    ck(cudaGetLastError(), "corner tables");
+    std::vector<int> hn(nb), first(nb, -1);
+    std::vector<uint16_t> hl(nb * V2M_BL);
+    ck(cudaMemcpyAsync(hn.data(), xn, 4 * nb, cudaMemcpyDeviceToHost, s->stream), "corner tables");
+    ck(cudaMemcpyAsync(hl.data(), xlab, 2 * nb * V2M_BL, cudaMemcpyDeviceToHost, s->stream), "corner tables");
+    ck(cudaFreeAsync(xn, s->stream), "cudaFreeAsync");
+    ck(cudaStreamSynchronize(s->stream), "synchronize");
+    std::vector<int2> tabs;
+    for (size_t b = 0; b < nb; ++b) {
+        if (hn[b] > 0) {
+            if (tabs.size() + hn[b] > (size_t)0x7FFFFFFF) {
+                throw ArgError("too many corner tables");
+            }
+            first[b] = (int)tabs.size();
+            for (int q = 0; q < hn[b]; ++q) {
+                tabs.push_back(make_int2((int)b, (int)hl[b * V2M_BL + q]));
+            }
+        }
+    }
+    const int2* dtabs = upload(s, tabs.data(), tabs.size());
+    ck(cudaMemcpyAsync(xfirst, first.data(), 4 * nb, cudaMemcpyHostToDevice, s->stream), "corner tables");
+    float* xphi = s->alloc<float>(tabs.size() * 729);
+    launch_xfill(s->stream, g, dtabs, xphi, (int)tabs.size());
+    ck(cudaGetLastError(), "corner tables");
+    ck(cudaStreamSynchronize(s->stream), "synchronize");   // (tabs and first are host vectors)
+    g.xcnt = xcnt;
+    g.xlab = xlab;
+    g.xfirst = xfirst;
+    g.xphi = xphi;
+}
+
 void init_ctl(v2m_session* s) {
     std::vector<VolCtl> c(s->nvol);
     for (int v = 0; v < s->nvol; ++v) {
@@ -400,6 +440,7 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
                 V.g.gI = nullptr;
                 V.g.gTW = s->alloc<float>(4);
             }
+            build_corner_tables(s, V.g, nb);
             V.nofs = I.nofs;
             V.n = I.n;
             V.kofs = I.kofs;

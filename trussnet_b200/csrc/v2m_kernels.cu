@@ -922,6 +922,104 @@ __global__ void __launch_bounds__(kMainThreads) k_move_main(const DVol* __restri
     }
 }
 
+// ---- corner tables (once per session) ----------------------------------------------
+// One thread per brick: the labels a cell based in the brick can meet -- the
+// brick's own and its + neighbours' listed labels, and label 0 when the
+// 9x9x9 region passes the grid's edge (phi_voxel is 1 for label 0 there) --
+// and whether the region is one label everywhere (no table needed). More than
+// 16 labels: no table (xcnt = -1; such cells take the per-corner path).
+// xn gets the number of tables the brick needs.
+__global__ void k_xcount(DGrid g, int* __restrict__ xcnt, uint16_t* __restrict__ xlab, int* __restrict__ xn, int nb) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) {
+        return;
+    }
+    const int bx = b % g.nbx, by = (b / g.nbx) % g.nby, bz = b / (g.nbx * g.nby);
+    uint16_t lst[V2M_BL];
+    int n = 0;
+    bool over = false;
+    const bool outside = bx * 8 + 8 >= g.nx || by * 8 + 8 >= g.ny || bz * 8 + 8 >= g.nz;
+    bool uni = !outside;
+    int ulab = -1;
+    for (int d = 0; d < 8; ++d) {
+        const int X = bx + (d & 1), Y = by + ((d >> 1) & 1), Z = bz + (d >> 2);
+        if (X >= g.nbx || Y >= g.nby || Z >= g.nbz) {
+            continue;   // only voxels past the grid's edge (counted by outside)
+        }
+        const int nbk = X + g.nbx * (Y + g.nby * Z);
+        const int cnt = g.bl_cnt[nbk];
+        const int c = cnt < V2M_BL ? cnt : V2M_BL;
+        if (!(cnt == 1 && g.bl_slot[nbk] < 0)) {
+            uni = false;
+        }
+        for (int k = 0; k < c; ++k) {
+            const int l = g.bl_lab[(size_t)nbk * V2M_BL + k];
+            if (ulab < 0) {
+                ulab = l;
+            } else if (l != ulab) {
+                uni = false;
+            }
+            bool have = false;
+            for (int q = 0; q < n; ++q) {
+                have |= lst[q] == l;
+            }
+            if (!have) {
+                if (n < V2M_BL) {
+                    lst[n++] = (uint16_t)l;
+                } else {
+                    over = true;
+                }
+            }
+        }
+    }
+    if (outside) {
+        bool have = false;
+        for (int q = 0; q < n; ++q) {
+            have |= lst[q] == 0;
+        }
+        if (!have) {
+            if (n < V2M_BL) {
+                lst[n++] = 0;
+            } else {
+                over = true;
+            }
+        }
+    }
+    if (uni && ulab >= 0) {
+        // a uniform region must hold its label in every voxel (phi_voxel reads L there)
+        for (int e = 0; e < 729 && uni; ++e) {
+            const int i = bx * 8 + e % 9, j = by * 8 + (e / 9) % 9, k = bz * 8 + e / 81;
+            uni = g.L[i + (size_t)g.nx * (j + (size_t)g.ny * k)] == ulab;
+        }
+    } else {
+        uni = false;
+    }
+    for (int q = 0; q < V2M_BL; ++q) {
+        xlab[(size_t)b * V2M_BL + q] = q < n ? lst[q] : (uint16_t)0;
+    }
+    if (over) {
+        xcnt[b] = -1;
+        xn[b] = 0;
+    } else if (uni) {
+        xlab[(size_t)b * V2M_BL] = (uint16_t)ulab;
+        xcnt[b] = 1;
+        xn[b] = 0;
+    } else {
+        xcnt[b] = n;
+        xn[b] = n;
+    }
+}
+
+// One block per table (brick, label): its 729 voxel values by phi_voxel.
+__global__ void k_xfill(DGrid g, const int2* __restrict__ tabs, float* __restrict__ xphi) {
+    const int t = blockIdx.x;
+    const int2 bl = tabs[t];
+    const int bx = bl.x % g.nbx, by = (bl.x / g.nbx) % g.nby, bz = bl.x / (g.nbx * g.nby);
+    for (int e = threadIdx.x; e < 729; e += blockDim.x) {
+        xphi[(size_t)t * 729 + e] = phi_voxel(g, bl.y, bx * 8 + e % 9, by * 8 + (e / 9) % 9, bz * 8 + e / 81);
+    }
+}
+
 // Serial FIRE power (the CPU's order: node 0 first, one double accumulator),
 // for bit-exact replays; one thread per volume.
 __global__ void k_power_serial(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl, const float* __restrict__ pw,
@@ -1216,6 +1314,16 @@ void launch_move(cudaStream_t s, const Dev& d) {
                                                                 d.N);
     k_move_main<<<nblk(d.N, kMainThreads), kMainThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.Vel, d.typ, d.lab,
                                                                  d.part, d.mv, d.P0, d.S, d.queue, d.rlist, d.G, d.N);
+}
+
+void launch_xcount(cudaStream_t s, const DGrid& g, int* xcnt, uint16_t* xlab, int* xn, int nb) {
+    k_xcount<<<nblk(nb, 128), 128, 0, s>>>(g, xcnt, xlab, xn, nb);
+}
+
+void launch_xfill(cudaStream_t s, const DGrid& g, const int2* tabs, float* xphi, int ntab) {
+    if (ntab > 0) {
+        k_xfill<<<ntab, 256, 0, s>>>(g, tabs, xphi);
+    }
 }
 
 void launch_control(cudaStream_t s, const Dev& d, int serial) {

@@ -35,6 +35,15 @@ struct DGrid {
     const float* gI;
     const float* gTW;
     int gm;
+    // Corner tables (built once per session): for every brick, the labels met by
+    // a trilinear cell based in it (its own, its + neighbours' and, past the
+    // grid's edge, label 0) and, per label, the 9x9x9 voxel values of the brick
+    // plus a one-voxel halo on the + sides, each the reference's per-voxel phi.
+    // Any cell based inside the grid then reads its 8 corners from one table.
+    const int* xcnt;        // labels listed; -1: no table (the per-corner path)
+    const uint16_t* xlab;   // 16 per brick
+    const int* xfirst;      // first table of the brick; -1: uniform (label xlab[0] is 1 at every corner)
+    const float* xphi;      // 729 floats per table, x fastest
 };
 
 // Multi-level hash geometry (V2mHash, src/opencl/v2m_particle_body.cl:21-27).
