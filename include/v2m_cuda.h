@@ -236,7 +236,8 @@ int v2m_session_queue_sizes(v2m_session* s, int32_t* trapped, int32_t* interior)
  * are taped by the forward pass and replayed by the backward pass; checkpoints
  * every `ckpt` steps. Loss = sum over the list entries of (l_ij / h_ij - 1)^2.
  * Position, gradient and grid arrays are DEVICE pointers (float, x/y/z
- * interleaved per node); the calls synchronize before returning.
+ * interleaved per node); the calls synchronize before returning. At most 2^29
+ * nodes, and no node in more than 255 lists.
  */
 typedef struct v2m_unroll v2m_unroll;
 int v2m_unroll_create(int64_t n, const int32_t* nbr, const int32_t* nnb, const uint8_t* typ, const int32_t* m,

@@ -155,7 +155,10 @@ __global__ void k_unpack(const float4* __restrict__ x4, float* __restrict__ x3, 
 
 // one step xh -> yh (the new state's sizes included); records (replay = 0) or
 // replays the active-bar masks. A replay visits only the taped bars, in the same
-// ascending slot order as the recording.
+// ascending slot order as the recording. Ids and positions are loaded kB at a
+// time (independent gathers in flight); the bars are added in slot order.
+constexpr int kB = 4;
+
 __global__ void k_step(Dims D, const float* __restrict__ G, const float4* __restrict__ xh,
                        const int* __restrict__ nbrf, const uint8_t* __restrict__ nnb, const uint8_t* __restrict__ typ,
                        float fscale, float fsurf, float dt, uint32_t* __restrict__ mask, int replay,
@@ -176,39 +179,53 @@ __global__ void k_step(Dims D, const float* __restrict__ G, const float4* __rest
     const bool ni = ti != V2M_INTERIOR;
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
     int act = 0;
-    if (replay) {
-        for (uint32_t b = mask[i]; b; b &= b - 1u) {
-            const int k = __ffs(b) - 1;
-            const int e = __ldg(nbrf + (size_t)k * n + i);
-            const float4 q = __ldg(xh + (e & kIdMask));
-            const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
-            const float l = sqrtf(ex * ex + ey * ey + ez * ez);
-            const float l0 = ((ni && e < 0) ? fsurf : fscale) * 0.5f * (p.w + q.w);
-            const float f = (l0 - l) / l;
-            fx += f * ex;
-            fy += f * ey;
-            fz += f * ez;
-            ++act;
-        }
-    } else {
-        uint32_t bits = 0u;
-        const int c = nnb[i];
-        for (int k = 0; k < c; ++k) {
-            const int e = __ldg(nbrf + (size_t)k * n + i);
-            const float4 q = __ldg(xh + (e & kIdMask));
-            const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
-            const float l = sqrtf(ex * ex + ey * ey + ez * ez);
-            const float l0 = ((ni && e < 0) ? fsurf : fscale) * 0.5f * (p.w + q.w);
-            if (!(l < l0 && l > 0.0f)) {
-                continue;
+    // the slots to visit: every listed one (recording) or the taped ones (replay)
+    const int c = nnb[i];
+    uint32_t todo = replay ? mask[i] : (c >= 32 ? 0xFFFFFFFFu : ((1u << c) - 1u));
+    uint32_t bits = 0u;
+    while (todo) {
+        int ks[kB], es[kB];
+        float4 qs[kB];
+        int m = 0;
+#pragma unroll
+        for (int q = 0; q < kB; ++q) {
+            ks[q] = -1;
+            if (todo) {
+                ks[q] = __ffs(todo) - 1;
+                todo &= todo - 1u;
+                m = q + 1;
             }
-            bits |= 1u << k;
-            const float f = (l0 - l) / l;
-            fx += f * ex;
-            fy += f * ey;
-            fz += f * ez;
-            ++act;
         }
+#pragma unroll
+        for (int q = 0; q < kB; ++q) {
+            if (q < m) {
+                es[q] = __ldg(nbrf + (size_t)ks[q] * n + i);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kB; ++q) {
+            if (q < m) {
+                qs[q] = __ldg(xh + (es[q] & kIdMask));
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kB; ++q) {
+            if (q < m) {
+                const float ex = p.x - qs[q].x, ey = p.y - qs[q].y, ez = p.z - qs[q].z;
+                const float l = sqrtf(ex * ex + ey * ey + ez * ez);
+                const float l0 = ((ni && es[q] < 0) ? fsurf : fscale) * 0.5f * (p.w + qs[q].w);
+                if (replay || (l < l0 && l > 0.0f)) {
+                    bits |= 1u << ks[q];
+                    const float f = (l0 - l) / l;
+                    fx += f * ex;
+                    fy += f * ey;
+                    fz += f * ez;
+                    ++act;
+                }
+            }
+        }
+    }
+    if (!replay) {
         mask[i] = bits;
     }
     const float s = dt / (float)(act > 1 ? act : 1);
@@ -302,7 +319,7 @@ __device__ __forceinline__ void size_tail(const Dims& D, const float* __restrict
 // d(loss)/dx and d(loss)/dh at x (loss = sum over list entries of (l/hm - 1)^2)
 __global__ void k_loss_bwd_g(Dims D, const float* __restrict__ G, const float4* __restrict__ xh,
                              const int* __restrict__ nbrf, const uint8_t* __restrict__ nnb,
-                             const int* __restrict__ tofs, const int* __restrict__ tsrcf, float gscale,
+                             const uint8_t* __restrict__ indeg, const int* __restrict__ tsrcf, float gscale,
                              float4* __restrict__ lam, unsigned long long* __restrict__ gG, int n) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) {
@@ -324,8 +341,9 @@ __global__ void k_loss_bwd_g(Dims D, const float* __restrict__ G, const float4* 
         g += 0.5 * (double)dhm;
     }
     // entries pointing at j (i -> j): - dl e/l
-    for (int t = tofs[j]; t < tofs[j + 1]; ++t) {
-        const float4 pi = __ldg(xh + (__ldg(tsrcf + t) & kIdMask));
+    const int cin = indeg[j];
+    for (int t = 0; t < cin; ++t) {
+        const float4 pi = __ldg(xh + (__ldg(tsrcf + (size_t)t * n + j) & kIdMask));
         const float e[3] = { pi.x - pj.x, pi.y - pj.y, pi.z - pj.z };
         const float l = sqrtf(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
         const float hm = 0.5f * (pi.w + pj.w);
@@ -340,79 +358,171 @@ __global__ void k_loss_bwd_g(Dims D, const float* __restrict__ G, const float4* 
     lam[j] = make_float4((float)l3[0], (float)l3[1], (float)l3[2], 0.0f);
 }
 
-// one bar's reverse terms: v = (d phi / d e)^T mu and s = (e . mu) / l
+// one bar's reverse terms: v = (d phi / d e)^T mu and s = (e . mu) / l, with
+// phi = f e, f = (l0 - l) / l (the hardware reciprocal square root of l^2, a
+// few ulps: the reverse pass needs the FP64 gradient to 1e-4, not bit-parity)
 __device__ __forceinline__ void bar_vjp(const float* e, float l0, float a, const float* mu, float* v, float* sa) {
-    const float l = sqrtf(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
-    const float f = (l0 - l) / l, dfl = -l0 / (l * l);
+    const float l2 = e[0] * e[0] + e[1] * e[1] + e[2] * e[2];
+    const float il = rsqrtf(l2);
+    const float l = l2 * il;
+    const float f = (l0 - l) * il;
     const float em = e[0] * mu[0] + e[1] * mu[1] + e[2] * mu[2];
+    const float c = -l0 * il * il * il * em;   // d f / d l * (e . mu) / l
     for (int d = 0; d < 3; ++d) {
-        v[d] = f * mu[d] + e[d] / l * dfl * em;
+        v[d] = f * mu[d] + c * e[d];
     }
-    *sa = a * (em / l);
+    *sa = a * em * il;
 }
 
 // reverse of step t: lam_in = dL/dx_{t+1} -> lam_out = dL/dx_t (with the size
-// term). When step t - 1 follows in the same segment, the thread also writes
-// node j's record for it (state x_{t-1}, mask_{t-1}, mu from lam_out).
-__global__ void k_step_bwd_g(Dims D, const float* __restrict__ G, const Rec* __restrict__ rec,
+// term). kRoles threads per node, in different warps of the block: for the
+// block's kBwdNodes nodes, role 0 sums each node's own taped bars and roles
+// 1 .. kRoles-1 consecutive parts of the taped bars pointing at it, each in
+// its fixed order (in float: the node's result is a float) with kB gathers in
+// flight (kRoles = 2: one thread for the own bars, one for the incoming ones;
+// more roles only duplicate the per-node loads). The other roles hand their
+// sums over through shared memory; role 0
+// adds them in role order, then the size term. When step t - 1 follows in the
+// same segment, it also writes node j's record for it (state x_{t-1},
+// mask_{t-1}, mu from lam_out).
+constexpr int kRoles = 2;
+constexpr int kBwdNodes = kT / kRoles;
+
+__global__ void __launch_bounds__(kT, 4) k_step_bwd_g(Dims D, const float* __restrict__ G, const Rec* __restrict__ rec,
                              const float4* __restrict__ lam_in, const int* __restrict__ nbrf,
                              const uint8_t* __restrict__ typ, float fscale, float fsurf, float dt,
-                             const int* __restrict__ tofs, const int* __restrict__ tsrcf,
+                             const uint8_t* __restrict__ indeg, const int* __restrict__ tsrcf,
                              const uint8_t* __restrict__ tslot, float4* __restrict__ lam_out,
                              const float4* __restrict__ xh_prev, const uint32_t* __restrict__ mask_prev,
                              Rec* __restrict__ rec_prev, unsigned long long* __restrict__ gG, int n) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) {
+    __shared__ float hand[kRoles - 1][4][kBwdNodes];
+    const int slot = threadIdx.x % kBwdNodes;
+    const int role = threadIdx.x / kBwdNodes;   // warp-uniform
+    const int j = blockIdx.x * kBwdNodes + slot;
+    float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, ag = 0.0f;
+    Rec rj;
+    rj.xh = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    bool nj = false;
+    if (j < n) {
+        rj = rec[j];
+        nj = typ[j] != V2M_INTERIOR;
+        const float4 pj = rj.xh;
+        if (role == 0) {
+            // own bars (a CORNER's mask is empty): + v
+            const float mu[3] = { rj.mub.x, rj.mub.y, rj.mub.z };
+            uint32_t todo = __float_as_uint(rj.mub.w);
+            while (todo) {
+                int es[kB];
+                float4 qs[kB];
+                int ks[kB], m = 0;
+#pragma unroll
+                for (int q = 0; q < kB; ++q) {
+                    ks[q] = 0;
+                    if (todo) {
+                        ks[q] = __ffs(todo) - 1;
+                        todo &= todo - 1u;
+                        m = q + 1;
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < kB; ++q) {
+                    if (q < m) {
+                        es[q] = __ldg(nbrf + (size_t)ks[q] * n + j);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < kB; ++q) {
+                    if (q < m) {
+                        qs[q] = __ldg(&rec[es[q] & kIdMask].xh);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < kB; ++q) {
+                    if (q < m) {
+                        const float e[3] = { pj.x - qs[q].x, pj.y - qs[q].y, pj.z - qs[q].z };
+                        const float a = ((nj && es[q] < 0) ? fsurf : fscale) * 0.5f;
+                        const float l0 = a * (pj.w + qs[q].w);
+                        float v[3], sa;
+                        bar_vjp(e, l0, a, mu, v, &sa);
+                        a0 += v[0];
+                        a1 += v[1];
+                        a2 += v[2];
+                        ag += sa;
+                    }
+                }
+            }
+        } else {
+            // the role's part of the bars pointing at j: - v
+            const int cin = indeg[j];
+            const int part = (cin + kRoles - 2) / (kRoles - 1);
+            const int t0 = (role - 1) * part, t1 = min(cin, t0 + part);
+            for (int t = t0; t < t1; t += kB) {
+                int es[kB], ks[kB];
+                float4 mb[kB];
+#pragma unroll
+                for (int q = 0; q < kB; ++q) {
+                    if (t + q < t1) {
+                        es[q] = __ldg(tsrcf + (size_t)(t + q) * n + j);
+                        ks[q] = __ldg(tslot + (size_t)(t + q) * n + j);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < kB; ++q) {
+                    if (t + q < t1) {
+                        mb[q] = __ldg(reinterpret_cast<const float4*>(rec + (es[q] & kIdMask)) + 1);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < kB; ++q) {
+                    if (t + q < t1 && ((__float_as_uint(mb[q].w) >> ks[q]) & 1u)) {
+                        const float4 pi = __ldg(reinterpret_cast<const float4*>(rec + (es[q] & kIdMask)));
+                        const float mu[3] = { mb[q].x, mb[q].y, mb[q].z };
+                        const float e[3] = { pi.x - pj.x, pi.y - pj.y, pi.z - pj.z };
+                        const float a = ((es[q] < 0 && nj) ? fsurf : fscale) * 0.5f;
+                        const float l0 = a * (pi.w + pj.w);
+                        float v[3], sa;
+                        bar_vjp(e, l0, a, mu, v, &sa);
+                        a0 -= v[0];
+                        a1 -= v[1];
+                        a2 -= v[2];
+                        ag += sa;
+                    }
+                }
+            }
+        }
+    }
+    if (role > 0) {
+        hand[role - 1][0][slot] = a0;
+        hand[role - 1][1][slot] = a1;
+        hand[role - 1][2][slot] = a2;
+        hand[role - 1][3][slot] = ag;
+    }
+    __syncthreads();
+    if (j >= n || role > 0) {
         return;
     }
+    double s0 = a0, s1 = a1, s2 = a2, sg = ag;
+#pragma unroll
+    for (int r = 0; r < kRoles - 1; ++r) {
+        s0 += (double)hand[r][0][slot];
+        s1 += (double)hand[r][1][slot];
+        s2 += (double)hand[r][2][slot];
+        sg += (double)hand[r][3][slot];
+    }
     const float4 lj = lam_in[j];
-    double l3[3] = { (double)lj.x, (double)lj.y, (double)lj.z }, g = 0.0;
-    const Rec rj = rec[j];
-    const float4 pj = rj.xh;
-    const bool nj = typ[j] != V2M_INTERIOR;
-    {
-        // own bars (a CORNER's mask is empty)
-        const float mu[3] = { rj.mub.x, rj.mub.y, rj.mub.z };
-        for (uint32_t b = __float_as_uint(rj.mub.w); b; b &= b - 1u) {
-            const int k = __ffs(b) - 1;
-            const int em = __ldg(nbrf + (size_t)k * n + j);
-            const float4 q = __ldg(&rec[em & kIdMask].xh);
-            const float e[3] = { pj.x - q.x, pj.y - q.y, pj.z - q.z };
-            const float a = ((nj && em < 0) ? fsurf : fscale) * 0.5f;
-            const float l0 = a * (pj.w + q.w);
-            float v[3], sa;
-            bar_vjp(e, l0, a, mu, v, &sa);
-            for (int d = 0; d < 3; ++d) {
-                l3[d] += (double)v[d];
-            }
-            g += (double)sa;
-        }
-    }
-    for (int t = tofs[j]; t < tofs[j + 1]; ++t) {
-        const int ei = __ldg(tsrcf + t);
-        const int k = __ldg(tslot + t);
-        const float4* ri = reinterpret_cast<const float4*>(rec + (ei & kIdMask));
-        const float4 mb = __ldg(ri + 1);
-        if (!((__float_as_uint(mb.w) >> k) & 1u)) {
-            continue;
-        }
-        const float4 pi = __ldg(ri);
-        const float mu[3] = { mb.x, mb.y, mb.z };
-        const float e[3] = { pi.x - pj.x, pi.y - pj.y, pi.z - pj.z };
-        const float a = ((ei < 0 && nj) ? fsurf : fscale) * 0.5f;
-        const float l0 = a * (pi.w + pj.w);
-        float v[3], sa;
-        bar_vjp(e, l0, a, mu, v, &sa);
-        for (int d = 0; d < 3; ++d) {
-            l3[d] -= (double)v[d];
-        }
-        g += (double)sa;
-    }
-    size_tail(D, G, pj, g, l3, gG);
+    double l3[3] = { (double)lj.x + s0, (double)lj.y + s1, (double)lj.z + s2 };
+    size_tail(D, G, rj.xh, sg, l3, gG);
     const float4 lo = make_float4((float)l3[0], (float)l3[1], (float)l3[2], 0.0f);
     lam_out[j] = lo;
     if (rec_prev) {
         rec_prev[j] = make_rec(xh_prev[j], lo, mask_prev[j], dt);
+    }
+}
+
+__global__ void k_add(float* __restrict__ a, const float* __restrict__ b, int m) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) {
+        a[i] += b[i];
     }
 }
 
@@ -451,17 +561,23 @@ struct v2m_unroll {
     Dims D{};
     float fscale = 1.2f, fsurf = 1.0f, dt = 0.2f;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;  // the backward pass's segment recomputation
+    std::vector<cudaEvent_t> seg_ready, seg_done;   // per segment: recomputed (stream2), walked back (stream)
     int* nbr = nullptr;              // slot-major lists, bit 31 = the neighbour is not INTERIOR
     uint8_t* nnb = nullptr;
     uint8_t* typ = nullptr;
     uint32_t* tape = nullptr;        // K x n
     float4* ck = nullptr;            // nck checkpoints x n
     float4* seg = nullptr;           // (ckpt + 1) x n segment states (x, h)
+    float4* seg2 = nullptr;          // a second segment buffer (the backward pass alternates)
     float4* lamf = nullptr;
     unsigned long long* gG = nullptr;
     double* part = nullptr;
-    int* tofs = nullptr;             // transpose of the lists: n + 1 offsets
-    int* tsrc = nullptr;             // source node i of each incoming entry (bit 31: i is not INTERIOR)
+    // transpose of the lists, slot-major like nbr: node j's t-th incoming entry
+    // (by ascending i, then k) at [t * n + j], t < indeg[j] <= maxin
+    int maxin = 0;
+    uint8_t* indeg = nullptr;
+    int* tsrc = nullptr;             // its source node i (bit 31: i is not INTERIOR)
     uint8_t* tslot = nullptr;        // its slot k in i's list
     float4* lamb = nullptr;          // second adjoint buffer
     Rec* rec = nullptr;              // 2 x n reverse-step records (double buffer)
@@ -485,6 +601,15 @@ struct v2m_unroll {
         if (e0) {
             cudaEventDestroy(e0);
             cudaEventDestroy(e1);
+        }
+        for (cudaEvent_t e : seg_ready) {
+            cudaEventDestroy(e);
+        }
+        for (cudaEvent_t e : seg_done) {
+            cudaEventDestroy(e);
+        }
+        if (stream2) {
+            cudaStreamDestroy(stream2);
         }
         if (stream) {
             cudaStreamDestroy(stream);
@@ -522,12 +647,13 @@ unsigned blocks(int n) {
 }
 
 // forward over steps [t0, t1) from the state xh, writing state t + 1 to seg[t - t0 + 1]
-void run_steps(v2m_unroll* u, const float* G, const float4* xh, int t0, int t1, float4* seg, int replay) {
+void run_steps(v2m_unroll* u, const float* G, const float4* xh, int t0, int t1, float4* seg, int replay,
+               cudaStream_t st) {
     const int n = u->n;
     const float4* cur = xh;
     for (int t = t0; t < t1; ++t) {
         float4* nxt = seg + (size_t)(t - t0 + 1) * n;
-        k_step<<<blocks(n), kT, 0, u->stream>>>(u->D, G, cur, u->nbr, u->nnb, u->typ, u->fscale, u->fsurf, u->dt,
+        k_step<<<blocks(n), kT, 0, st>>>(u->D, G, cur, u->nbr, u->nnb, u->typ, u->fscale, u->fsurf, u->dt,
                                                 u->tape + (size_t)t * n, replay, nxt, n);
         cur = nxt;
     }
@@ -545,7 +671,7 @@ int v2m_unroll_create(int64_t n, const int32_t* nbr, const int32_t* nnb, const u
                       const float* cs, float fscale, float fsurf, float dt, int K, int ckpt, int device,
                       v2m_unroll** out) {
     return uguard([&] {
-        if (!out || n < 1 || n > (1 << 30) || !nbr || !nnb || !typ || !m || !cs || K < 1 || ckpt < 1) {
+        if (!out || n < 1 || n > (1 << 29) || !nbr || !nnb || !typ || !m || !cs || K < 1 || ckpt < 1) {
             throw std::invalid_argument("bad argument");
         }
         if (m[0] < 1 || m[1] < 1 || m[2] < 1 || !(cs[0] > 0 && cs[1] > 0 && cs[2] > 0)) {
@@ -580,6 +706,13 @@ int v2m_unroll_create(int64_t n, const int32_t* nbr, const int32_t* nnb, const u
             u->fsurf = fsurf;
             u->dt = dt;
             uck(cudaStreamCreateWithFlags(&u->stream, cudaStreamNonBlocking), "stream");
+            uck(cudaStreamCreateWithFlags(&u->stream2, cudaStreamNonBlocking), "stream");
+            u->seg_ready.assign(u->nck, nullptr);
+            u->seg_done.assign(u->nck, nullptr);
+            for (int c = 0; c < u->nck; ++c) {
+                uck(cudaEventCreateWithFlags(&u->seg_ready[c], cudaEventDisableTiming), "event");
+                uck(cudaEventCreateWithFlags(&u->seg_done[c], cudaEventDisableTiming), "event");
+            }
             uck(cudaEventCreate(&u->e0), "event");
             uck(cudaEventCreate(&u->e1), "event");
             const size_t nn = (size_t)n;
@@ -589,35 +722,39 @@ int v2m_unroll_create(int64_t n, const int32_t* nbr, const int32_t* nnb, const u
             u->tape = u->alloc<uint32_t>(nn * K);
             u->ck = u->alloc<float4>(nn * u->nck);
             u->seg = u->alloc<float4>(nn * (ckpt + 1));
+            u->seg2 = u->alloc<float4>(nn * (ckpt + 1));
             u->lamf = u->alloc<float4>(nn);
             u->gG = u->alloc<unsigned long long>((size_t)m[0] * m[1] * m[2]);
             u->part = u->alloc<double>(nn / kT + 1);
             u->lamb = u->alloc<float4>(nn);
             u->rec = u->alloc<Rec>(2 * nn);
             // the transpose of the lists: incoming entries of every node, by (i, k)
-            std::vector<int> tofs(nn + 1, 0);
+            std::vector<int> deg(nn, 0);
             for (int64_t i = 0; i < n; ++i) {
                 for (int k = 0; k < nnb[i]; ++k) {
-                    ++tofs[nbr[i * V2M_K + k] + 1];
+                    ++deg[nbr[i * V2M_K + k]];
                 }
             }
-            for (size_t j = 0; j < nn; ++j) {
-                tofs[j + 1] += tofs[j];
+            const int maxin = std::max(1, *std::max_element(deg.begin(), deg.end()));
+            if (maxin > 255) {
+                throw std::invalid_argument("a node is in more than 255 lists");
             }
-            std::vector<int> cur(tofs.begin(), tofs.end() - 1), tsrc(std::max(tofs[nn], 1));
-            std::vector<uint8_t> tslot(std::max(tofs[nn], 1));
+            u->maxin = maxin;
+            std::vector<int> tsrc(nn * maxin, 0);
+            std::vector<uint8_t> tslot(nn * maxin, 0), indeg(nn, 0);
             for (int64_t i = 0; i < n; ++i) {
                 for (int k = 0; k < nnb[i]; ++k) {
                     const int j = nbr[i * V2M_K + k];
-                    tsrc[cur[j]] = (int)i | (typ[i] != V2M_INTERIOR ? (int)0x80000000u : 0);
-                    tslot[cur[j]] = (uint8_t)k;
-                    ++cur[j];
+                    const size_t e = (size_t)indeg[j] * nn + j;
+                    tsrc[e] = (int)i | (typ[i] != V2M_INTERIOR ? (int)0x80000000u : 0);
+                    tslot[e] = (uint8_t)k;
+                    ++indeg[j];
                 }
             }
-            u->tofs = u->alloc<int>(nn + 1);
+            u->indeg = u->alloc<uint8_t>(nn);
             u->tsrc = u->alloc<int>(tsrc.size());
             u->tslot = u->alloc<uint8_t>(tslot.size());
-            uck(cudaMemcpy(u->tofs, tofs.data(), 4 * (nn + 1), cudaMemcpyHostToDevice), "upload");
+            uck(cudaMemcpy(u->indeg, indeg.data(), nn, cudaMemcpyHostToDevice), "upload");
             uck(cudaMemcpy(u->tsrc, tsrc.data(), 4 * tsrc.size(), cudaMemcpyHostToDevice), "upload");
             uck(cudaMemcpy(u->tslot, tslot.data(), tslot.size(), cudaMemcpyHostToDevice), "upload");
             int* tmp = u->alloc<int>(nn * V2M_K + nn);
@@ -663,7 +800,7 @@ int v2m_unroll_forward(v2m_unroll* u, const float* x0, const float* G, float* xK
             const int t0 = c * u->ckpt, t1 = std::min(u->K, t0 + u->ckpt);
             uck(cudaMemcpyAsync(u->ck + (size_t)c * n, u->seg, 16 * (size_t)n, cudaMemcpyDeviceToDevice, u->stream),
                 "checkpoint");
-            run_steps(u, G, u->ck + (size_t)c * n, t0, t1, u->seg, replay);
+            run_steps(u, G, u->ck + (size_t)c * n, t0, t1, u->seg, replay, u->stream);
             uck(cudaMemcpyAsync(u->seg, u->seg + (size_t)(t1 - t0) * n, 16 * (size_t)n, cudaMemcpyDeviceToDevice,
                                 u->stream), "segment");
         }
@@ -711,7 +848,7 @@ int v2m_unroll_loss_backward(v2m_unroll* u, const float* x, const float* G, floa
         if (!accumulate) {
             uck(cudaMemsetAsync(u->gG, 0, 8 * (size_t)mg, u->stream), "memset");
         }
-        k_loss_bwd_g<<<blocks(n), kT, 0, u->stream>>>(u->D, G, xh, u->nbr, u->nnb, u->tofs, u->tsrc, gscale,
+        k_loss_bwd_g<<<blocks(n), kT, 0, u->stream>>>(u->D, G, xh, u->nbr, u->nnb, u->indeg, u->tsrc, gscale,
                                                       u->lamf, u->gG, n);
         k_unpack<<<blocks(n), kT, 0, u->stream>>>(u->lamf, gx, n);
         k_fix_to_float<<<blocks(mg), kT, 0, u->stream>>>(u->gG, gG, mg, 0);
@@ -735,25 +872,45 @@ int v2m_unroll_backward(v2m_unroll* u, const float* G, const float* gxK, float* 
         uck(cudaEventRecord(u->e0, u->stream), "event");
         uck(cudaMemsetAsync(u->gG, 0, 8 * (size_t)mg, u->stream), "memset");
         k_pack<<<blocks(n), kT, 0, u->stream>>>(gxK, u->lamf, n);
-        for (int c = u->nck - 1; c >= 0; --c) {
+        // Segment c's states are recomputed from its checkpoint on stream2 into
+        // buffer c % 2 while stream walks segment c + 1 back from the other buffer:
+        // the recomputation waits for the walk that last used its buffer, the
+        // walk for its segment's recomputation.
+        float4* buf[2] = { u->seg, u->seg2 };
+        uck(cudaStreamWaitEvent(u->stream2, u->e0, 0), "wait");
+        auto recompute = [&](int c) {
             const int t0 = c * u->ckpt, t1 = std::min(u->K, t0 + u->ckpt);
-            // recompute the segment's states from its checkpoint (replaying the tape)
-            uck(cudaMemcpyAsync(u->seg, u->ck + (size_t)c * n, 16 * (size_t)n, cudaMemcpyDeviceToDevice, u->stream),
+            float4* b = buf[c & 1];
+            if (c + 2 < u->nck) {
+                uck(cudaStreamWaitEvent(u->stream2, u->seg_done[c + 2], 0), "wait");
+            }
+            uck(cudaMemcpyAsync(b, u->ck + (size_t)c * n, 16 * (size_t)n, cudaMemcpyDeviceToDevice, u->stream2),
                 "segment");
-            run_steps(u, G, u->seg, t0, t1 - 1, u->seg, 1);
+            run_steps(u, G, b, t0, t1 - 1, b, 1, u->stream2);
+            uck(cudaEventRecord(u->seg_ready[c], u->stream2), "event");
+        };
+        recompute(u->nck - 1);
+        for (int c = u->nck - 1; c >= 0; --c) {
+            if (c > 0) {
+                recompute(c - 1);
+            }
+            const int t0 = c * u->ckpt, t1 = std::min(u->K, t0 + u->ckpt);
+            float4* b = buf[c & 1];
+            uck(cudaStreamWaitEvent(u->stream, u->seg_ready[c], 0), "wait");
             Rec* rc = u->rec;
             Rec* rp = u->rec + n;
-            k_rec<<<blocks(n), kT, 0, u->stream>>>(u->seg + (size_t)(t1 - 1 - t0) * n, u->lamf,
+            k_rec<<<blocks(n), kT, 0, u->stream>>>(b + (size_t)(t1 - 1 - t0) * n, u->lamf,
                                                    u->tape + (size_t)(t1 - 1) * n, u->dt, rc, n);
             for (int t = t1 - 1; t >= t0; --t) {
                 const bool more = t > t0;
-                k_step_bwd_g<<<blocks(n), kT, 0, u->stream>>>(
-                    u->D, G, rc, u->lamf, u->nbr, u->typ, u->fscale, u->fsurf, u->dt, u->tofs, u->tsrc, u->tslot,
-                    u->lamb, more ? u->seg + (size_t)(t - 1 - t0) * n : nullptr,
+                k_step_bwd_g<<<(unsigned)((n + kBwdNodes - 1) / kBwdNodes), kT, 0, u->stream>>>(
+                    u->D, G, rc, u->lamf, u->nbr, u->typ, u->fscale, u->fsurf, u->dt, u->indeg, u->tsrc, u->tslot,
+                    u->lamb, more ? b + (size_t)(t - 1 - t0) * n : nullptr,
                     more ? u->tape + (size_t)(t - 1) * n : nullptr, more ? rp : nullptr, u->gG, n);
                 std::swap(u->lamf, u->lamb);
                 std::swap(rc, rp);
             }
+            uck(cudaEventRecord(u->seg_done[c], u->stream), "event");
         }
         k_unpack<<<blocks(n), kT, 0, u->stream>>>(u->lamf, gx0, n);
         k_fix_to_float<<<blocks(mg), kT, 0, u->stream>>>(u->gG, gG, mg, 1);
@@ -762,13 +919,9 @@ int v2m_unroll_backward(v2m_unroll* u, const float* G, const float* gxK, float* 
         uck(cudaStreamSynchronize(u->stream), "synchronize");
         uck(cudaEventElapsedTime(&u->ms_bwd, u->e0, u->e1), "elapsed");
         if (gG_in) {
-            std::vector<float> a(mg), b(mg);
-            uck(cudaMemcpy(a.data(), gG, 4 * (size_t)mg, cudaMemcpyDeviceToHost), "read");
-            uck(cudaMemcpy(b.data(), gG_in, 4 * (size_t)mg, cudaMemcpyDeviceToHost), "read");
-            for (int i = 0; i < mg; ++i) {
-                a[i] += b[i];
-            }
-            uck(cudaMemcpy(gG, a.data(), 4 * (size_t)mg, cudaMemcpyHostToDevice), "write");
+            k_add<<<blocks(mg), kT, 0, u->stream>>>(gG, gG_in, mg);
+            uck(cudaGetLastError(), "launch");
+            uck(cudaStreamSynchronize(u->stream), "synchronize");
         }
     });
 }
