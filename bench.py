@@ -9,6 +9,14 @@ trigger. One step = one whole relaxation from the seeds (first list build +
 500 iterations), inputs resident in HBM.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+  python bench.py --workload batch64   (the batched form against sequential runs)
+
+--workload batch64: 64 independent volumes of seeded sizes 32^3..160^3 with
+2..18 nested-shell labels (~4M nodes in all), 200 FIRE iterations each. One
+step relaxes all of them in one session whose iteration loop is a CUDA graph
+(the tiles picked by the autotuner); the line adds the time of the same 64
+relaxations run one after another, each in its own session with plain
+launches, and the ratio of the two.
 
 N > 1 runs under torchrun, one process per GPU: a single volume does not
 shard, so each rank relaxes its own replica (weak scaling, no collective on the
@@ -218,6 +226,55 @@ def pinned_copy(a: np.ndarray) -> np.ndarray:
     return out
 
 
+def run_batch(args):
+    """The batched form (64 volumes, one graph-captured session) against the same
+    relaxations run one volume at a time with plain launches; device time by CUDA
+    events on each session's stream. One GPU."""
+    import torch
+    from trussnet_b200 import Session, synth
+    world, rank, local = dist_setup(args)
+    if world > 1 and rank != 0:
+        return
+    vols = synth.batch()
+    prm = synth.params_for("batch64")
+    if args.iters:
+        prm.max_iters = args.iters
+    iters = prm.max_iters
+    grids = [g for g, _ in vols]
+    nodes = [nd for _, nd in vols]
+    prms = [prm] * len(vols)
+    n = sum(nd.size() for nd in nodes)
+    sess = Session(grids, prms, nodes, device=local)
+    tune = sess.autotune()
+    sess.timed_runs(args.warmup, graph=True)
+    sess.clear_counters()
+    torch.cuda.synchronize(local)
+    clk = ClockSampler(local)
+    clk.start()
+    ms = sess.timed_runs(args.steps, graph=True)
+    clocks = clk.stop()
+    cnt = sess.counters()
+    sess.close()
+    step_ms = ms / args.steps
+    # the same relaxations, one volume at a time, plain launches (each session warmed once)
+    seq_ms = 0.0
+    for g, nd in vols:
+        with Session(g, prm, nd, device=local) as s1:
+            s1.timed_runs(1, graph=False)
+            seq_ms += s1.timed_runs(1, graph=False)
+    torch.cuda.synchronize(local)
+    line = {"metric": "batched relax node-iters/s, 64 volumes", "value": n * iters / (step_ms / 1e3), "unit": UNIT,
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batch64: 64 volumes 32^3..160^3, 2..18 nested-shell labels, h in [1.55, 6.2] "
+                                   "vox, 200 FIRE iterations, dptol 0", "volumes": len(vols), "nodes": n,
+                       "min_nodes": min(nd.size() for nd in nodes), "max_nodes": max(nd.size() for nd in nodes),
+                       "iters_per_step": iters, "autotune": tune.strip().splitlines()[-1] if tune else None},
+            "sequential_plain_ms": seq_ms, "batched_speedup": seq_ms / step_ms,
+            "clocks": clocks, "gpu_launches": int(cnt["launches"])}
+    print(json.dumps(line), flush=True)
+
+
 def run_cuda(args):
     import torch
     world, rank, local = dist_setup(args)
@@ -334,6 +391,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch64":
+        run_batch(args)
     else:
         run_cuda(args)
 

@@ -289,8 +289,16 @@ void init_ctl(v2m_session* s) {
     ck(cudaStreamSynchronize(s->stream), "synchronize");
 }
 
+void upload_vols(v2m_session* s) {
+    ck(cudaMemcpyAsync(s->d.vols, s->hvols.data(), sizeof(DVol) * s->nvol, cudaMemcpyHostToDevice, s->stream), "vols");
+}
+
 void do_reset(v2m_session* s) {
     const Dev& d = s->d;
+    for (DVol& V : s->hvols) {
+        V.hn_exact = 1;   // the seeds' sizes are packed from their positions
+    }
+    upload_vols(s);
     ck(cudaMemcpyAsync(d.Pq, s->Pq0, sizeof(float4) * d.N, cudaMemcpyDeviceToDevice, s->stream), "reset P");
     ck(cudaMemcpyAsync(d.typ, s->typ0, d.N, cudaMemcpyDeviceToDevice, s->stream), "reset typ");
     ck(cudaMemcpyAsync(d.part, s->part0, sizeof(uint32_t) * d.N, cudaMemcpyDeviceToDevice, s->stream), "reset part");
@@ -328,7 +336,7 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
         ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
         s->serial_power = env_int("V2M_CUDA_SERIAL_POWER", 0);
         s->force_threads = env_int("V2M_CUDA_FORCE_THREADS", 256);
-        if (s->force_threads != 64 && s->force_threads != 128 && s->force_threads != 256 && s->force_threads != 512) {
+        if (s->force_threads != 64 && s->force_threads != 128 && s->force_threads != 256) {
             s->force_threads = 256;
         }
         s->graph_iters = std::max(1, env_int("V2M_CUDA_GRAPH_ITERS", 10));
@@ -463,6 +471,7 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
             V.rebuild_div = p->rebuild_div > 0 ? p->rebuild_div : (env_div > 0 ? env_div : 1);
             V.hmode = p->h_mode;
             V.policy = p->rebuild_policy;
+            V.hn_exact = 1;
             V.fire_dt0 = std::sqrt(p->dt);
             V.fire_dtmax = p->fire_dtmax * V.fire_dt0;
             std::fill(nodevol.begin() + I.nofs, nodevol.begin() + I.nofs + I.n, (uint16_t)v);
@@ -1028,6 +1037,10 @@ int v2m_session_write_array(v2m_session* s, int vol, int what, const void* host,
             ck(cudaMemcpyAsync(tmp, host, (size_t)b, cudaMemcpyHostToDevice, s->stream), "write");
             return tmp;
         };
+        if (what == V2M_ARR_P || what == V2M_ARR_HN) {
+            s->hvols[vol].hn_exact = 0;   // the move reads h from the size field from now on
+            upload_vols(s);
+        }
         switch (what) {
         case V2M_ARR_P: {
             exact(12LL * n);
@@ -1148,7 +1161,8 @@ bool tune_lookup(v2m_session* s) {
     bool hit = false;
     const std::string want = tune_key(s);
     while (std::fscanf(f, "%511s %d %d", key, &ft, &nt) == 3) {
-        if (want == key) {
+        // (entries with shapes outside the kernels' launch bounds are ignored)
+        if (want == key && (ft == 64 || ft == 128 || ft == 256) && (nt == 64 || nt == 128 || nt == 256)) {
             s->force_threads = ft;
             s->nbr_threads = nt;
             hit = true;
@@ -1197,7 +1211,7 @@ std::string do_autotune(v2m_session* s, int reps) {
     std::string rep;
     float best = 1e30f;
     int bf = s->force_threads;
-    for (int t : { 64, 128, 256, 512 }) {
+    for (int t : { 64, 128, 256 }) {   // k_force's launch bound is 256
         const float ms = time_launches(s, reps, [&] { launch_force(s->stream, s->d, t); });
         rep += "force " + std::to_string(t) + " " + std::to_string(ms) + " ms\n";
         if (ms < best) {

@@ -348,6 +348,25 @@ __device__ __forceinline__ int warp_prune(NbrWarpSmem& sm, int m, int lane) {
     return m < V2M_K ? m : V2M_K;
 }
 
+// Distance from p to the bin interval [o + c b, o + (c + 1) b) along one axis;
+// the edge bins reach to infinity (bin_coord clamps nodes outside the hash
+// grid into them).
+__device__ __forceinline__ float axis_gap(float p, int c, float o, float b, int n) {
+    if (c > 0) {
+        const float lo = o + (float)c * b;
+        if (p < lo) {
+            return lo - p;
+        }
+    }
+    if (c < n - 1) {
+        const float hi = o + (float)(c + 1) * b;
+        if (p > hi) {
+            return p - hi;
+        }
+    }
+    return 0.0f;
+}
+
 __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& sm, const float4* __restrict__ Pq,
                                const uint8_t* __restrict__ typ, const uint16_t* __restrict__ lab,
                                const int* __restrict__ cstart, const int* __restrict__ sorted,
@@ -365,6 +384,11 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
     // The bins of a level inside the search box form rows along x with
     // consecutive keys, so a row's candidates are one contiguous range of the
     // sorted ids: the lanes take rows (of all three levels), not bins.
+    // Below the top level every node has ts h_j <= the level's bin side b, so a
+    // candidate is accepted only within r = (Ri + b) / 2 of node i (the box's
+    // half-width): rows and the ends of rows wholly farther than r (with a
+    // margin of 1e-3 b for rounding) hold only rejected candidates and are
+    // skipped. The top level also holds larger nodes: it is scanned whole.
     int lx0[3], lx1[3], ly0[3], lz0[3], lny[3], lrow[4], lkey[3];
     lrow[0] = 0;
 #pragma unroll
@@ -389,6 +413,10 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
     }
     const int nrows = lrow[3];
     int m = 0;
+    // once the buffer holds K entries, the K-th smallest so far (after a prune,
+    // entry K-1): a candidate above it can never make the list
+    float bd = __int_as_float(0x7f800000);
+    int bid = 0x7FFFFFFF;
     for (int rb = 0; rb < nrows; rb += 32) {
         const int r = rb + lane;
         int s0 = 0, c = 0;
@@ -398,9 +426,29 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
             const int rr = r - lrow[q];
             const int zz = rr / lny[q];
             const int cy = ly0[q] + (rr - zz * lny[q]), cz = lz0[q] + zz;
-            const int key0 = lkey[q] + H.dim[L][0] * (cy + H.dim[L][1] * cz);
-            s0 = cs[key0];
-            c = cs[key0 + (lx1[q] - lx0[q]) + 1] - s0;
+            int xa = lx0[q], xb = lx1[q];
+            bool skip = false;
+            if (L < H.nlev - 1) {
+                const float bL = H.b0 * (float)(1 << L);
+                const float m = 1e-3f * bL;
+                const float rad = 0.5f * (Ri + bL) + m;
+                const float dy = axis_gap(py, cy, H.oy, bL, H.dim[L][1]);
+                const float dz = axis_gap(pz, cz, H.oz, bL, H.dim[L][2]);
+                const float rem = rad * rad - dy * dy - dz * dz;
+                if (rem < 0.0f) {
+                    skip = true;
+                } else {
+                    const float w = sqrtf(rem) + m;
+                    xa = max(xa, bin_coord(H, L, px - w, H.ox, 0));
+                    xb = min(xb, bin_coord(H, L, px + w, H.ox, 0));
+                    skip = xa > xb;
+                }
+            }
+            if (!skip) {
+                const int key0 = lkey[q] + (xa - lx0[q]) + H.dim[L][0] * (cy + H.dim[L][1] * cz);
+                s0 = cs[key0];
+                c = cs[key0 + (xb - xa) + 1] - s0;
+            }
         }
         int incl = c;
         for (int o = 1; o < 32; o <<= 1) {
@@ -430,20 +478,24 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
             float dist = 0.0f;
             int j = -1;
             if (q < total) {
+                // the id is read only for a candidate within range (node i itself,
+                // at distance 0, is dropped there)
                 const int sidx = bs0 + (q - bexc);
-                j = sorted[sidx];
-                if (j != (int)i) {
-                    const float4 ps = Ps[sidx];
-                    const float ex = ps.x - px, ey = ps.y - py, ez = ps.z - pz;
-                    const float d2 = ex * ex + ey * ey + ez * ez;
-                    const float rj = ts * 0.5f * (hi + ps.w);
-                    ok = !(d2 >= rj * rj);
-                    if (ok && ti_int && typ[j] == V2M_INTERIOR && lab[j] != li) {
-                        ok = false;
-                    }
-                    if (ok) {
-                        dist = sqrtf(d2);
-                    }
+                const float4 ps = Ps[sidx];
+                const float ex = ps.x - px, ey = ps.y - py, ez = ps.z - pz;
+                const float d2 = ex * ex + ey * ey + ez * ez;
+                const float rj = ts * 0.5f * (hi + ps.w);
+                ok = !(d2 >= rj * rj);
+                if (ok) {
+                    j = sorted[sidx];
+                    ok = j != (int)i;
+                }
+                if (ok && ti_int && typ[j] == V2M_INTERIOR && lab[j] != li) {
+                    ok = false;
+                }
+                if (ok) {
+                    dist = sqrtf(d2);
+                    ok = !(dist > bd || (dist == bd && j > bid));   // (a NaN distance is kept, as before)
                 }
             }
             const unsigned mask = __ballot_sync(0xffffffffu, ok);
@@ -456,6 +508,10 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
             __syncwarp();
             if (m > kCap - 32) {
                 m = warp_prune(sm, m, lane);
+                if (m == V2M_K) {
+                    bd = sm.d[V2M_K - 1];
+                    bid = sm.id[V2M_K - 1];
+                }
             }
         }
     }
@@ -728,7 +784,9 @@ __global__ void __launch_bounds__(kMoveThreads) k_move_pre(const DVol* __restric
             const float fdt = c.fdt, falpha = c.falpha;
             const float4 pq = Pq[i];
             const int ty0 = typ[i];
-            const float h = size_at(Vd.g, Vd.hmode, pq.x, pq.y, pq.z);
+            // h at the node's position (v2m_move's v2m_h_at), which the stored size is unless a caller
+            // overwrote positions or sizes
+            const float h = Vd.hn_exact ? fabsf(pq.w) : size_at(Vd.g, Vd.hmode, pq.x, pq.y, pq.z);
             bool finished = true;
             if (ty0 != V2M_CORNER) {
                 const float4 f4 = F[i];
@@ -833,7 +891,7 @@ __global__ void __launch_bounds__(kMoveThreads) k_move_pre(const DVol* __restric
 // kMainThreads with no block-wide barrier: a warp's statistics are combined
 // with warp votes and flushed by one lane per (volume, bin), so a finished warp
 // never waits for a slower one.
-__global__ void __launch_bounds__(kMainThreads) k_move_main(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl,
+__global__ void __launch_bounds__(kMainThreads, 8) k_move_main(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl,
                                                            const uint16_t* __restrict__ nodevol, float4* __restrict__ Pq,
                                                            float4* __restrict__ Vel, uint8_t* __restrict__ typ,
                                                            const uint16_t* __restrict__ lab, uint32_t* __restrict__ part,

@@ -69,6 +69,10 @@ struct DVol {
     float t, skin, fscale, fsurf, dt, maxstep, snap, dptol;
     int voxmode, fire, max_iters, rebuild_div, hmode, policy;
     float fire_dt0, fire_dtmax;
+    // 1: every node's stored size (|Pq.w|) is the size field at its position --
+    // true from the seeds on (the pack and every move set it so); 0 after a
+    // caller wrote positions or sizes directly, until the next reset
+    int hn_exact;
 };
 
 // Mutable per-volume loop state (relax_cpu's locals, src/v2m_particles.cpp:822-946).
