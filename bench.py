@@ -263,6 +263,23 @@ def run_batch(args):
             s1.timed_runs(1, graph=False)
             seq_ms += s1.timed_runs(1, graph=False)
     torch.cuda.synchronize(local)
+    # end to end through the C ABI: one batch call against one relax_cl call per
+    # volume (host buffers, every upload, set-up and read-back inside), same results
+    from trussnet_b200 import relax_cl, relax_cl_batch
+    e2e = {}
+    for k in range(2):   # the first pass warms the module and the allocator
+        outs_b = [nd.copy() for nd in nodes]
+        t0 = time.perf_counter()
+        relax_cl_batch(grids, prms, outs_b, device=local)
+        tb = time.perf_counter() - t0
+        outs_s = [nd.copy() for nd in nodes]
+        t0 = time.perf_counter()
+        for g, o in zip(grids, outs_s):
+            relax_cl(g, prm, o, device=local)
+        ts_ = time.perf_counter() - t0
+        e2e = {"batch_call_s": tb, "sequential_calls_s": ts_, "speedup": ts_ / tb}
+    e2e["identical"] = all(np.array_equal(a.P.view(np.uint32), b.P.view(np.uint32)) and
+                           np.array_equal(a.typ, b.typ) for a, b in zip(outs_b, outs_s))
     line = {"metric": "batched relax node-iters/s, 64 volumes", "value": n * iters / (step_ms / 1e3), "unit": UNIT,
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -271,6 +288,11 @@ def run_batch(args):
                        "min_nodes": min(nd.size() for nd in nodes), "max_nodes": max(nd.size() for nd in nodes),
                        "iters_per_step": iters, "autotune": tune.strip().splitlines()[-1] if tune else None},
             "sequential_plain_ms": seq_ms, "batched_speedup": seq_ms / step_ms,
+            "e2e": {"value": n * iters / e2e["batch_call_s"], "unit": UNIT,
+                    "h2d_bytes_per_step": int(sum(g.nbytes() for g in grids) + sum(nd.nbytes() for nd in nodes)),
+                    "d2h_bytes_per_step": int(sum(nd.P.nbytes + nd.typ.nbytes + nd.part.nbytes for nd in nodes)),
+                    "batch_call_s": e2e["batch_call_s"], "sequential_relax_cl_calls_s": e2e["sequential_calls_s"],
+                    "speedup": e2e["speedup"], "results_identical": e2e["identical"]},
             "clocks": clocks, "gpu_launches": int(cnt["launches"])}
     print(json.dumps(line), flush=True)
 

@@ -123,15 +123,15 @@ __device__ __forceinline__ void cell_at(const DGrid& g, float px, float py, floa
     c.first = -1;
     if (c.i0 >= 0 && c.j0 >= 0 && c.k0 >= 0 && c.i0 < g.nx && c.j0 < g.ny && c.k0 < g.nz) {
         const int b = brick_index(g, c.i0, c.j0, c.k0);
-        const int n = __ldg(g.xcnt + b);
+        const uint4* p = g.xbrick + (size_t)3 * b;
+        const uint4 a = __ldg(p), e = __ldg(p + 1), f = __ldg(p + 2);
+        const int n = (int)a.x;
         if (n >= 0) {
             c.fast = 1;
             c.n = n;
-            const uint4* p = reinterpret_cast<const uint4*>(g.xlab + (size_t)b * V2M_BL);
-            const uint4 a = __ldg(p), e = __ldg(p + 1);
-            c.ll.w[0] = a.x; c.ll.w[1] = a.y; c.ll.w[2] = a.z; c.ll.w[3] = a.w;
-            c.ll.w[4] = e.x; c.ll.w[5] = e.y; c.ll.w[6] = e.z; c.ll.w[7] = e.w;
-            c.first = __ldg(g.xfirst + b);
+            c.first = (int)a.y;
+            c.ll.w[0] = a.z; c.ll.w[1] = a.w; c.ll.w[2] = e.x; c.ll.w[3] = e.y;
+            c.ll.w[4] = e.z; c.ll.w[5] = e.w; c.ll.w[6] = f.x; c.ll.w[7] = f.y;
         }
     }
 }

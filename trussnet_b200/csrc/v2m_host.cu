@@ -238,20 +238,18 @@ T* upload(v2m_session* s, const T* host, size_t count) {
     return d;
 }
 
-// The corner tables of one volume's grid (DGrid::xcnt .. xphi), built on the
+// The corner tables of one volume's grid (DGrid::xbrick, xphi), built on the
 // device from the uploaded grid; the table list is laid out on the host.
 void build_corner_tables(v2m_session* s, DGrid& g, size_t nb) {
-    int* xcnt = s->alloc<int>(nb);
-    uint16_t* xlab = s->alloc<uint16_t>(nb * V2M_BL);
-    int* xfirst = s->alloc<int>(nb);
+    uint4* xbrick = s->alloc<uint4>(3 * nb);
     int* xn = nullptr;
     ck(cudaMallocAsync((void**)&xn, 4 * std::max<size_t>(nb, 1), s->stream), "cudaMallocAsync");
-    launch_xcount(s->stream, g, xcnt, xlab, xn, (int)nb);
+    launch_xcount(s->stream, g, xbrick, xn, (int)nb);
     ck(cudaGetLastError(), "corner tables");
-    std::vector<int> hn(nb), first(nb, -1);
-    std::vector<uint16_t> hl(nb * V2M_BL);
+    std::vector<int> hn(nb);
+    std::vector<uint4> rec(3 * nb);
     ck(cudaMemcpyAsync(hn.data(), xn, 4 * nb, cudaMemcpyDeviceToHost, s->stream), "corner tables");
-    ck(cudaMemcpyAsync(hl.data(), xlab, 2 * nb * V2M_BL, cudaMemcpyDeviceToHost, s->stream), "corner tables");
+    ck(cudaMemcpyAsync(rec.data(), xbrick, sizeof(uint4) * 3 * nb, cudaMemcpyDeviceToHost, s->stream), "corner tables");
     ck(cudaFreeAsync(xn, s->stream), "cudaFreeAsync");
     ck(cudaStreamSynchronize(s->stream), "synchronize");
     std::vector<int2> tabs;
@@ -260,21 +258,21 @@ void build_corner_tables(v2m_session* s, DGrid& g, size_t nb) {
             if (tabs.size() + hn[b] > (size_t)0x7FFFFFFF) {
                 throw ArgError("too many corner tables");
             }
-            first[b] = (int)tabs.size();
+            rec[3 * b].y = (uint32_t)tabs.size();   // the first table
+            const uint32_t w[8] = { rec[3 * b].z, rec[3 * b].w, rec[3 * b + 1].x, rec[3 * b + 1].y,
+                                    rec[3 * b + 1].z, rec[3 * b + 1].w, rec[3 * b + 2].x, rec[3 * b + 2].y };
             for (int q = 0; q < hn[b]; ++q) {
-                tabs.push_back(make_int2((int)b, (int)hl[b * V2M_BL + q]));
+                tabs.push_back(make_int2((int)b, (int)((w[q >> 1] >> (16 * (q & 1))) & 0xFFFFu)));
             }
         }
     }
     const int2* dtabs = upload(s, tabs.data(), tabs.size());
-    ck(cudaMemcpyAsync(xfirst, first.data(), 4 * nb, cudaMemcpyHostToDevice, s->stream), "corner tables");
+    ck(cudaMemcpyAsync(xbrick, rec.data(), sizeof(uint4) * 3 * nb, cudaMemcpyHostToDevice, s->stream), "corner tables");
     float* xphi = s->alloc<float>(tabs.size() * 729);
     launch_xfill(s->stream, g, dtabs, xphi, (int)tabs.size());
     ck(cudaGetLastError(), "corner tables");
-    ck(cudaStreamSynchronize(s->stream), "synchronize");   // (tabs and first are host vectors)
-    g.xcnt = xcnt;
-    g.xlab = xlab;
-    g.xfirst = xfirst;
+    ck(cudaStreamSynchronize(s->stream), "synchronize");   // (tabs and rec are host vectors)
+    g.xbrick = xbrick;
     g.xphi = xphi;
 }
 

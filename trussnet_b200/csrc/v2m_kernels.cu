@@ -985,9 +985,11 @@ __global__ void __launch_bounds__(kMainThreads, 8) k_move_main(const DVol* __res
 // brick's own and its + neighbours' listed labels, and label 0 when the
 // 9x9x9 region passes the grid's edge (phi_voxel is 1 for label 0 there) --
 // and whether the region is one label everywhere (no table needed). More than
-// 16 labels: no table (xcnt = -1; such cells take the per-corner path).
+// 16 labels: no table (count -1; such cells take the per-corner path). The
+// brick's record (DGrid::xbrick) gets the count and the labels; the host fills
+// in the first table.
 // xn gets the number of tables the brick needs.
-__global__ void k_xcount(DGrid g, int* __restrict__ xcnt, uint16_t* __restrict__ xlab, int* __restrict__ xn, int nb) {
+__global__ void k_xcount(DGrid g, uint4* __restrict__ xbrick, int* __restrict__ xn, int nb) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb) {
         return;
@@ -1052,20 +1054,28 @@ __global__ void k_xcount(DGrid g, int* __restrict__ xcnt, uint16_t* __restrict__
     } else {
         uni = false;
     }
-    for (int q = 0; q < V2M_BL; ++q) {
-        xlab[(size_t)b * V2M_BL + q] = q < n ? lst[q] : (uint16_t)0;
-    }
+    int cnt;
     if (over) {
-        xcnt[b] = -1;
+        cnt = -1;
         xn[b] = 0;
     } else if (uni) {
-        xlab[(size_t)b * V2M_BL] = (uint16_t)ulab;
-        xcnt[b] = 1;
+        lst[0] = (uint16_t)ulab;
+        n = 1;
+        cnt = 1;
         xn[b] = 0;
     } else {
-        xcnt[b] = n;
+        cnt = n;
         xn[b] = n;
     }
+    uint32_t w[8];
+    for (int q = 0; q < 8; ++q) {
+        const uint32_t lo = 2 * q < n ? lst[2 * q] : 0u, hi = 2 * q + 1 < n ? lst[2 * q + 1] : 0u;
+        w[q] = lo | (hi << 16);
+    }
+    uint4* r = xbrick + (size_t)3 * b;
+    r[0] = make_uint4((uint32_t)cnt, 0xFFFFFFFFu, w[0], w[1]);
+    r[1] = make_uint4(w[2], w[3], w[4], w[5]);
+    r[2] = make_uint4(w[6], w[7], 0u, 0u);
 }
 
 // One block per table (brick, label): its 729 voxel values by phi_voxel.
@@ -1374,8 +1384,8 @@ void launch_move(cudaStream_t s, const Dev& d) {
                                                                  d.part, d.mv, d.P0, d.S, d.queue, d.rlist, d.G, d.N);
 }
 
-void launch_xcount(cudaStream_t s, const DGrid& g, int* xcnt, uint16_t* xlab, int* xn, int nb) {
-    k_xcount<<<nblk(nb, 128), 128, 0, s>>>(g, xcnt, xlab, xn, nb);
+void launch_xcount(cudaStream_t s, const DGrid& g, uint4* xbrick, int* xn, int nb) {
+    k_xcount<<<nblk(nb, 128), 128, 0, s>>>(g, xbrick, xn, nb);
 }
 
 void launch_xfill(cudaStream_t s, const DGrid& g, const int2* tabs, float* xphi, int ntab) {

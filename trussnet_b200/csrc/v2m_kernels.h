@@ -62,7 +62,7 @@ void launch_neighbors(cudaStream_t s, const Dev& d, int threads);
 void launch_force(cudaStream_t s, const Dev& d, int threads);
 void launch_move(cudaStream_t s, const Dev& d);
 void launch_control(cudaStream_t s, const Dev& d, int serial);
-void launch_xcount(cudaStream_t s, const DGrid& g, int* xcnt, uint16_t* xlab, int* xn, int nb);
+void launch_xcount(cudaStream_t s, const DGrid& g, uint4* xbrick, int* xn, int nb);
 void launch_xfill(cudaStream_t s, const DGrid& g, const int2* tabs, float* xphi, int ntab);
 void launch_refresh(cudaStream_t s, const Dev& d, int blocks);
 void launch_set_rebuild(cudaStream_t s, const Dev& d, int val);

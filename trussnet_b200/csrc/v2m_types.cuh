@@ -40,9 +40,11 @@ struct DGrid {
     // grid's edge, label 0) and, per label, the 9x9x9 voxel values of the brick
     // plus a one-voxel halo on the + sides, each the reference's per-voxel phi.
     // Any cell based inside the grid then reads its 8 corners from one table.
-    const int* xcnt;        // labels listed; -1: no table (the per-corner path)
-    const uint16_t* xlab;   // 16 per brick
-    const int* xfirst;      // first table of the brick; -1: uniform (label xlab[0] is 1 at every corner)
+    // A brick's record is 48 bytes, read as three 16-byte loads issued together:
+    // int count (labels listed; -1: no table, the per-corner path), int first
+    // table (-1: uniform, the first label is 1 at every corner), 16 u16 labels,
+    // 8 bytes of padding.
+    const uint4* xbrick;    // 3 per brick
     const float* xphi;      // 729 floats per table, x fastest
 };
 
