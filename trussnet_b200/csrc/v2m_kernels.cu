@@ -590,12 +590,12 @@ __global__ void __launch_bounds__(kNbrMaxThreads) k_refresh(const DVol* __restri
 }
 
 // ---- bar forces ----------------------------------------------------------------
-constexpr int kForceBatch = 8;
+constexpr int kForceBatch = 4;
 
 // One thread per node; the lists are slot-major (nbr[k*N + i]) so a warp's k-th
 // entries are one coalesced 128-byte row; neighbour position + signed size is
 // one 16-byte gather. Bars are added in list order, as v2m_force does.
-__global__ void __launch_bounds__(256) k_force(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
+__global__ void __launch_bounds__(256, 4) k_force(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
                                                const uint16_t* __restrict__ nodevol, const float4* __restrict__ Pq,
                                                const int* __restrict__ nbr, const uint8_t* __restrict__ nnb,
                                                float4* __restrict__ F, int64_t N) {
