@@ -10,6 +10,7 @@ trigger. One step = one whole relaxation from the seeds (first list build +
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
   python bench.py --workload batch64   (the batched form against sequential runs)
+  python bench.py --workload adjoint   (the unroll's backward against its forward)
 
 --workload batch64: 64 independent volumes of seeded sizes 32^3..160^3 with
 2..18 nested-shell labels (~4M nodes in all), 200 FIRE iterations each. One
@@ -297,6 +298,51 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+def adjoint_leg(local, steps=3, warmup=3):
+    """The differentiable unroll: K = 50 Jacobi steps on a 128^3 4-label nested
+    ellipsoid volume (~150k nodes) with a 64^3 sizing grid, checkpoint every 10
+    steps; device time (CUDA events) of the forward pass and of the backward pass
+    (gradients w.r.t. the nodes and the grid, the loss's gradient included)."""
+    import torch
+    from trussnet_b200 import Session, synth
+    from trussnet_b200.adjoint import Unroll
+    from trussnet_b200.types import RelaxParams
+    g, nd, G, cs = synth.ellipsoids_adjoint()
+    with Session(g, RelaxParams(max_iters=1), nd, device=local) as s:
+        s.rebuild()
+        nbr, nnb = s.read("nbr"), s.read("nnb")
+    K, ckpt = 50, 10
+    u = Unroll(nbr, nnb, nd.typ, G.shape[::-1], cs, 1.2, 1.0, 0.2, K, ckpt, device=local)
+    x0 = torch.tensor(nd.P, device=f"cuda:{local}")
+    Gt = torch.tensor(G, device=f"cuda:{local}")
+    f = b = 0.0
+    for k in range(warmup + steps):
+        xK = u.forward(x0, Gt)
+        gxK, _ = u.loss_backward(xK, Gt)
+        u.backward(Gt, gxK)
+        if k >= warmup:
+            tf, tb = u.timing()
+            f += tf
+            b += tb
+    u.close()
+    return {"workload": "ellipsoids_adjoint: 128^3, 4 nested labels, 64^3 sizing grid in [1.5,4], K=50, "
+                        "checkpoint every 10", "nodes": nd.size(), "K": K, "ckpt": ckpt,
+            "forward_us_per_step": f / steps / K * 1e3, "backward_us_per_step": b / steps / K * 1e3,
+            "backward_over_forward": b / f}
+
+
+def run_adjoint(args):
+    world, rank, local = dist_setup(args)
+    if rank != 0:
+        return
+    a = adjoint_leg(local, args.steps, args.warmup)
+    line = {"metric": "adjoint/fwd ratio", "value": a["backward_over_forward"], "unit": "x", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": a["backward_us_per_step"] * a["K"] / 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": a}
+    print(json.dumps(line), flush=True)
+
+
 def run_cuda(args):
     import torch
     world, rank, local = dist_setup(args)
@@ -359,6 +405,7 @@ def run_cuda(args):
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(g, nd, prm, args.ref_iters)
+    adj = adjoint_leg(local) if rank == 0 and world == 1 and args.e2e_steps > 0 else None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
@@ -369,7 +416,7 @@ def run_cuda(args):
                            "rebuilds_per_step": st.rebuilds, "final_types": [st.n_interior, st.n_interface,
                                                                              st.n_junction, st.n_corner]},
                 "clocks": clocks, "e2e": e2e, "gpu_launches": int(cnt["launches"]), "roofline": roofline,
-                "stage_ms_first100": stages, "cpu_baseline": cb}
+                "stage_ms_first100": stages, "cpu_baseline": cb, "adjoint": adj}
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -415,6 +462,8 @@ def main():
         run_reference(args)
     elif args.workload == "batch64":
         run_batch(args)
+    elif args.workload == "adjoint":
+        run_adjoint(args)
     else:
         run_cuda(args)
 
