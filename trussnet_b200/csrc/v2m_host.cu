@@ -392,7 +392,7 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
         d.nnb = s->alloc<uint8_t>(N);
         d.rlist = s->alloc<int>(N);
         d.S = s->alloc<float4>(N);
-        d.queue = s->alloc<int>(N);
+        d.queue = s->alloc<int>(2 * N);
         d.cnt = s->alloc<int>(KT);
         d.cstart = s->alloc<int>(KT);
         d.cursor = s->alloc<int>(KT);

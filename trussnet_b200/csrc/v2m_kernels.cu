@@ -579,10 +579,11 @@ __global__ void __launch_bounds__(kNbrMaxThreads) k_refresh(const DVol* __restri
         const int d = atomicAdd(&G->blocks_done, 1);
         if (d == (int)gridDim.x - 1) {
             G->nrefresh = 0;
-            G->qtrap_last = G->qtrap;
+            G->qtrap_last = G->qtrap + G->qjun;
             G->qint_last = G->qint;
             G->qtrap = 0;
             G->qint = 0;
+            G->qjun = 0;
             G->blocks_done = 0;
             __threadfence();
         }
@@ -832,7 +833,7 @@ __global__ void __launch_bounds__(kMoveThreads) k_move_pre(const DVol* __restric
                     }
                     S[i] = make_float4(s[0], s[1], s[2], h);
                     finished = false;
-                    qkind = ty0 == V2M_INTERIOR ? 1 : 0;
+                    qkind = ty0 == V2M_INTERIOR ? 1 : (ty0 == V2M_JUNCTION ? 2 : 0);
                 }
             }
             if (fire) {
@@ -847,20 +848,22 @@ __global__ void __launch_bounds__(kMoveThreads) k_move_pre(const DVol* __restric
             }
         }
     }
-    // queue the moving nodes: one atomic per warp and kind
+    // queue the moving nodes, one atomic per warp and kind: INTERFACE (and other
+    // non-junction trapped) nodes from the front of queue[0, N), INTERIOR ones
+    // from its back, JUNCTION ones from the front of queue[N, 2N)
     const unsigned lane = threadIdx.x & 31u;
 #pragma unroll
-    for (int kind = 0; kind < 2; ++kind) {
+    for (int kind = 0; kind < 3; ++kind) {
         const unsigned m = __ballot_sync(0xffffffffu, qkind == kind);
         if (m) {
             int base = 0;
             if (lane == (unsigned)(__ffs(m) - 1)) {
-                base = atomicAdd(kind == 0 ? &G->qtrap : &G->qint, __popc(m));
+                base = atomicAdd(kind == 0 ? &G->qtrap : (kind == 1 ? &G->qint : &G->qjun), __popc(m));
             }
             base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
             if (qkind == kind) {
                 const int slot = base + __popc(m & ((1u << lane) - 1u));
-                queue[kind == 0 ? slot : (int)(N - 1 - slot)] = (int)i;
+                queue[kind == 0 ? (int64_t)slot : (kind == 1 ? N - 1 - slot : N + slot)] = (int)i;
             }
         }
     }
@@ -898,13 +901,16 @@ __global__ void __launch_bounds__(kMainThreads, 8) k_move_main(const DVol* __res
                                                            float* __restrict__ mvout, const float4* __restrict__ P0,
                                                            const float4* __restrict__ S, const int* __restrict__ queue,
                                                            int* __restrict__ rlist, Global* G, int64_t N) {
+    // blocks over queue[0, 2N): a warp holds nodes of one kind (the junction
+    // moves, ten times an interface move, get warps of their own)
     const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int qa = *((volatile int*)&G->qtrap), qb = *((volatile int*)&G->qint);
-    if (blockIdx.x * (int64_t)blockDim.x >= qa && (blockIdx.x + 1) * (int64_t)blockDim.x <= N - qb) {
-        return;   // the whole block lies between the two queues
+    const int qa = *((volatile int*)&G->qtrap), qb = *((volatile int*)&G->qint), qj = *((volatile int*)&G->qjun);
+    const int64_t b0 = blockIdx.x * (int64_t)blockDim.x, b1 = b0 + blockDim.x;
+    if ((b0 >= qa && b1 <= N - qb) || b0 >= N + qj) {
+        return;   // the whole block lies between the queues or past the junction queue
     }
     int64_t i = -1;
-    if (q < N && (q < qa || q >= N - qb)) {
+    if (q < N ? (q < qa || q >= N - qb) : q < N + qj) {
         i = queue[q];
     }
     const int v = i >= 0 ? nodevol[i] : -1;
@@ -1380,7 +1386,7 @@ void launch_move(cudaStream_t s, const Dev& d) {
     k_move_pre<<<nblk(d.N, kMoveThreads), kMoveThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.F, d.Vel, d.typ,
                                                                 d.mv, d.pw, d.P0, d.S, d.queue, d.psum, d.rlist, d.G,
                                                                 d.N);
-    k_move_main<<<nblk(d.N, kMainThreads), kMainThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.Vel, d.typ, d.lab,
+    k_move_main<<<nblk(2 * d.N, kMainThreads), kMainThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.Vel, d.typ, d.lab,
                                                                  d.part, d.mv, d.P0, d.S, d.queue, d.rlist, d.G, d.N);
 }
 

@@ -104,9 +104,10 @@ struct Global {
     int blocks_done;     // last-block-done counter of the refresh kernel
     int err;             // kernel error flag (first error code)
     int err_info;
-    int qtrap, qint;     // move queue lengths: trapped nodes (front), interior nodes (back)
-    int qtrap_last, qint_last;   // the last iteration's queue lengths
+    int qtrap, qint;     // move queue lengths: trapped non-junction nodes (front), interior nodes (back)
+    int qtrap_last, qint_last;   // the last iteration's queue lengths (trapped: junctions included)
     int rebuild_any;     // some volume rebuilds this iteration (the rebuild stages return at once otherwise)
+    int qjun;            // junction moves (queue[N, N + qjun))
 };
 
 constexpr int kMaxVol = 1024;
