@@ -266,7 +266,9 @@ def ellipsoids(dim=128, nlab=4, h=(1.5, 4.0), density=1.0, seed=0):
 
 def batch(nvol=64, seed=0, dmin=32, dmax=160, lmin=2, lmax=18, scale=1.55):
     """`nvol` independent volumes of seeded sizes dmin^3..dmax^3 with lmin..lmax
-    nested-shell labels; shells at least 2R+8 voxels apart where they fit."""
+    nested-shell labels: the outer shell at 0.45 dim, the others 4 voxels apart
+    inwards (radius at least 4), shell noise 0.02 dim; h graded from 1.0 to 4.0
+    times `scale` by the distance to the nearest interface."""
     rng = np.random.default_rng(seed)
     out = []
     for v in range(nvol):
