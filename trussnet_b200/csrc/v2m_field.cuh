@@ -275,18 +275,36 @@ __device__ __forceinline__ int owner_label(const DGrid& g, int voxmode, float px
     }
     Cell cl;
     cell_at(g, px, py, pz, cl);
+    // two labels per turn: both labels' corner loads are in flight together;
+    // the ranking still takes the labels one by one in list order
 #pragma unroll 1
-    for (int s = 0; s < n; ++s) {
-        const int ls = ll.get(s);
-        const float v = cell_phi(g, cl, ls);
-        if (v > pb) {
+    for (int s = 0; s < n; s += 2) {
+        const int l0 = ll.get(s);
+        const bool two = s + 1 < n;
+        const int l1 = two ? ll.get(s + 1) : l0;
+        float c0[8], c1[8];
+        cell_corners(g, cl, l0, c0);
+        cell_corners(g, cl, l1, c1);
+        const float v0 = trilerp8(c0, cl.fx, cl.fy, cl.fz), v1 = trilerp8(c1, cl.fx, cl.fy, cl.fz);
+        if (v0 > pb) {
             ps = pb;
             sec = best;
-            pb = v;
-            best = ls;
-        } else if (v > ps) {
-            ps = v;
-            sec = ls;
+            pb = v0;
+            best = l0;
+        } else if (v0 > ps) {
+            ps = v0;
+            sec = l0;
+        }
+        if (two) {
+            if (v1 > pb) {
+                ps = pb;
+                sec = best;
+                pb = v1;
+                best = l1;
+            } else if (v1 > ps) {
+                ps = v1;
+                sec = l1;
+            }
         }
     }
     *second = sec;
@@ -353,11 +371,14 @@ __device__ __forceinline__ float psi_grad(const DGrid& g, int a, int b, float px
 
 // Bracketed root of psi_ab along unit direction u from p, within rad: doubling
 // probes from the Newton guess tg, then Illinois regula falsi
-// (src/opencl/v2m_seed_body.cl:255-320). Moves p and returns 1 on success.
-__device__ __noinline__ int bisect_dir(const DGrid& g, int a, int b, float* p, const float* u, float v0, float rad,
-                                       float tg) {
+// (src/opencl/v2m_seed_body.cl:255-320). Returns (the moved p, 1) on success,
+// (p, 0) otherwise. (The out-of-line helpers take and return points by value,
+// so their callers' points stay in registers; the pointer forms below wrap them.)
+__device__ __noinline__ float4 bisect_dirv(const DGrid& g, int a, int b, float px, float py, float pz, float ux,
+                                           float uy, float uz, float v0, float rad, float tg) {
+    const float p[3] = { px, py, pz }, u[3] = { ux, uy, uz };
     if (v0 == 0.0f) {
-        return 1;
+        return make_float4(px, py, pz, 1.0f);
     }
     const float sg = v0 > 0.0f ? -1.0f : 1.0f;
     float t0 = 0.0f, t1 = -1.0f, f0 = v0, f1 = 0.0f;
@@ -377,7 +398,7 @@ __device__ __noinline__ int bisect_dir(const DGrid& g, int a, int b, float* p, c
         t = fminf(2.0f * t, rad);
     }
     if (t1 < 0.0f) {
-        return 0;
+        return make_float4(px, py, pz, 0.0f);
     }
     int side = 0;
     for (int it = 0; it < 8 && f1 != 0.0f && fabsf(t1 - t0) > 1e-4f * rad; ++it) {
@@ -398,67 +419,89 @@ __device__ __noinline__ int bisect_dir(const DGrid& g, int a, int b, float* p, c
             side = 1;
         }
     }
-    for (int k = 0; k < 3; ++k) {
-        p[k] += sg * t1 * u[k];
-    }
-    return 1;
+    return make_float4(p[0] + sg * t1 * u[0], p[1] + sg * t1 * u[1], p[2] + sg * t1 * u[2], 1.0f);
+}
+
+__device__ __forceinline__ int bisect_dir(const DGrid& g, int a, int b, float* p, const float* u, float v0, float rad,
+                                          float tg) {
+    const float4 r = bisect_dirv(g, a, b, p[0], p[1], p[2], u[0], u[1], u[2], v0, rad, tg);
+    p[0] = r.x;
+    p[1] = r.y;
+    p[2] = r.z;
+    return r.w != 0.0f;
 }
 
 // Projection onto psi_ab = 0 along the local normal within rad (src/opencl/v2m_seed_body.cl:324-335)
-__device__ __noinline__ int project1(const DGrid& g, int a, int b, float* p, float rad) {
+__device__ __noinline__ float4 project1v(const DGrid& g, int a, int b, float px, float py, float pz, float rad) {
     float gr[3];
-    const float v = psi_grad(g, a, b, p[0], p[1], p[2], gr);
+    const float v = psi_grad(g, a, b, px, py, pz, gr);
     const float gn = sqrtf(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
     if (gn < 1e-9f) {
-        return 0;
+        return make_float4(px, py, pz, 0.0f);
     }
-    const float u[3] = { gr[0] / gn, gr[1] / gn, gr[2] / gn };
-    return bisect_dir(g, a, b, p, u, v, rad, 1.5f * fabsf(v) / gn);
+    return bisect_dirv(g, a, b, px, py, pz, gr[0] / gn, gr[1] / gn, gr[2] / gn, v, rad, 1.5f * fabsf(v) / gn);
+}
+
+__device__ __forceinline__ int project1(const DGrid& g, int a, int b, float* p, float rad) {
+    const float4 r = project1v(g, a, b, p[0], p[1], p[2], rad);
+    p[0] = r.x;
+    p[1] = r.y;
+    p[2] = r.z;
+    return r.w != 0.0f;
 }
 
 // Projection onto the junction curve psi_ab = psi_ac = 0 by alternating
 // bracketed legs (src/opencl/v2m_seed_body.cl:342-420, sampled fields).
-__device__ __noinline__ int project2(const DGrid& g, int a, int b, int c, float* p, float rad) {
-    float q[3] = { p[0], p[1], p[2] };
+__device__ __noinline__ float4 project2v(const DGrid& g, int a, int b, int c, float px, float py, float pz,
+                                         float rad) {
+    const float p[3] = { px, py, pz };
+    float q[3] = { px, py, pz };
     for (int it = 0; it < 3; ++it) {
         float g1[3], g2[3];
         if (!project1(g, a, b, q, rad)) {
-            return 0;
+            return make_float4(px, py, pz, 0.0f);
         }
         psi_grad(g, a, b, q[0], q[1], q[2], g1);
         const float v2 = psi_grad(g, a, c, q[0], q[1], q[2], g2);
         const float a11 = g1[0] * g1[0] + g1[1] * g1[1] + g1[2] * g1[2];
         if (a11 < 1e-18f) {
-            return 0;
+            return make_float4(px, py, pz, 0.0f);
         }
         const float pr = (g1[0] * g2[0] + g1[1] * g2[1] + g1[2] * g2[2]) / a11;
         float u[3] = { g2[0] - pr * g1[0], g2[1] - pr * g1[1], g2[2] - pr * g1[2] };
         const float un = sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
         if (un < 1e-9f) {
-            return 0;
+            return make_float4(px, py, pz, 0.0f);
         }
         u[0] /= un;
         u[1] /= un;
         u[2] /= un;
         if (!bisect_dir(g, a, c, q, u, v2, rad, 1.5f * fabsf(v2) / un)) {
-            return 0;
+            return make_float4(px, py, pz, 0.0f);
         }
     }
     if (!project1(g, a, b, q, rad)) {
-        return 0;
+        return make_float4(px, py, pz, 0.0f);
     }
     const float m2 = (q[0] - p[0]) * (q[0] - p[0]) + (q[1] - p[1]) * (q[1] - p[1]) + (q[2] - p[2]) * (q[2] - p[2]);
     if (m2 > rad * rad) {
-        return 0;
+        return make_float4(px, py, pz, 0.0f);
     }
-    p[0] = q[0];
-    p[1] = q[1];
-    p[2] = q[2];
-    return 1;
+    return make_float4(q[0], q[1], q[2], 1.0f);
+}
+
+__device__ __forceinline__ int project2(const DGrid& g, int a, int b, int c, float* p, float rad) {
+    const float4 r = project2v(g, a, b, c, p[0], p[1], p[2], rad);
+    p[0] = r.x;
+    p[1] = r.y;
+    p[2] = r.z;
+    return r.w != 0.0f;
 }
 
 // Crossing of p -> q with psi_ab = 0: 6 bisections and a secant (src/opencl/v2m_particle_body.cl:188-212)
-__device__ __noinline__ void crossing(const DGrid& g, int a, int b, const float* p, const float* q, float* c) {
+__device__ __noinline__ float4 crossingv(const DGrid& g, int a, int b, float px, float py, float pz, float qx,
+                                         float qy, float qz) {
+    const float p[3] = { px, py, pz }, q[3] = { qx, qy, qz };
     float t0 = 0.0f, t1 = 1.0f;
     float v0 = psi(g, a, b, p[0], p[1], p[2]);
     float v1 = psi(g, a, b, q[0], q[1], q[2]);
@@ -474,9 +517,14 @@ __device__ __noinline__ void crossing(const DGrid& g, int a, int b, const float*
         }
     }
     const float t = (v0 - v1) != 0.0f ? t0 + (t1 - t0) * v0 / (v0 - v1) : 0.5f * (t0 + t1);
-    for (int k = 0; k < 3; ++k) {
-        c[k] = p[k] + t * (q[k] - p[k]);
-    }
+    return make_float4(p[0] + t * (q[0] - p[0]), p[1] + t * (q[1] - p[1]), p[2] + t * (q[2] - p[2]), 0.0f);
+}
+
+__device__ __forceinline__ void crossing(const DGrid& g, int a, int b, const float* p, const float* q, float* c) {
+    const float4 r = crossingv(g, a, b, p[0], p[1], p[2], q[0], q[1], q[2]);
+    c[0] = r.x;
+    c[1] = r.y;
+    c[2] = r.z;
 }
 
 // Drop v's component along psi_ab's normal at p (src/opencl/v2m_particle_body.cl:215-229)
@@ -494,7 +542,8 @@ __device__ __forceinline__ void tangential(const DGrid& g, int a, int b, const f
 }
 
 // A third label competing at q (phi_c > 0.5 phi_a), or NOLAB (src/opencl/v2m_particle_body.cl:232-260)
-__device__ __noinline__ int third_label(const DGrid& g, int a, int b, const float* q) {
+__device__ __noinline__ int third_labelv(const DGrid& g, int a, int b, float qx, float qy, float qz) {
+    const float q[3] = { qx, qy, qz };
     LabList ll;
     const int n = labels_near(g, q[0], q[1], q[2], ll);
     int other = 0;
@@ -527,8 +576,13 @@ __device__ __noinline__ int third_label(const DGrid& g, int a, int b, const floa
     return c;
 }
 
+__device__ __forceinline__ int third_label(const DGrid& g, int a, int b, const float* q) {
+    return third_labelv(g, a, b, q[0], q[1], q[2]);
+}
+
 // Do the node's labels dominate at q? (src/opencl/v2m_particle_body.cl:266-291)
-__device__ __noinline__ int valid_on(const DGrid& g, int a, int b, int c, const float* q) {
+__device__ __noinline__ int valid_onv(const DGrid& g, int a, int b, int c, float qx, float qy, float qz) {
+    const float q[3] = { qx, qy, qz };
     LabList ll;
     const int n = labels_near(g, q[0], q[1], q[2], ll);
     int other = 0;
@@ -556,6 +610,50 @@ __device__ __noinline__ int valid_on(const DGrid& g, int a, int b, int c, const 
         }
     }
     return 1;
+}
+
+__device__ __forceinline__ int valid_on(const DGrid& g, int a, int b, int c, const float* q) {
+    return valid_onv(g, a, b, c, q[0], q[1], q[2]);
+}
+
+// third_label(a, b, q) and valid_on(a, b, NOLAB, q) together: one label list,
+// one cell and one phi evaluation per label serve both (the same values as
+// the two calls). Returns (third label or NOLAB, valid).
+__device__ __noinline__ int2 third_and_valid(const DGrid& g, int a, int b, float qx, float qy, float qz) {
+    LabList ll;
+    const int n = labels_near(g, qx, qy, qz, ll);
+    int other = 0;
+#pragma unroll
+    for (int s = 0; s < V2M_BL; ++s) {
+        if (s < n) {
+            const int l = ll.get(s);
+            other |= l != a && l != b;
+        }
+    }
+    if (!other) {
+        return make_int2(V2M_NOLAB, 1);
+    }
+    Cell cl;
+    cell_at(g, qx, qy, qz, cl);
+    const float pa = cell_phi(g, cl, a);
+    const float mine = fminf(pa, cell_phi(g, cl, b));
+    int c = V2M_NOLAB, valid = 1;
+    float pc = 0.5f * pa;
+#pragma unroll 1
+    for (int s = 0; s < n; ++s) {
+        const int l = ll.get(s);
+        if (l != a && l != b) {
+            const float w = cell_phi(g, cl, l);
+            if (w > pc) {
+                pc = w;
+                c = l;
+            }
+            if (w > mine + 0.02f) {
+                valid = 0;
+            }
+        }
+    }
+    return make_int2(c, valid);
 }
 
 // ---- voxel trap mode (src/opencl/v2m_particle_body.cl:358-650) -------------------
@@ -903,8 +1001,12 @@ __device__ __noinline__ float move_step(const DGrid& g, int hmode, float h, floa
         }
     }
     // an interface node meeting a third label joins the junction curve
+    // (third_and_valid also gives valid_on's answer for q as an INTERFACE node)
+    int valid_here = -1;
     if (ty == V2M_INTERFACE) {
-        const int cc = third_label(g, a, b, q);
+        const int2 tv = third_and_valid(g, a, b, q[0], q[1], q[2]);
+        const int cc = tv.x;
+        valid_here = tv.y;
         if (cc != V2M_NOLAB) {
             float r[3] = { q[0], q[1], q[2] };
             if (project2(g, a, b, cc, r, 0.5f * h)) {
@@ -928,7 +1030,9 @@ __device__ __noinline__ float move_step(const DGrid& g, int hmode, float h, floa
         }
     }
     // refuse a move onto an invalid branch of the constraint
-    if (ty != V2M_INTERIOR && !valid_on(g, a, st.pb, ty >= V2M_JUNCTION ? st.pc : V2M_NOLAB, q)) {
+    if (ty != V2M_INTERIOR &&
+        !(ty == V2M_INTERFACE && valid_here >= 0 ? valid_here
+                                                  : valid_on(g, a, st.pb, ty >= V2M_JUNCTION ? st.pc : V2M_NOLAB, q))) {
         if (ty == V2M_INTERFACE || ty_in == V2M_INTERIOR) {
             const int cc = third_label(g, a, st.pb, q);
             float r[3] = { q[0], q[1], q[2] };

@@ -901,17 +901,23 @@ __global__ void __launch_bounds__(kMainThreads, 8) k_move_main(const DVol* __res
                                                            float* __restrict__ mvout, const float4* __restrict__ P0,
                                                            const float4* __restrict__ S, const int* __restrict__ queue,
                                                            int* __restrict__ rlist, Global* G, int64_t N) {
-    // blocks over queue[0, 2N): a warp holds nodes of one kind (the junction
-    // moves, ten times an interface move, get warps of their own)
+    // the three queues laid end to end -- trapped [0, qa), junction [qa, qa+qj),
+    // interior [qa+qj, qa+qj+qb) -- over at most N threads: a warp holds nodes of
+    // one kind (a junction move costs several interface moves), save the two warps
+    // at the seams
     const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int qa = *((volatile int*)&G->qtrap), qb = *((volatile int*)&G->qint), qj = *((volatile int*)&G->qjun);
-    const int64_t b0 = blockIdx.x * (int64_t)blockDim.x, b1 = b0 + blockDim.x;
-    if ((b0 >= qa && b1 <= N - qb) || b0 >= N + qj) {
-        return;   // the whole block lies between the queues or past the junction queue
+    const int64_t tot = (int64_t)qa + qj + qb;
+    if (blockIdx.x * (int64_t)blockDim.x >= tot) {
+        return;
     }
     int64_t i = -1;
-    if (q < N ? (q < qa || q >= N - qb) : q < N + qj) {
+    if (q < qa) {
         i = queue[q];
+    } else if (q < (int64_t)qa + qj) {
+        i = queue[N + (q - qa)];
+    } else if (q < tot) {
+        i = queue[N - 1 - (q - qa - qj)];
     }
     const int v = i >= 0 ? nodevol[i] : -1;
     const unsigned lane = threadIdx.x & 31u;
@@ -1386,7 +1392,7 @@ void launch_move(cudaStream_t s, const Dev& d) {
     k_move_pre<<<nblk(d.N, kMoveThreads), kMoveThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.F, d.Vel, d.typ,
                                                                 d.mv, d.pw, d.P0, d.S, d.queue, d.psum, d.rlist, d.G,
                                                                 d.N);
-    k_move_main<<<nblk(2 * d.N, kMainThreads), kMainThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.Vel, d.typ, d.lab,
+    k_move_main<<<nblk(d.N, kMainThreads), kMainThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.Vel, d.typ, d.lab,
                                                                  d.part, d.mv, d.P0, d.S, d.queue, d.rlist, d.G, d.N);
 }
 
