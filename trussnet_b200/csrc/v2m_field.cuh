@@ -315,6 +315,55 @@ __device__ __forceinline__ int owner_label(const DGrid& g, int voxmode, float px
     return best;
 }
 
+// owner_label's label-field branch (gm == 0), also handing out the cell it
+// ranked the labels on (*ranked = 1; not when the brick lists one label)
+__device__ __forceinline__ int owner_on_cell(const DGrid& g, float px, float py, float pz, int* second, Cell& cl,
+                                             int* ranked) {
+    LabList ll;
+    const int n = labels_near(g, px, py, pz, ll);
+    int best = ll.get(0), sec = V2M_NOLAB;
+    float pb = -1.0f, ps = pb;
+    *ranked = 0;
+    if (n == 1) {
+        *second = V2M_NOLAB;
+        return best;
+    }
+    cell_at(g, px, py, pz, cl);
+    *ranked = 1;
+#pragma unroll 1
+    for (int s = 0; s < n; s += 2) {
+        const int l0 = ll.get(s);
+        const bool two = s + 1 < n;
+        const int l1 = two ? ll.get(s + 1) : l0;
+        float c0[8], c1[8];
+        cell_corners(g, cl, l0, c0);
+        cell_corners(g, cl, l1, c1);
+        const float v0 = trilerp8(c0, cl.fx, cl.fy, cl.fz), v1 = trilerp8(c1, cl.fx, cl.fy, cl.fz);
+        if (v0 > pb) {
+            ps = pb;
+            sec = best;
+            pb = v0;
+            best = l0;
+        } else if (v0 > ps) {
+            ps = v0;
+            sec = l0;
+        }
+        if (two) {
+            if (v1 > pb) {
+                ps = pb;
+                sec = best;
+                pb = v1;
+                best = l1;
+            } else if (v1 > ps) {
+                ps = v1;
+                sec = l1;
+            }
+        }
+    }
+    *second = sec;
+    return best;
+}
+
 // psi_ab = phi_a - phi_b at p (src/opencl/v2m_seed_body.cl:179-205)
 __device__ __noinline__ float psi(const DGrid& g, int a, int b, float px, float py, float pz) {
     float gv;
@@ -333,17 +382,10 @@ __device__ __noinline__ float psi(const DGrid& g, int a, int b, float px, float 
     return trilerp8(c, cl.fx, cl.fy, cl.fz);
 }
 
-// psi_ab and its cell-analytic gradient (src/opencl/v2m_seed_body.cl:211-247)
-// (one out-of-line copy returning (gradient, value); psi_grad below unpacks it)
-__device__ __noinline__ float4 psi_grad4(const DGrid& g, int a, int b, float px, float py, float pz) {
-    float gv, gr[3];
-    if (gray_psi(g, a, b, px, py, pz, &gv, gr)) {
-        return make_float4(gr[0], gr[1], gr[2], gv);
-    }
-    Cell cl;
-    cell_at(g, px, py, pz, cl);
+// psi_ab's value and cell-analytic gradient on a cell already located: (gradient, value)
+__device__ __forceinline__ float4 psi_grad_on(const DGrid& g, const Cell& cl, int a, int b) {
     const float fx = cl.fx, fy = cl.fy, fz = cl.fz;
-    float c[8], e[8];
+    float c[8], e[8], gr[3];
     cell_corners(g, cl, a, c);
     cell_corners(g, cl, b, e);
 #pragma unroll
@@ -359,6 +401,18 @@ __device__ __noinline__ float4 psi_grad4(const DGrid& g, int a, int b, float px,
     gr[1] = ((x10 - x00) + fz * ((x11 - x01) - (x10 - x00))) / g.vy;
     gr[2] = (y1 - y0) / g.vz;
     return make_float4(gr[0], gr[1], gr[2], y0 + fz * (y1 - y0));
+}
+
+// psi_ab and its cell-analytic gradient (src/opencl/v2m_seed_body.cl:211-247)
+// (one out-of-line copy returning (gradient, value); psi_grad below unpacks it)
+__device__ __noinline__ float4 psi_grad4(const DGrid& g, int a, int b, float px, float py, float pz) {
+    float gv, gr[3];
+    if (gray_psi(g, a, b, px, py, pz, &gv, gr)) {
+        return make_float4(gr[0], gr[1], gr[2], gv);
+    }
+    Cell cl;
+    cell_at(g, px, py, pz, cl);
+    return psi_grad_on(g, cl, a, b);
 }
 
 __device__ __forceinline__ float psi_grad(const DGrid& g, int a, int b, float px, float py, float pz, float* gr) {
@@ -945,9 +999,11 @@ __device__ __noinline__ float move_step(const DGrid& g, int hmode, float h, floa
         for (int k = 0; k < 3; ++k) {
             q[k] = p[k] + s[k];
         }
-        int sec;
+        int sec, ranked = 0;
         float mg;
-        const int l = owner_label(g, 0, q[0], q[1], q[2], &sec, &mg);
+        Cell oc;
+        const int l = g.gm > 0 ? owner_label(g, 0, q[0], q[1], q[2], &sec, &mg)
+                               : owner_on_cell(g, q[0], q[1], q[2], &sec, oc, &ranked);
         if (l != a) {
             b = l;
             float x[3], r[3];
@@ -967,8 +1023,10 @@ __device__ __noinline__ float move_step(const DGrid& g, int hmode, float h, floa
             ty = V2M_INTERFACE;
             st.pb = b;
         } else if (sec != V2M_NOLAB && snap > 0.0f) {
-            float gq[3];
-            const float v = psi_grad(g, a, sec, q[0], q[1], q[2], gq);
+            // psi_grad(a, sec) at q; on the cell the ranking located (the same cell psi_grad4 finds)
+            const float4 r = ranked ? psi_grad_on(g, oc, a, sec) : psi_grad4(g, a, sec, q[0], q[1], q[2]);
+            const float gq[3] = { r.x, r.y, r.z };
+            const float v = r.w;
             const float gn = sqrtf(gq[0] * gq[0] + gq[1] * gq[1] + gq[2] * gq[2]);
             if (gn > 1e-9f && v / gn < snap * h && project1(g, a, sec, q, 1.2f * snap * h)) {
                 ty = V2M_INTERFACE;
