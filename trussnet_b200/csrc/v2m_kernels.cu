@@ -50,6 +50,14 @@ __device__ __forceinline__ int bin_coord(const DHash& H, int L, float x, float o
     return c < 0 ? 0 : (c >= n ? n - 1 : c);
 }
 
+// bin_coord with a reciprocal of the bin side instead of the division: within
+// a few 1e-5 of a bin of it, for search boxes that are widened by more than that
+__device__ __forceinline__ int bin_coord_near(const DHash& H, int L, float x, float o, int ax, float inv) {
+    const int c = (int)floorf((x - o) * inv);
+    const int n = H.dim[L][ax];
+    return c < 0 ? 0 : (c >= n ? n - 1 : c);
+}
+
 __device__ __forceinline__ int bin_key(const DHash& H, int L, float px, float py, float pz) {
     const int cx = bin_coord(H, L, px, H.ox, 0), cy = bin_coord(H, L, py, H.oy, 1), cz = bin_coord(H, L, pz, H.oz, 2);
     return H.off[L] + cx + H.dim[L][0] * (cy + H.dim[L][1] * cz);
@@ -389,22 +397,39 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
     // half-width): rows and the ends of rows wholly farther than r (with a
     // margin of 1e-3 b for rounding) hold only rejected candidates and are
     // skipped. The top level also holds larger nodes: it is scanned whole.
+    // (below the top level the box is widened by 1e-3 b and found with a
+    // reciprocal: it still holds every bin within r; the top level's box is
+    // the reference's, from the same divisions)
     int lx0[3], lx1[3], ly0[3], lz0[3], lny[3], lrow[4], lkey[3];
+    float linv[3];
     lrow[0] = 0;
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
         const int L = Li - 1 + q;
         int nrows = 0;
         lx0[q] = lx1[q] = ly0[q] = lz0[q] = lny[q] = lkey[q] = 0;
+        linv[q] = 0.0f;
         if (L >= 0 && L < H.nlev) {
             const float bL = H.b0 * (float)(1 << L);
             const float r = 0.5f * (Ri + bL);
-            lx0[q] = bin_coord(H, L, px - r, H.ox, 0);
-            lx1[q] = bin_coord(H, L, px + r, H.ox, 0);
-            ly0[q] = bin_coord(H, L, py - r, H.oy, 1);
-            const int y1 = bin_coord(H, L, py + r, H.oy, 1);
-            lz0[q] = bin_coord(H, L, pz - r, H.oz, 2);
-            const int z1 = bin_coord(H, L, pz + r, H.oz, 2);
+            int y1, z1;
+            if (L < H.nlev - 1) {
+                const float inv = 1.0f / bL, rw = r + 1e-3f * bL;
+                linv[q] = inv;
+                lx0[q] = bin_coord_near(H, L, px - rw, H.ox, 0, inv);
+                lx1[q] = bin_coord_near(H, L, px + rw, H.ox, 0, inv);
+                ly0[q] = bin_coord_near(H, L, py - rw, H.oy, 1, inv);
+                y1 = bin_coord_near(H, L, py + rw, H.oy, 1, inv);
+                lz0[q] = bin_coord_near(H, L, pz - rw, H.oz, 2, inv);
+                z1 = bin_coord_near(H, L, pz + rw, H.oz, 2, inv);
+            } else {
+                lx0[q] = bin_coord(H, L, px - r, H.ox, 0);
+                lx1[q] = bin_coord(H, L, px + r, H.ox, 0);
+                ly0[q] = bin_coord(H, L, py - r, H.oy, 1);
+                y1 = bin_coord(H, L, py + r, H.oy, 1);
+                lz0[q] = bin_coord(H, L, pz - r, H.oz, 2);
+                z1 = bin_coord(H, L, pz + r, H.oz, 2);
+            }
             lny[q] = y1 - ly0[q] + 1;
             nrows = lny[q] * (z1 - lz0[q] + 1);
             lkey[q] = H.off[L] + lx0[q];
@@ -439,8 +464,8 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
                     skip = true;
                 } else {
                     const float w = sqrtf(rem) + m;
-                    xa = max(xa, bin_coord(H, L, px - w, H.ox, 0));
-                    xb = min(xb, bin_coord(H, L, px + w, H.ox, 0));
+                    xa = max(xa, bin_coord_near(H, L, px - w, H.ox, 0, linv[q]));
+                    xb = min(xb, bin_coord_near(H, L, px + w, H.ox, 0, linv[q]));
                     skip = xa > xb;
                 }
             }
