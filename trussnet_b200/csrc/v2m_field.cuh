@@ -14,6 +14,7 @@
 // as 8 registers (LabList), so the label loops do not spill to local memory.
 #pragma once
 
+#include <climits>
 #include <cstdint>
 
 #include "v2m_types.cuh"
@@ -382,16 +383,10 @@ __device__ __noinline__ float psi(const DGrid& g, int a, int b, float px, float 
     return trilerp8(c, cl.fx, cl.fy, cl.fz);
 }
 
-// psi_ab's value and cell-analytic gradient on a cell already located: (gradient, value)
-__device__ __forceinline__ float4 psi_grad_on(const DGrid& g, const Cell& cl, int a, int b) {
-    const float fx = cl.fx, fy = cl.fy, fz = cl.fz;
-    float c[8], e[8], gr[3];
-    cell_corners(g, cl, a, c);
-    cell_corners(g, cl, b, e);
-#pragma unroll
-    for (int n = 0; n < 8; ++n) {
-        c[n] -= e[n];
-    }
+// psi's value and cell-analytic gradient from the corner differences
+// c = phi_a - phi_b and the fractions: (gradient, value)
+__device__ __forceinline__ float4 psi_grad_diff(const DGrid& g, const float* c, float fx, float fy, float fz) {
+    float gr[3];
     const float x00 = c[0] + fx * (c[1] - c[0]), x10 = c[2] + fx * (c[3] - c[2]);
     const float x01 = c[4] + fx * (c[5] - c[4]), x11 = c[6] + fx * (c[7] - c[6]);
     const float y0 = x00 + fy * (x10 - x00), y1 = x01 + fy * (x11 - x01);
@@ -401,6 +396,61 @@ __device__ __forceinline__ float4 psi_grad_on(const DGrid& g, const Cell& cl, in
     gr[1] = ((x10 - x00) + fz * ((x11 - x01) - (x10 - x00))) / g.vy;
     gr[2] = (y1 - y0) / g.vz;
     return make_float4(gr[0], gr[1], gr[2], y0 + fz * (y1 - y0));
+}
+
+// psi_ab's value and cell-analytic gradient on a cell already located: (gradient, value)
+__device__ __forceinline__ float4 psi_grad_on(const DGrid& g, const Cell& cl, int a, int b) {
+    float c[8], e[8];
+    cell_corners(g, cl, a, c);
+    cell_corners(g, cl, b, e);
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+        c[n] -= e[n];
+    }
+    return psi_grad_diff(g, c, cl.fx, cl.fy, cl.fz);
+}
+
+// The corner differences phi_a - phi_b of the last cell a search evaluated psi_ab
+// on (label fields): the probes of a bracketed search mostly stay in one cell,
+// and there psi and its gradient need no memory access. The values are the
+// ones psi / psi_grad4 read (same cell, same corners), so the results are too.
+struct PsiCache {
+    int i0, j0, k0;   // i0 == INT_MIN: empty
+    float d[8];
+};
+
+__device__ __forceinline__ PsiCache psi_cache_empty() {
+    PsiCache pc;
+    pc.i0 = pc.j0 = pc.k0 = INT_MIN;
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+        pc.d[n] = 0.0f;
+    }
+    return pc;
+}
+
+// p's cell into the cache (read from the tables unless it is the cached one); its fractions out
+__device__ __forceinline__ void psi_cache_at(const DGrid& g, int a, int b, float px, float py, float pz, PsiCache& pc,
+                                             float& fx, float& fy, float& fz) {
+    const float u = px / g.vx, v = py / g.vy, w = pz / g.vz;
+    const int i0 = (int)floorf(u), j0 = (int)floorf(v), k0 = (int)floorf(w);
+    fx = u - i0;
+    fy = v - j0;
+    fz = w - k0;
+    if (i0 != pc.i0 || j0 != pc.j0 || k0 != pc.k0) {
+        Cell cl;
+        cell_at(g, px, py, pz, cl);
+        float c[8], e[8];
+        cell_corners(g, cl, a, c);
+        cell_corners(g, cl, b, e);
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+            pc.d[n] = c[n] - e[n];
+        }
+        pc.i0 = i0;
+        pc.j0 = j0;
+        pc.k0 = k0;
+    }
 }
 
 // psi_ab and its cell-analytic gradient (src/opencl/v2m_seed_body.cl:211-247)
@@ -413,6 +463,27 @@ __device__ __noinline__ float4 psi_grad4(const DGrid& g, int a, int b, float px,
     Cell cl;
     cell_at(g, px, py, pz, cl);
     return psi_grad_on(g, cl, a, b);
+}
+
+// psi and psi_grad4 through a PsiCache (the gray-scale branch bypasses it)
+__device__ __forceinline__ float psi_c(const DGrid& g, int a, int b, float px, float py, float pz, PsiCache& pc) {
+    float gv;
+    if (gray_psi(g, a, b, px, py, pz, &gv, nullptr)) {
+        return gv;
+    }
+    float fx, fy, fz;
+    psi_cache_at(g, a, b, px, py, pz, pc, fx, fy, fz);
+    return trilerp8(pc.d, fx, fy, fz);
+}
+
+__device__ __forceinline__ float4 psi_grad4_c(const DGrid& g, int a, int b, float px, float py, float pz, PsiCache& pc) {
+    float gv, gr[3];
+    if (gray_psi(g, a, b, px, py, pz, &gv, gr)) {
+        return make_float4(gr[0], gr[1], gr[2], gv);
+    }
+    float fx, fy, fz;
+    psi_cache_at(g, a, b, px, py, pz, pc, fx, fy, fz);
+    return psi_grad_diff(g, pc.d, fx, fy, fz);
 }
 
 __device__ __forceinline__ float psi_grad(const DGrid& g, int a, int b, float px, float py, float pz, float* gr) {
@@ -429,7 +500,7 @@ __device__ __forceinline__ float psi_grad(const DGrid& g, int a, int b, float px
 // (p, 0) otherwise. (The out-of-line helpers take and return points by value,
 // so their callers' points stay in registers; the pointer forms below wrap them.)
 __device__ __noinline__ float4 bisect_dirv(const DGrid& g, int a, int b, float px, float py, float pz, float ux,
-                                           float uy, float uz, float v0, float rad, float tg) {
+                                           float uy, float uz, float v0, float rad, float tg, PsiCache pc) {
     const float p[3] = { px, py, pz }, u[3] = { ux, uy, uz };
     if (v0 == 0.0f) {
         return make_float4(px, py, pz, 1.0f);
@@ -438,7 +509,7 @@ __device__ __noinline__ float4 bisect_dirv(const DGrid& g, int a, int b, float p
     float t0 = 0.0f, t1 = -1.0f, f0 = v0, f1 = 0.0f;
     float t = (tg > 0.0f && tg < rad) ? tg : 0.25f * rad;
     for (int k = 0; k < 8; ++k) {
-        const float v = psi(g, a, b, p[0] + sg * t * u[0], p[1] + sg * t * u[1], p[2] + sg * t * u[2]);
+        const float v = psi_c(g, a, b, p[0] + sg * t * u[0], p[1] + sg * t * u[1], p[2] + sg * t * u[2], pc);
         if ((v > 0.0f) != (v0 > 0.0f) || v == 0.0f) {
             t1 = t;
             f1 = v;
@@ -457,7 +528,7 @@ __device__ __noinline__ float4 bisect_dirv(const DGrid& g, int a, int b, float p
     int side = 0;
     for (int it = 0; it < 8 && f1 != 0.0f && fabsf(t1 - t0) > 1e-4f * rad; ++it) {
         const float tm = (f0 != f1) ? t1 - f1 * (t1 - t0) / (f1 - f0) : 0.5f * (t0 + t1);
-        const float v = psi(g, a, b, p[0] + sg * tm * u[0], p[1] + sg * tm * u[1], p[2] + sg * tm * u[2]);
+        const float v = psi_c(g, a, b, p[0] + sg * tm * u[0], p[1] + sg * tm * u[1], p[2] + sg * tm * u[2], pc);
         if ((v > 0.0f) == (f1 > 0.0f)) {
             t1 = tm;
             f1 = v;
@@ -478,7 +549,7 @@ __device__ __noinline__ float4 bisect_dirv(const DGrid& g, int a, int b, float p
 
 __device__ __forceinline__ int bisect_dir(const DGrid& g, int a, int b, float* p, const float* u, float v0, float rad,
                                           float tg) {
-    const float4 r = bisect_dirv(g, a, b, p[0], p[1], p[2], u[0], u[1], u[2], v0, rad, tg);
+    const float4 r = bisect_dirv(g, a, b, p[0], p[1], p[2], u[0], u[1], u[2], v0, rad, tg, psi_cache_empty());
     p[0] = r.x;
     p[1] = r.y;
     p[2] = r.z;
@@ -486,18 +557,21 @@ __device__ __forceinline__ int bisect_dir(const DGrid& g, int a, int b, float* p
 }
 
 // Projection onto psi_ab = 0 along the local normal within rad (src/opencl/v2m_seed_body.cl:324-335)
-__device__ __noinline__ float4 project1v(const DGrid& g, int a, int b, float px, float py, float pz, float rad) {
-    float gr[3];
-    const float v = psi_grad(g, a, b, px, py, pz, gr);
+// (pc: a cache of psi_ab's corners from the caller, or empty)
+__device__ __noinline__ float4 project1v(const DGrid& g, int a, int b, float px, float py, float pz, float rad,
+                                         PsiCache pc) {
+    const float4 r4 = psi_grad4_c(g, a, b, px, py, pz, pc);
+    const float gr[3] = { r4.x, r4.y, r4.z };
+    const float v = r4.w;
     const float gn = sqrtf(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
     if (gn < 1e-9f) {
         return make_float4(px, py, pz, 0.0f);
     }
-    return bisect_dirv(g, a, b, px, py, pz, gr[0] / gn, gr[1] / gn, gr[2] / gn, v, rad, 1.5f * fabsf(v) / gn);
+    return bisect_dirv(g, a, b, px, py, pz, gr[0] / gn, gr[1] / gn, gr[2] / gn, v, rad, 1.5f * fabsf(v) / gn, pc);
 }
 
 __device__ __forceinline__ int project1(const DGrid& g, int a, int b, float* p, float rad) {
-    const float4 r = project1v(g, a, b, p[0], p[1], p[2], rad);
+    const float4 r = project1v(g, a, b, p[0], p[1], p[2], rad, psi_cache_empty());
     p[0] = r.x;
     p[1] = r.y;
     p[2] = r.z;
@@ -556,12 +630,13 @@ __device__ __forceinline__ int project2(const DGrid& g, int a, int b, int c, flo
 __device__ __noinline__ float4 crossingv(const DGrid& g, int a, int b, float px, float py, float pz, float qx,
                                          float qy, float qz) {
     const float p[3] = { px, py, pz }, q[3] = { qx, qy, qz };
+    PsiCache pc = psi_cache_empty();
     float t0 = 0.0f, t1 = 1.0f;
-    float v0 = psi(g, a, b, p[0], p[1], p[2]);
-    float v1 = psi(g, a, b, q[0], q[1], q[2]);
+    float v0 = psi_c(g, a, b, p[0], p[1], p[2], pc);
+    float v1 = psi_c(g, a, b, q[0], q[1], q[2], pc);
     for (int it = 0; it < 6; ++it) {
         const float tm = 0.5f * (t0 + t1);
-        const float vm = psi(g, a, b, p[0] + tm * (q[0] - p[0]), p[1] + tm * (q[1] - p[1]), p[2] + tm * (q[2] - p[2]));
+        const float vm = psi_c(g, a, b, p[0] + tm * (q[0] - p[0]), p[1] + tm * (q[1] - p[1]), p[2] + tm * (q[2] - p[2]), pc);
         if (vm > 0.0f) {
             t0 = tm;
             v0 = vm;
@@ -1035,13 +1110,29 @@ __device__ __noinline__ float move_step(const DGrid& g, int hmode, float h, floa
             }
         }
     } else if (ty == V2M_INTERFACE) {
-        tangential(g, a, b, p, s);
+        // tangential(p, s), then project1(q, h / 2) through one psi cache
+        PsiCache pc = psi_cache_empty();
+        {
+            const float4 r4 = psi_grad4_c(g, a, b, p[0], p[1], p[2], pc);
+            const float gr[3] = { r4.x, r4.y, r4.z };
+            const float gn2 = gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2];
+            if (!(gn2 < 1e-12f)) {
+                const float vn = (s[0] * gr[0] + s[1] * gr[1] + s[2] * gr[2]) / gn2;
+                for (int k = 0; k < 3; ++k) {
+                    s[k] -= vn * gr[k];
+                }
+            }
+        }
         for (int k = 0; k < 3; ++k) {
             q[k] = p[k] + s[k];
         }
-        if (!project1(g, a, b, q, 0.5f * h)) {
+        const float4 pr = project1v(g, a, b, q[0], q[1], q[2], 0.5f * h, pc);
+        if (pr.w == 0.0f) {
             return 0.0f;
         }
+        q[0] = pr.x;
+        q[1] = pr.y;
+        q[2] = pr.z;
     } else {
         float g1[3], g2[3], td[3];
         psi_grad(g, a, b, p[0], p[1], p[2], g1);
