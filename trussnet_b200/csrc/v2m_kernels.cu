@@ -320,6 +320,7 @@ constexpr int kCap = 64;
 struct NbrWarpSmem {
     float d[kCap];
     int id[kCap];
+    int rs0[32], rc[32];   // the non-empty rows of a batch, compacted
 };
 
 __device__ __forceinline__ bool pair_less(float da, int ia, float db, int ib) {
@@ -475,6 +476,21 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
                 c = cs[key0 + (xb - xa) + 1] - s0;
             }
         }
+        // compact the non-empty rows to the first lanes (so that row ends are
+        // distinct), then an inclusive prefix sum of their counts
+        {
+            const unsigned ne = __ballot_sync(0xffffffffu, c > 0);
+            if (c > 0) {
+                const int rk = __popc(ne & ((1u << lane) - 1u));
+                sm.rs0[rk] = s0;
+                sm.rc[rk] = c;
+            }
+            __syncwarp();
+            const int nne = __popc(ne);
+            s0 = lane < nne ? sm.rs0[lane] : 0;
+            c = lane < nne ? sm.rc[lane] : 0;
+            __syncwarp();
+        }
         int incl = c;
         for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, incl, o);
@@ -485,20 +501,14 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
         const int total = __shfl_sync(0xffffffffu, incl, 31);
         for (int cb = 0; cb < total; cb += 32) {
             const int q = cb + lane;
-            // row of candidate q: the first lane whose inclusive count exceeds q
-            int lo = 0, hi2 = 31;
-#pragma unroll
-            for (int st = 0; st < 5; ++st) {
-                const int mid = (lo + hi2) >> 1;
-                const int vm = __shfl_sync(0xffffffffu, incl, mid);
-                if (q < vm) {
-                    hi2 = mid;
-                } else {
-                    lo = mid + 1;
-                }
-            }
-            const int bs0 = __shfl_sync(0xffffffffu, s0, lo);
-            const int bexc = __shfl_sync(0xffffffffu, incl - c, lo);
+            // row of candidate q: the rows ending at or before q (row ends are
+            // distinct: a bit each for those inside this batch of 32)
+            const int before = __popc(__ballot_sync(0xffffffffu, c > 0 && incl <= cb));
+            const unsigned ends = __reduce_or_sync(
+                0xffffffffu, (c > 0 && incl > cb && incl < cb + 32) ? (1u << (incl - cb)) : 0u);
+            const int lo = before + __popc(ends & ((2u << lane) - 1u));
+            const int bs0 = __shfl_sync(0xffffffffu, s0, lo & 31);
+            const int bexc = __shfl_sync(0xffffffffu, incl - c, lo & 31);
             bool ok = false;
             float dist = 0.0f;
             int j = -1;
