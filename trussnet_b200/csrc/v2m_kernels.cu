@@ -357,6 +357,53 @@ __device__ __forceinline__ int warp_prune(NbrWarpSmem& sm, int m, int lane) {
     return m < V2M_K ? m : V2M_K;
 }
 
+// Buffer entries of the candidate scan come in two forms: accepted ones,
+// (distance, id); and raw ones, appended by the scan as (squared distance,
+// -(bin-order index + 1)), which passed the distance test only. Before a prune
+// (and at the end) the raw ones are checked -- node i itself and the
+// interior-across-labels test of src/opencl/v2m_particle_body.cl:104-123 -- and
+// given their distance, all in one pass over the buffer, instead of inside the
+// scan's batches. Returns the number of accepted entries, packed to the front.
+__device__ __forceinline__ int warp_validate(NbrWarpSmem& sm, int m, int lane, int64_t i, int ti_int, int li,
+                                             const int* __restrict__ sorted, const uint8_t* __restrict__ typ,
+                                             const uint16_t* __restrict__ lab) {
+    float dd[2];
+    int ii[2];
+    bool keep[2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        const int e = lane + 32 * r;
+        keep[r] = false;
+        dd[r] = 0.0f;
+        ii[r] = 0;
+        if (e < m) {
+            dd[r] = sm.d[e];
+            ii[r] = sm.id[e];
+            keep[r] = true;
+            if (ii[r] < 0) {
+                const int j = sorted[-ii[r] - 1];
+                keep[r] = j != (int)i && !(ti_int && typ[j] == V2M_INTERIOR && lab[j] != li);
+                ii[r] = j;
+                dd[r] = sqrtf(dd[r]);
+            }
+        }
+    }
+    __syncwarp();
+    int out = 0;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        const unsigned mk = __ballot_sync(0xffffffffu, keep[r]);
+        if (keep[r]) {
+            const int slot = out + __popc(mk & ((1u << lane) - 1u));
+            sm.d[slot] = dd[r];
+            sm.id[slot] = ii[r];
+        }
+        out += __popc(mk);
+    }
+    __syncwarp();
+    return out;
+}
+
 // Distance from p to the bin interval [o + c b, o + (c + 1) b) along one axis;
 // the edge bins reach to infinity (bin_coord clamps nodes outside the hash
 // grid into them).
@@ -439,10 +486,11 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
     }
     const int nrows = lrow[3];
     int m = 0;
-    // once the buffer holds K entries, the K-th smallest so far (after a prune,
-    // entry K-1): a candidate above it can never make the list
-    float bd = __int_as_float(0x7f800000);
-    int bid = 0x7FFFFFFF;
+    // once the buffer holds K entries, the K-th smallest distance so far (after a
+    // prune, entry K-1): a candidate whose squared distance is above bd2 =
+    // (1.0001 bd)^2 is farther than it, whatever the rounding, and can never
+    // make the list
+    float bd2 = __int_as_float(0x7f800000);
     for (int rb = 0; rb < nrows; rb += 32) {
         const int r = rb + lane;
         int s0 = 0, c = 0;
@@ -509,48 +557,38 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
             const int lo = before + __popc(ends & ((2u << lane) - 1u));
             const int bs0 = __shfl_sync(0xffffffffu, s0, lo & 31);
             const int bexc = __shfl_sync(0xffffffffu, incl - c, lo & 31);
+            // the distance test only; the rest waits for warp_validate
             bool ok = false;
-            float dist = 0.0f;
-            int j = -1;
+            float d2 = 0.0f;
+            int sidx = 0;
             if (q < total) {
-                // the id is read only for a candidate within range (node i itself,
-                // at distance 0, is dropped there)
-                const int sidx = bs0 + (q - bexc);
+                sidx = bs0 + (q - bexc);
                 const float4 ps = Ps[sidx];
                 const float ex = ps.x - px, ey = ps.y - py, ez = ps.z - pz;
-                const float d2 = ex * ex + ey * ey + ez * ez;
+                d2 = ex * ex + ey * ey + ez * ez;
                 const float rj = ts * 0.5f * (hi + ps.w);
-                ok = !(d2 >= rj * rj);
-                if (ok) {
-                    j = sorted[sidx];
-                    ok = j != (int)i;
-                }
-                if (ok && ti_int && typ[j] == V2M_INTERIOR && lab[j] != li) {
-                    ok = false;
-                }
-                if (ok) {
-                    dist = sqrtf(d2);
-                    ok = !(dist > bd || (dist == bd && j > bid));   // (a NaN distance is kept, as before)
-                }
+                ok = !(d2 >= rj * rj) && !(d2 > bd2);   // (a NaN distance is kept, as before)
             }
             const unsigned mask = __ballot_sync(0xffffffffu, ok);
             if (ok) {
                 const int slot = m + __popc(mask & ((1u << lane) - 1u));
-                sm.d[slot] = dist;
-                sm.id[slot] = j;
+                sm.d[slot] = d2;
+                sm.id[slot] = -sidx - 1;
             }
             m += __popc(mask);
             __syncwarp();
             if (m > kCap - 32) {
+                m = warp_validate(sm, m, lane, i, ti_int, li, sorted, typ, lab);
                 m = warp_prune(sm, m, lane);
                 if (m == V2M_K) {
-                    bd = sm.d[V2M_K - 1];
-                    bid = sm.id[V2M_K - 1];
+                    const float bd = sm.d[V2M_K - 1] * 1.0001f;
+                    bd2 = bd * bd;
                 }
             }
         }
     }
     // final ranks
+    m = warp_validate(sm, m, lane, i, ti_int, li, sorted, typ, lab);
     m = warp_prune(sm, m, lane);
     if (lane < m) {
         nbr[(int64_t)lane * N + i] = sm.id[lane];
