@@ -921,23 +921,19 @@ __global__ void __launch_bounds__(kMoveThreads) k_move_pre(const DVol* __restric
             }
         }
     }
-    // queue the moving nodes, one atomic per warp and kind: INTERFACE (and other
+    // queue the moving nodes, one atomic per block and kind: INTERFACE (and other
     // non-junction trapped) nodes from the front of queue[0, N), INTERIOR ones
     // from its back, JUNCTION ones from the front of queue[N, 2N)
+    __shared__ int sh_cnt[3][kMoveThreads / 32];
+    __shared__ int sh_base[3];
     const unsigned lane = threadIdx.x & 31u;
+    const int wid = threadIdx.x >> 5;
+    unsigned km[3];
 #pragma unroll
     for (int kind = 0; kind < 3; ++kind) {
-        const unsigned m = __ballot_sync(0xffffffffu, qkind == kind);
-        if (m) {
-            int base = 0;
-            if (lane == (unsigned)(__ffs(m) - 1)) {
-                base = atomicAdd(kind == 0 ? &G->qtrap : (kind == 1 ? &G->qint : &G->qjun), __popc(m));
-            }
-            base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
-            if (qkind == kind) {
-                const int slot = base + __popc(m & ((1u << lane) - 1u));
-                queue[kind == 0 ? (int64_t)slot : (kind == 1 ? N - 1 - slot : N + slot)] = (int)i;
-            }
+        km[kind] = __ballot_sync(0xffffffffu, qkind == kind);
+        if (lane == 0) {
+            sh_cnt[kind][wid] = __popc(km[kind]);
         }
     }
     double pd = active ? (double)pwv : 0.0;
@@ -945,9 +941,25 @@ __global__ void __launch_bounds__(kMoveThreads) k_move_pre(const DVol* __restric
         pd += __shfl_down_sync(0xffffffffu, pd, o);
     }
     if (lane == 0) {
-        sh_pw[threadIdx.x >> 5] = pd;
+        sh_pw[wid] = pd;
     }
     __syncthreads();
+    if (threadIdx.x < 3) {
+        const int kind = threadIdx.x;
+        int tot = 0;
+        for (int w = 0; w < kMoveThreads / 32; ++w) {
+            tot += sh_cnt[kind][w];
+        }
+        sh_base[kind] = tot ? atomicAdd(kind == 0 ? &G->qtrap : (kind == 1 ? &G->qint : &G->qjun), tot) : 0;
+    }
+    __syncthreads();
+    if (qkind >= 0) {
+        int slot = sh_base[qkind] + __popc(km[qkind] & ((1u << lane) - 1u));
+        for (int w = 0; w < wid; ++w) {
+            slot += sh_cnt[qkind][w];
+        }
+        queue[qkind == 0 ? (int64_t)slot : (qkind == 1 ? N - 1 - slot : N + slot)] = (int)i;
+    }
     const int bv = sh_vol;
     if (bv < 0) {
         return;
