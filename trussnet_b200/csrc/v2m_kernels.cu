@@ -1059,21 +1059,34 @@ __global__ void __launch_bounds__(kMainThreads, 8) k_move_main(const DVol* __res
     if (Vd.policy == 1) {
         md = __reduce_max_sync(gvol, __float_as_uint(sqrtf(m2) / hh));
     }
+    const int slot = blockIdx.x & (kCtlSlots - 1);
     if (lane == leader) {
         if (mx) {
-            atomicMax(&cv->maxbits, mx);
+            atomicMax(&cv->maxbits_p[slot], mx);
         }
         if (nh) {
-            atomicAdd(&cv->nhalf, (int)nh);
+            atomicAdd(&cv->nhalf_p[slot], (int)nh);
         }
         if (md) {
-            atomicMax(reinterpret_cast<unsigned*>(&cv->pad1), md);
+            atomicMax(&cv->maxd_p[slot], md);
         }
     }
-    if (refresh) {
-        const int e = atomicAdd(&G->nrefresh, 1);
-        rlist[e] = (int)i;
-        atomicAdd(&cv->nrefresh, 1);
+    // the refresh list: one atomic per warp
+    const unsigned rm = __ballot_sync(act, refresh);
+    if (rm) {
+        const unsigned first = (unsigned)(__ffs(rm) - 1);
+        int base = 0;
+        if (lane == first) {
+            base = atomicAdd(&G->nrefresh, __popc(rm));
+        }
+        base = __shfl_sync(act, base, first);
+        if (refresh) {
+            rlist[base + __popc(rm & ((1u << lane) - 1u))] = (int)i;
+        }
+        const unsigned rv = rm & gvol;
+        if (lane == leader && rv) {
+            atomicAdd(&cv->nrefresh, __popc(rv));
+        }
     }
 }
 
@@ -1263,6 +1276,15 @@ __global__ void k_control(const DVol* __restrict__ vols, VolCtl* __restrict__ ct
         }
     }
     c.iters = it + 1;
+    // fold the move kernel's slots
+    for (int k = 0; k < kCtlSlots; ++k) {
+        c.maxbits = c.maxbits > c.maxbits_p[k] ? c.maxbits : c.maxbits_p[k];
+        c.nhalf += c.nhalf_p[k];
+        c.pad1 = (unsigned)c.pad1 > c.maxd_p[k] ? c.pad1 : (int)c.maxd_p[k];
+        c.maxbits_p[k] = 0u;
+        c.nhalf_p[k] = 0;
+        c.maxd_p[k] = 0u;
+    }
     c.last_move = __uint_as_float(c.maxbits);
     int acc = 0, b99 = 31;
     for (int b = 0; b < 32; ++b) {

@@ -96,7 +96,15 @@ struct VolCtl {
     int nhalf;
     int nrefresh;
     int pad1;
+    // the move kernel's partial max / half-skin count / max displacement, spread
+    // over kCtlSlots slots (by block) to keep its atomics off one address; the
+    // control stage folds them into maxbits, nhalf and pad1
+    unsigned int maxbits_p[16];
+    int nhalf_p[16];
+    unsigned int maxd_p[16];
 };
+
+constexpr int kCtlSlots = 16;
 
 // Session-wide counters and the self-refresh work list.
 struct Global {
