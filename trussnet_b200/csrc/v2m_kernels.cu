@@ -448,43 +448,41 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
     // (below the top level the box is widened by 1e-3 b and found with a
     // reciprocal: it still holds every bin within r; the top level's box is
     // the reference's, from the same divisions)
-    int lx0[3], lx1[3], ly0[3], lz0[3], lny[3], lrow[4], lkey[3];
-    float linv[3];
-    lrow[0] = 0;
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-        const int L = Li - 1 + q;
-        int nrows = 0;
-        lx0[q] = lx1[q] = ly0[q] = lz0[q] = lny[q] = lkey[q] = 0;
-        linv[q] = 0.0f;
-        if (L >= 0 && L < H.nlev) {
+    // Lane q < 3 computes the box of level Li - 1 + q; a row takes its
+    // level's box from that lane by shuffle.
+    int bx0 = 0, bx1 = 0, by0 = 0, bz0 = 0, bny = 1, bkey = 0, bnr = 0;
+    float binv = 0.0f;
+    {
+        const int L = Li - 1 + lane;
+        if (lane < 3 && L >= 0 && L < H.nlev) {
             const float bL = H.b0 * (float)(1 << L);
             const float r = 0.5f * (Ri + bL);
             int y1, z1;
             if (L < H.nlev - 1) {
                 const float inv = 1.0f / bL, rw = r + 1e-3f * bL;
-                linv[q] = inv;
-                lx0[q] = bin_coord_near(H, L, px - rw, H.ox, 0, inv);
-                lx1[q] = bin_coord_near(H, L, px + rw, H.ox, 0, inv);
-                ly0[q] = bin_coord_near(H, L, py - rw, H.oy, 1, inv);
+                binv = inv;
+                bx0 = bin_coord_near(H, L, px - rw, H.ox, 0, inv);
+                bx1 = bin_coord_near(H, L, px + rw, H.ox, 0, inv);
+                by0 = bin_coord_near(H, L, py - rw, H.oy, 1, inv);
                 y1 = bin_coord_near(H, L, py + rw, H.oy, 1, inv);
-                lz0[q] = bin_coord_near(H, L, pz - rw, H.oz, 2, inv);
+                bz0 = bin_coord_near(H, L, pz - rw, H.oz, 2, inv);
                 z1 = bin_coord_near(H, L, pz + rw, H.oz, 2, inv);
             } else {
-                lx0[q] = bin_coord(H, L, px - r, H.ox, 0);
-                lx1[q] = bin_coord(H, L, px + r, H.ox, 0);
-                ly0[q] = bin_coord(H, L, py - r, H.oy, 1);
+                bx0 = bin_coord(H, L, px - r, H.ox, 0);
+                bx1 = bin_coord(H, L, px + r, H.ox, 0);
+                by0 = bin_coord(H, L, py - r, H.oy, 1);
                 y1 = bin_coord(H, L, py + r, H.oy, 1);
-                lz0[q] = bin_coord(H, L, pz - r, H.oz, 2);
+                bz0 = bin_coord(H, L, pz - r, H.oz, 2);
                 z1 = bin_coord(H, L, pz + r, H.oz, 2);
             }
-            lny[q] = y1 - ly0[q] + 1;
-            nrows = lny[q] * (z1 - lz0[q] + 1);
-            lkey[q] = H.off[L] + lx0[q];
+            bny = y1 - by0 + 1;
+            bnr = bny * (z1 - bz0 + 1);
+            bkey = H.off[L] + bx0;
         }
-        lrow[q + 1] = lrow[q] + nrows;
     }
-    const int nrows = lrow[3];
+    const int row1 = __shfl_sync(0xffffffffu, bnr, 0);
+    const int row2 = row1 + __shfl_sync(0xffffffffu, bnr, 1);
+    const int nrows = row2 + __shfl_sync(0xffffffffu, bnr, 2);
     int m = 0;
     // once the buffer holds K entries, the K-th smallest distance so far (after a
     // prune, entry K-1): a candidate whose squared distance is above bd2 =
@@ -493,14 +491,21 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
     float bd2 = __int_as_float(0x7f800000);
     for (int rb = 0; rb < nrows; rb += 32) {
         const int r = rb + lane;
+        const int q = r < row1 ? 0 : (r < row2 ? 1 : 2);
+        const int qx0 = __shfl_sync(0xffffffffu, bx0, q);
+        const int qx1 = __shfl_sync(0xffffffffu, bx1, q);
+        const int qy0 = __shfl_sync(0xffffffffu, by0, q);
+        const int qz0 = __shfl_sync(0xffffffffu, bz0, q);
+        const int qny = __shfl_sync(0xffffffffu, bny, q);
+        const int qkey = __shfl_sync(0xffffffffu, bkey, q);
+        const float qinv = __shfl_sync(0xffffffffu, binv, q);
         int s0 = 0, c = 0;
         if (r < nrows) {
-            const int q = r < lrow[1] ? 0 : (r < lrow[2] ? 1 : 2);
             const int L = Li - 1 + q;
-            const int rr = r - lrow[q];
-            const int zz = rr / lny[q];
-            const int cy = ly0[q] + (rr - zz * lny[q]), cz = lz0[q] + zz;
-            int xa = lx0[q], xb = lx1[q];
+            const int rr = r - (q == 0 ? 0 : (q == 1 ? row1 : row2));
+            const int zz = rr / qny;
+            const int cy = qy0 + (rr - zz * qny), cz = qz0 + zz;
+            int xa = qx0, xb = qx1;
             bool skip = false;
             if (L < H.nlev - 1) {
                 const float bL = H.b0 * (float)(1 << L);
@@ -513,13 +518,13 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
                     skip = true;
                 } else {
                     const float w = sqrtf(rem) + m;
-                    xa = max(xa, bin_coord_near(H, L, px - w, H.ox, 0, linv[q]));
-                    xb = min(xb, bin_coord_near(H, L, px + w, H.ox, 0, linv[q]));
+                    xa = max(xa, bin_coord_near(H, L, px - w, H.ox, 0, qinv));
+                    xb = min(xb, bin_coord_near(H, L, px + w, H.ox, 0, qinv));
                     skip = xa > xb;
                 }
             }
             if (!skip) {
-                const int key0 = lkey[q] + (xa - lx0[q]) + H.dim[L][0] * (cy + H.dim[L][1] * cz);
+                const int key0 = qkey + (xa - qx0) + H.dim[L][0] * (cy + H.dim[L][1] * cz);
                 s0 = cs[key0];
                 c = cs[key0 + (xb - xa) + 1] - s0;
             }
@@ -599,7 +604,9 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(kNbrMaxThreads) k_neighbors(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
+// 64 registers (32 resident warps per multiprocessor): faster than the
+// uncapped 71-register build, whose occupancy is lower.
+__global__ void __launch_bounds__(kNbrMaxThreads, 4) k_neighbors(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
                                                            const uint16_t* __restrict__ nodevol, const float4* __restrict__ Pq,
                                                            const uint8_t* __restrict__ typ, const uint16_t* __restrict__ lab,
                                                            const int* __restrict__ cstart, const int* __restrict__ sorted,
@@ -622,7 +629,7 @@ __global__ void __launch_bounds__(kNbrMaxThreads) k_neighbors(const DVol* __rest
 
 // The self-refresh of the nodes past a full skin (list filled by k_move), one
 // warp per entry; the last block to finish empties the list.
-__global__ void __launch_bounds__(kNbrMaxThreads) k_refresh(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
+__global__ void __launch_bounds__(kNbrMaxThreads, 4) k_refresh(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
                                                          const uint16_t* __restrict__ nodevol, const float4* __restrict__ Pq,
                                                          const uint8_t* __restrict__ typ, const uint16_t* __restrict__ lab,
                                                          const int* __restrict__ cstart, const int* __restrict__ sorted,
