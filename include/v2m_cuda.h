@@ -63,8 +63,11 @@ typedef struct {
     const float* h;              /* nx*ny*nz target size (mm) */
     float hmin, hmax;            /* range of h (mm): the hash geometry */
     const float* gI;             /* gray-scale intensity nx*ny*nz (gm > 0), else NULL */
-    const float* gTW;            /* gray-scale [t_0..t_{m-1}, W_0..W_{m-1}] (gm > 0), else NULL */
-    int32_t gm;                  /* number of gray thresholds; 0 = label volume; < 0 (analytic shapes) is rejected */
+    const float* gTW;            /* gray-scale [t_0..t_{m-1}, W_0..W_{m-1}] (gm > 0); the labels' compiled
+                                    analytic fields (gm < 0, the layout of src/opencl/v2m_sdf_body.cl:9-21);
+                                    else NULL */
+    int32_t gm;                  /* number of gray thresholds; 0 = label volume; < 0 = analytic shape fields */
+    int64_t ngTW;                /* floats in gTW (tn::Grid::gTW.size()); 0 = 2 gm (gray-scale) */
 } v2m_grid_view;
 
 /*

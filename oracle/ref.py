@@ -48,6 +48,9 @@ class RefLib:
         L.ref_grid_build.restype = vp
         L.ref_grid_build.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, C.c_float, C.c_float, C.c_float, C.c_float]
         L.ref_grid_view.argtypes = [vp, C.POINTER(GridView)]
+        L.ref_shape_grid.restype = vp
+        L.ref_shape_grid.argtypes = [C.c_char_p, C.c_char_p, C.c_double, C.c_double, C.c_double, C.c_int, C.c_float,
+                                     C.c_float, C.c_float, C.c_float]
         L.ref_grid_free.argtypes = [vp]
         L.ref_seed.restype = vp
         L.ref_seed.argtypes = [vp, vp, C.POINTER(C.c_int64)]
@@ -101,13 +104,27 @@ class RefLib:
     def build_and_seed(self, L, vs=(1.0, 1.0, 1.0), sigma=1.0, hbase=0.0, hmin=0.0, hmax=0.0,
                        prm: RelaxParams | None = None):
         """build_grid_cpu + seed_cpu of the reference (the pipeline's stages 2-3)."""
-        prm = prm or RelaxParams()
         L = np.ascontiguousarray(L, np.uint16)
         nz, ny, nx = L.shape
         vsa = np.array(vs, np.float32)
         h = self.L.ref_grid_build(L.ctypes.data, nx, ny, nz, vsa.ctypes.data, sigma, hbase, hmin, hmax)
         if not h:
             raise RuntimeError(self.err())
+        return self._grid_and_seeds(h, prm)
+
+    def shape_and_seed(self, scene: str, voxel=1.0, gap=0.0, margin=3.0, bricks=True, sigma=1.0, hbase=0.0,
+                       hmin=0.0, hmax=0.0, prm: RelaxParams | None = None, overlap="overwrite"):
+        """Shape input: the reference's shape compiler on a JSON scene, a grid
+        over its raster with the compiled program as the fields (gm = -1), and
+        seed_cpu on it (ref_shape_grid)."""
+        h = self.L.ref_shape_grid(scene.encode(), overlap.encode(), voxel, gap, margin, int(bricks), sigma, hbase,
+                                  hmin, hmax)
+        if not h:
+            raise RuntimeError(self.err())
+        return self._grid_and_seeds(h, prm)
+
+    def _grid_and_seeds(self, h, prm):
+        prm = prm or RelaxParams()
         try:
             gv = GridView()
             self.L.ref_grid_view(h, C.byref(gv))

@@ -7,6 +7,10 @@
 // What it exposes:
 //   ref_relax_cpu      tn::relax_cpu itself (src/v2m_particles.cpp:728-976)
 //   ref_grid_build     tn::build_grid_cpu (src/v2m_grid.cpp) on a label volume
+//   ref_shape_grid     shape input: the reference's shape compiler
+//                      (src/v2m_sdfshape.cpp) on a JSON scene, its raster's argmax
+//                      labels through build_grid_cpu, and the grid's fields set to
+//                      the compiled program (gm = -1), as src/v2m_grid.cpp:350-353
 //   ref_seed           tn::seed_cpu (src/v2m_particles.cpp:624-635)
 //   ref_state_*        relax_cpu's loop split into its stages (rebuild / force /
 //                      the rest of an iteration) over the reference's own bodies
@@ -28,6 +32,7 @@
 #include "v2m_grid.h"
 #include "v2m_omp.h"
 #include "v2m_particles.h"
+#include "v2m_sdfshape.h"
 #include "v2m_volume.h"
 
 #include "../include/v2m_cuda.h"
@@ -103,6 +108,9 @@ void grid_from_view(const v2m_grid_view* v, OwnedGrid& o) {
         o.gI.assign(v->gI, v->gI + nv);
         g.gI = o.gI.data();
         g.gTW.assign(v->gTW, v->gTW + 2 * v->gm);
+    } else if (v->gm < 0) {   // the analytic shape program
+        g.gI = nullptr;
+        g.gTW.assign(v->gTW, v->gTW + v->ngTW);
     } else {
         g.gI = nullptr;
         g.gTW.assign(1, 0.0f);
@@ -260,6 +268,58 @@ void* ref_grid_build(const uint16_t* labels, int nx, int ny, int nz, const float
     }
 }
 
+// Shape input. The scene is compiled (with the overlap rule) and its program completed as the
+// reference's shape front end does (src/v2m_modes.cpp:508-546: the gap-closing
+// radius gap and the cull margin, then the per-brick programs when bricks != 0,
+// then the raster that sets the field width, origin and blend radius). The
+// label volume is the raster's per-voxel argmax (the lowest label on a tie);
+// the grid is built from it (sigma, hbase, hmin, hmax as in ref_grid_build) and
+// then takes the program as its fields: gm = -1, gTW = the program.
+void* ref_shape_grid(const char* json, const char* overlap, double voxel, double gap, double margin, int bricks,
+                     float sigma, float hbase, float hmin, float hmax) {
+    try {
+        tn::ShapeScene sc = tn::load_shapes(std::string(json), true, std::string(overlap));
+        const size_t N = static_cast<size_t>(sc.nlab);
+        sc.prog[6 + N] = static_cast<float>(gap);
+        sc.prog[7 + N] = static_cast<float>(margin);
+        if (bricks) {
+            tn::build_brick_programs(sc, voxel);
+        }
+        const tn::Tpm t = tn::rasterize_scene(sc, voxel);
+        RefGrid* r = new RefGrid();
+        r->lv.nx = t.nx;
+        r->lv.ny = t.ny;
+        r->lv.nz = t.nz;
+        r->lv.voxelsize = { { static_cast<float>(voxel), static_cast<float>(voxel), static_cast<float>(voxel) } };
+        const size_t nv = t.nv();
+        r->lv.data.assign(nv, 0);
+        int m = 0;
+        for (size_t v = 0; v < nv; ++v) {
+            int best = 0;
+            for (int l = 1; l < t.C; ++l) {
+                if (t.p[static_cast<size_t>(l) * nv + v] > t.p[static_cast<size_t>(best) * nv + v]) {
+                    best = l;
+                }
+            }
+            r->lv.data[v] = static_cast<uint16_t>(best);
+            m = std::max(m, best);
+        }
+        r->lv.maxlabel = m;
+        tn::GridParams gp;
+        gp.sigma = sigma;
+        gp.hbase = hbase;
+        gp.hmin = hmin;
+        gp.hmax = hmax;
+        tn::build_grid_cpu(r->lv, gp, r->g);
+        r->g.gm = -1;
+        r->g.gTW = sc.prog;
+        return r;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return nullptr;
+    }
+}
+
 // Pointers into the reference grid (valid until ref_grid_free).
 int ref_grid_view(void* h, v2m_grid_view* v) {
     RefGrid* r = static_cast<RefGrid*>(h);
@@ -285,6 +345,7 @@ int ref_grid_view(void* h, v2m_grid_view* v) {
     v->gI = g.gI;
     v->gTW = g.gTW.empty() ? nullptr : g.gTW.data();
     v->gm = g.gm;
+    v->ngTW = static_cast<int64_t>(g.gTW.size());
     return 0;
 }
 

@@ -815,6 +815,9 @@ static void FN(free)(FN(state)* s) {
 }
 
 static FN(state)* FN(create)(const v2m_grid_view* g, const v2m_relax_params* p, const v2m_nodes_view* nd) {
+    /* analytic shape fields (gm < 0) are not restated here: the compiled
+       reference (oracle/_ref) is their checker */
+    if (g->gm < 0) return NULL;
     FN(state)* s = (FN(state)*)calloc(1, sizeof(FN(state)));
     if (!s) return NULL;
     s->nx = g->nx; s->ny = g->ny; s->nz = g->nz; s->nbx = g->nbx; s->nby = g->nby; s->nbz = g->nbz;

@@ -84,3 +84,82 @@ def copy_nodes(nd: Nodes) -> Nodes:
 def gray_small():
     """48^3 gray-scale sphere, 2 thresholds (labels 0..2)."""
     return synth.gray_sphere(dim=48, seed=6)
+
+
+# ---- shape input (analytic fields, gm < 0) ------------------------------------------
+# JSON scenes for the reference's shape compiler (src/v2m_sdfshape.cpp), chosen so
+# that together they reach every primitive the relaxation meets in practice and
+# the program's opcodes: MCX and JMesh vocabularies, CSG (CMIN / CMAX), the
+# "split" overlap rule (ADD, SCALE, CONST), per-brick programs and bounding-box
+# culling (BBOX, MCONST), crease blending and gap closing.
+SHAPE_SCENES = {
+    "mcx": ('{"Shapes": ['
+            '{"Grid": {"Tag": 0, "Size": [40, 40, 40]}},'
+            '{"Sphere": {"O": [20, 20, 20], "R": 14, "Tag": 1}},'
+            '{"Box": {"O": [12, 12, 17], "Size": [16, 16, 7], "Tag": 2}},'
+            '{"Cylinder": {"C0": [20, 20, 3], "C1": [20, 20, 37], "R": 4, "Tag": 3}},'
+            '{"Lens": {"O": [20, 20, 31], "Dir": [0, 0, 1], "R": 5, "Front": {"D": 2, "R": 8},'
+            ' "Back": {"D": 2, "R": 8}, "Tag": 4}}]}',
+            dict(overlap="overwrite", bricks=True, gap=0.0)),
+    "jmesh": ('{"ShapeBox3": {"O": [0, 0, 0], "P": [36, 36, 36], "Tag": 1},'
+              '"ShapePlane3": {"O": [0, 0, 30], "N": [0, 0.2, -1], "Tag": 5},'
+              '"ShapeEllipsoid": {"O": [18, 18, 14], "R": [10, 7, 5], "Angle": [30, 20], "Tag": 2},'
+              '"ShapeTorus": {"O": [18, 18, 24], "R": 9, "Rtube": 2.5, "N": [0, 0.3, 1], "Tag": 3},'
+              '"ShapeConeFrustum": {"O": [6, 6, 4], "P": [6, 6, 30], "R": [4, 1.5], "Tag": 4}}',
+              dict(overlap="overwrite", bricks=True, gap=0.0)),
+    "csg": ('{"CSGObject": [{"CSGSubtract": [{"CSGUnion": [{"ShapeSphere": {"O": [18, 18, 18], "R": 12}},'
+            '{"ShapeBox3": {"O": [8, 8, 15], "P": [28, 28, 21]}}]},'
+            '{"ShapeCylinder": {"O": [18, 18, 0], "P": [18, 18, 36], "R": 4}}]}, {"Tag": 1}],'
+            '"ShapeSphereShell": {"O": [18, 18, 18], "R": [6, 9], "Tag": 2}}',
+            dict(overlap="overwrite", bricks=False, gap=0.0)),
+    "split": ('{"Shapes": ['
+              '{"Grid": {"Tag": 0, "Size": [36, 36, 36]}},'
+              '{"ZSlabs": {"Bound": [[10, 20]], "Tag": 2}},'
+              '{"Sphere": {"O": [14, 18, 18], "R": 9, "Tag": 3}},'
+              '{"Sphere": {"O": [23, 18, 18], "R": 9, "Tag": 4}}]}',
+              dict(overlap="split", bricks=True, gap=2.0)),
+}
+
+
+def shape_case(ref, name, exact=False):
+    """A shape-input grid (gm = -1, gTW = the compiled program) and the
+    reference's seeds on it. exact: crease blending off (exact CSG)."""
+    scene, kw = SHAPE_SCENES[name]
+    g, nd = ref.shape_and_seed(scene, voxel=1.0, hbase=2.5, hmin=1.5, hmax=3.5, **kw)
+    if exact:
+        g.gTW = g.gTW.copy()
+        g.gTW[5 + int(g.gTW[0])] = 0.0
+    return g, nd
+
+
+def shape_opcodes(prog: np.ndarray):
+    """The primitive types and opcodes a compiled program holds (its documented
+    layout: src/opencl/v2m_sdf_body.cl:9-45), over every label's code and every
+    brick's."""
+    nparam = {1: 4, 2: 6, 3: 7, 4: 6, 5: 8, 6: 8, 7: 15, 8: 8, 9: 7}
+    N = int(prog[0])
+    starts = {int(prog[5 + l]) for l in range(N)}
+    T = int(prog[8 + N])
+    if T > 0:
+        nb = int(prog[T]) * int(prog[T + 1]) * int(prog[T + 2])
+        for b in range(nb):
+            off = int(prog[T + 4 + b])
+            starts.update(int(prog[off + l]) for l in range(N))
+    prims, ops = set(), set()
+    for pc in starts:
+        while True:
+            op = int(prog[pc])
+            ops.add(op)
+            if op == 0:
+                break
+            if op == 1:
+                t = int(prog[pc + 1])
+                prims.add(t)
+                pc += 2 + nparam[t]
+            elif op == 6:
+                pc += 9
+            elif op in (5, 7, 9):
+                pc += 2
+            else:
+                pc += 1
+    return prims, ops

@@ -1,0 +1,74 @@
+"""Shape input (analytic fields, gm < 0) without a GPU: the test scenes reach
+the whole program language of src/opencl/v2m_sdf_body.cl, and the C ABI checks
+a shape program before any device work."""
+import numpy as np
+import pytest
+
+import cases
+from trussnet_b200 import V2mError, _lib, relax_cl
+from trussnet_b200.types import RelaxParams
+
+
+def sphere_program(c, r, w=1.5):
+    """A two-label program in the documented layout (src/opencl/v2m_sdf_body.cl:9-21):
+    label 1 inside the sphere, label 0 (its complement) outside; no brick table."""
+    N = 2
+    head = [N, w, 0.0, 0.0, 0.0, 0, 0, 0.0, 0.0, 3.0, 0.0]
+    code1 = [1, 1, c[0], c[1], c[2], r, 0]            # PRIM SPHERE c r, END
+    code0 = [1, 1, c[0], c[1], c[2], r, 4, 0]         # PRIM SPHERE c r, NEG, END
+    head[5] = len(head)
+    head[6] = len(head) + len(code0)
+    return np.array(head + code0 + code1, np.float32)
+
+
+def test_shape_scenes_cover_the_program_language(ref):
+    prims, ops = set(), set()
+    for name in cases.SHAPE_SCENES:
+        g, nd = cases.shape_case(ref, name)
+        assert g.gm == -1 and nd.size() > 500
+        assert set(np.unique(nd.lab)) <= set(range(int(g.gTW[0])))
+        p, o = cases.shape_opcodes(g.gTW)
+        prims |= p
+        ops |= o
+    assert prims == set(range(1, 10)), prims      # every primitive type
+    assert ops == set(range(0, 12)), ops          # every opcode
+
+
+def test_shape_relax_reference_runs(ref):
+    g, nd = cases.shape_case(ref, "split")
+    st = ref.relax_cpu(g, cases.params(5), nd)
+    assert st.iters == 5
+
+
+def shape_grid(prog):
+    g, nd = cases.sphere_small()
+    return type(g)(**{**g.__dict__, "gm": -1, "gTW": prog}), nd
+
+
+def test_shape_program_checked_before_any_device():
+    c = (16.0, 16.0, 16.0)
+    good = sphere_program(c, 10.0)
+    bad = {
+        "label count": good.copy(),
+        "width": good.copy(),
+        "code offset": good.copy(),
+        "brick table": good.copy(),
+        "header": good[:8].copy(),
+    }
+    bad["label count"][0] = 0.0
+    bad["width"][1] = 0.0
+    bad["code offset"][5] = float(good.size)
+    bad["brick table"][10] = float(good.size)
+    for what, prog in bad.items():
+        g, nd = shape_grid(prog)
+        with pytest.raises(V2mError) as e:
+            relax_cl(g, RelaxParams(max_iters=1), nd)
+        assert e.value.code == _lib.V2M_ERR_ARG, what
+        assert "shape" in str(e.value) or "analytic" in str(e.value), (what, str(e.value))
+
+
+def test_oracle_restatement_declines_shapes():
+    from oracle.oracle import Oracle
+    g, nd = shape_grid(sphere_program((16.0, 16.0, 16.0), 10.0))
+    with pytest.raises(Exception):
+        Oracle("f32").relax(g, RelaxParams(max_iters=1), nd)

@@ -48,6 +48,7 @@ void relax_cl(const Grid& g, const RelaxParams& prm, Nodes& nd, RelaxStats& st, 
     gv.gI = g.gI;
     gv.gTW = g.gTW.empty() ? nullptr : g.gTW.data();
     gv.gm = g.gm;
+    gv.ngTW = static_cast<int64_t>(g.gTW.size());
 
     v2m_relax_params pv;
     v2m_relax_params_default(&pv);

@@ -17,6 +17,7 @@
 #include <climits>
 #include <cstdint>
 
+#include "v2m_sdf.cuh"
 #include "v2m_types.cuh"
 
 namespace v2m {
@@ -182,8 +183,23 @@ __device__ __forceinline__ float cell_phi(const DGrid& g, const Cell& c, int l) 
     return trilerp8(v, c.fx, c.fy, c.fz);
 }
 
+// phi_l at p, located in cell c: the analytic fields' own value, else the cell's
+// (src/opencl/v2m_seed_body.cl:33-39)
+template <bool kShape>
+__device__ __forceinline__ float field_phi(const DGrid& g, const Cell& c, int l, float px, float py, float pz) {
+    if constexpr (kShape) {
+        return sdf_phi(g, l, px, py, pz);
+    } else {
+        return cell_phi(g, c, l);
+    }
+}
+
 // phi_l trilinear at p (src/opencl/v2m_grid_body.cl:189-200)
+template <bool kShape>
 __device__ __noinline__ float phi_point(const DGrid& g, int l, float px, float py, float pz) {
+    if constexpr (kShape) {
+        return sdf_phi(g, l, px, py, pz);
+    }
     Cell c;
     cell_at(g, px, py, pz, c);
     return cell_phi(g, c, l);
@@ -232,8 +248,15 @@ __device__ __forceinline__ float gray_sample(const DGrid& g, float px, float py,
     return y0 + fz * (y1 - y0);
 }
 
-// psi_ab straight from the intensity for adjacent gray labels; 0 if not applicable
+// psi_ab straight from the field's own formula: the analytic shape fields
+// (gm < 0), or the intensity for adjacent gray labels; 0 if not applicable
+// (then psi comes from the sampled cells)
+template <bool kShape>
 __device__ __forceinline__ int gray_psi(const DGrid& g, int a, int b, float px, float py, float pz, float* val, float* gr) {
+    if constexpr (kShape) {
+        *val = sdf_psi(g, a, b, px, py, pz, gr);
+        return 1;
+    }
     if (g.gm <= 0 || (a - b != 1 && b - a != 1)) {
         return 0;
     }
@@ -250,6 +273,7 @@ __device__ __forceinline__ int gray_psi(const DGrid& g, int a, int b, float px, 
 
 // The label owning p: argmax phi_l (smooth mode) or the voxel's label (voxel
 // mode), with the runner-up and the margin (src/opencl/v2m_seed_body.cl:116-175).
+template <bool kShape>
 __device__ __forceinline__ int owner_label(const DGrid& g, int voxmode, float px, float py, float pz, int* second,
                                            float* margin) {
     const int i = (int)floorf(px / g.vx + 0.5f), j = (int)floorf(py / g.vy + 0.5f), k = (int)floorf(pz / g.vz + 0.5f);
@@ -268,11 +292,35 @@ __device__ __forceinline__ int owner_label(const DGrid& g, int voxmode, float px
     LabList ll;
     const int n = labels_near(g, px, py, pz, ll);
     int best = ll.get(0), sec = V2M_NOLAB;
-    float pb = -1.0f, ps = pb;
+    float pb = kShape ? -1e30f : -1.0f, ps = pb;
     if (n == 1) {
         *second = V2M_NOLAB;
         *margin = 1.0f;
         return best;
+    }
+    if constexpr (kShape) {
+        // analytic fields: ranked by s itself (phi saturates beyond w / 2 of a
+        // surface); the margin in phi units
+#pragma unroll 1
+        for (int s = 0; s < n; ++s) {
+            const int l = ll.get(s);
+            const float v = sdf_value(g, l, px, py, pz);
+            if (v > pb) {
+                ps = pb;
+                sec = best;
+                pb = v;
+                best = l;
+            } else if (v > ps) {
+                ps = v;
+                sec = l;
+            }
+        }
+        const float w = sdf_at(g, 1);
+        pb = fminf(1.0f, fmaxf(0.0f, 0.5f + pb / w));
+        ps = sec == V2M_NOLAB ? 0.0f : fminf(1.0f, fmaxf(0.0f, 0.5f + ps / w));
+        *second = sec;
+        *margin = pb - ps;
+        return voxmode ? label_at(g, i, j, k) : best;
     }
     Cell cl;
     cell_at(g, px, py, pz, cl);
@@ -366,9 +414,10 @@ __device__ __forceinline__ int owner_on_cell(const DGrid& g, float px, float py,
 }
 
 // psi_ab = phi_a - phi_b at p (src/opencl/v2m_seed_body.cl:179-205)
+template <bool kShape>
 __device__ __noinline__ float psi(const DGrid& g, int a, int b, float px, float py, float pz) {
     float gv;
-    if (gray_psi(g, a, b, px, py, pz, &gv, nullptr)) {
+    if (gray_psi<kShape>(g, a, b, px, py, pz, &gv, nullptr)) {
         return gv;
     }
     Cell cl;
@@ -455,9 +504,10 @@ __device__ __forceinline__ void psi_cache_at(const DGrid& g, int a, int b, float
 
 // psi_ab and its cell-analytic gradient (src/opencl/v2m_seed_body.cl:211-247)
 // (one out-of-line copy returning (gradient, value); psi_grad below unpacks it)
+template <bool kShape>
 __device__ __noinline__ float4 psi_grad4(const DGrid& g, int a, int b, float px, float py, float pz) {
     float gv, gr[3];
-    if (gray_psi(g, a, b, px, py, pz, &gv, gr)) {
+    if (gray_psi<kShape>(g, a, b, px, py, pz, &gv, gr)) {
         return make_float4(gr[0], gr[1], gr[2], gv);
     }
     Cell cl;
@@ -466,9 +516,10 @@ __device__ __noinline__ float4 psi_grad4(const DGrid& g, int a, int b, float px,
 }
 
 // psi and psi_grad4 through a PsiCache (the gray-scale branch bypasses it)
+template <bool kShape>
 __device__ __forceinline__ float psi_c(const DGrid& g, int a, int b, float px, float py, float pz, PsiCache& pc) {
     float gv;
-    if (gray_psi(g, a, b, px, py, pz, &gv, nullptr)) {
+    if (gray_psi<kShape>(g, a, b, px, py, pz, &gv, nullptr)) {
         return gv;
     }
     float fx, fy, fz;
@@ -476,9 +527,10 @@ __device__ __forceinline__ float psi_c(const DGrid& g, int a, int b, float px, f
     return trilerp8(pc.d, fx, fy, fz);
 }
 
+template <bool kShape>
 __device__ __forceinline__ float4 psi_grad4_c(const DGrid& g, int a, int b, float px, float py, float pz, PsiCache& pc) {
     float gv, gr[3];
-    if (gray_psi(g, a, b, px, py, pz, &gv, gr)) {
+    if (gray_psi<kShape>(g, a, b, px, py, pz, &gv, gr)) {
         return make_float4(gr[0], gr[1], gr[2], gv);
     }
     float fx, fy, fz;
@@ -486,8 +538,9 @@ __device__ __forceinline__ float4 psi_grad4_c(const DGrid& g, int a, int b, floa
     return psi_grad_diff(g, pc.d, fx, fy, fz);
 }
 
+template <bool kShape>
 __device__ __forceinline__ float psi_grad(const DGrid& g, int a, int b, float px, float py, float pz, float* gr) {
-    const float4 r = psi_grad4(g, a, b, px, py, pz);
+    const float4 r = psi_grad4<kShape>(g, a, b, px, py, pz);
     gr[0] = r.x;
     gr[1] = r.y;
     gr[2] = r.z;
@@ -499,6 +552,7 @@ __device__ __forceinline__ float psi_grad(const DGrid& g, int a, int b, float px
 // (src/opencl/v2m_seed_body.cl:255-320). Returns (the moved p, 1) on success,
 // (p, 0) otherwise. (The out-of-line helpers take and return points by value,
 // so their callers' points stay in registers; the pointer forms below wrap them.)
+template <bool kShape>
 __device__ __noinline__ float4 bisect_dirv(const DGrid& g, int a, int b, float px, float py, float pz, float ux,
                                            float uy, float uz, float v0, float rad, float tg, PsiCache pc) {
     const float p[3] = { px, py, pz }, u[3] = { ux, uy, uz };
@@ -509,7 +563,7 @@ __device__ __noinline__ float4 bisect_dirv(const DGrid& g, int a, int b, float p
     float t0 = 0.0f, t1 = -1.0f, f0 = v0, f1 = 0.0f;
     float t = (tg > 0.0f && tg < rad) ? tg : 0.25f * rad;
     for (int k = 0; k < 8; ++k) {
-        const float v = psi_c(g, a, b, p[0] + sg * t * u[0], p[1] + sg * t * u[1], p[2] + sg * t * u[2], pc);
+        const float v = psi_c<kShape>(g, a, b, p[0] + sg * t * u[0], p[1] + sg * t * u[1], p[2] + sg * t * u[2], pc);
         if ((v > 0.0f) != (v0 > 0.0f) || v == 0.0f) {
             t1 = t;
             f1 = v;
@@ -528,7 +582,7 @@ __device__ __noinline__ float4 bisect_dirv(const DGrid& g, int a, int b, float p
     int side = 0;
     for (int it = 0; it < 8 && f1 != 0.0f && fabsf(t1 - t0) > 1e-4f * rad; ++it) {
         const float tm = (f0 != f1) ? t1 - f1 * (t1 - t0) / (f1 - f0) : 0.5f * (t0 + t1);
-        const float v = psi_c(g, a, b, p[0] + sg * tm * u[0], p[1] + sg * tm * u[1], p[2] + sg * tm * u[2], pc);
+        const float v = psi_c<kShape>(g, a, b, p[0] + sg * tm * u[0], p[1] + sg * tm * u[1], p[2] + sg * tm * u[2], pc);
         if ((v > 0.0f) == (f1 > 0.0f)) {
             t1 = tm;
             f1 = v;
@@ -547,9 +601,10 @@ __device__ __noinline__ float4 bisect_dirv(const DGrid& g, int a, int b, float p
     return make_float4(p[0] + sg * t1 * u[0], p[1] + sg * t1 * u[1], p[2] + sg * t1 * u[2], 1.0f);
 }
 
+template <bool kShape>
 __device__ __forceinline__ int bisect_dir(const DGrid& g, int a, int b, float* p, const float* u, float v0, float rad,
                                           float tg) {
-    const float4 r = bisect_dirv(g, a, b, p[0], p[1], p[2], u[0], u[1], u[2], v0, rad, tg, psi_cache_empty());
+    const float4 r = bisect_dirv<kShape>(g, a, b, p[0], p[1], p[2], u[0], u[1], u[2], v0, rad, tg, psi_cache_empty());
     p[0] = r.x;
     p[1] = r.y;
     p[2] = r.z;
@@ -558,20 +613,22 @@ __device__ __forceinline__ int bisect_dir(const DGrid& g, int a, int b, float* p
 
 // Projection onto psi_ab = 0 along the local normal within rad (src/opencl/v2m_seed_body.cl:324-335)
 // (pc: a cache of psi_ab's corners from the caller, or empty)
+template <bool kShape>
 __device__ __noinline__ float4 project1v(const DGrid& g, int a, int b, float px, float py, float pz, float rad,
                                          PsiCache pc) {
-    const float4 r4 = psi_grad4_c(g, a, b, px, py, pz, pc);
+    const float4 r4 = psi_grad4_c<kShape>(g, a, b, px, py, pz, pc);
     const float gr[3] = { r4.x, r4.y, r4.z };
     const float v = r4.w;
     const float gn = sqrtf(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
     if (gn < 1e-9f) {
         return make_float4(px, py, pz, 0.0f);
     }
-    return bisect_dirv(g, a, b, px, py, pz, gr[0] / gn, gr[1] / gn, gr[2] / gn, v, rad, 1.5f * fabsf(v) / gn, pc);
+    return bisect_dirv<kShape>(g, a, b, px, py, pz, gr[0] / gn, gr[1] / gn, gr[2] / gn, v, rad, 1.5f * fabsf(v) / gn, pc);
 }
 
+template <bool kShape>
 __device__ __forceinline__ int project1(const DGrid& g, int a, int b, float* p, float rad) {
-    const float4 r = project1v(g, a, b, p[0], p[1], p[2], rad, psi_cache_empty());
+    const float4 r = project1v<kShape>(g, a, b, p[0], p[1], p[2], rad, psi_cache_empty());
     p[0] = r.x;
     p[1] = r.y;
     p[2] = r.z;
@@ -579,18 +636,48 @@ __device__ __forceinline__ int project1(const DGrid& g, int a, int b, float* p, 
 }
 
 // Projection onto the junction curve psi_ab = psi_ac = 0 by alternating
-// bracketed legs (src/opencl/v2m_seed_body.cl:342-420, sampled fields).
+// bracketed legs (src/opencl/v2m_seed_body.cl:342-420).
+template <bool kShape>
 __device__ __noinline__ float4 project2v(const DGrid& g, int a, int b, int c, float px, float py, float pz,
                                          float rad) {
     const float p[3] = { px, py, pz };
     float q[3] = { px, py, pz };
+    if constexpr (kShape) {
+        // analytic fields: of the three pairs' constraints, solve the two whose
+        // gradients are the most independent (the largest cross product), with
+        // the label they share as the pivot a (T-junctions of exact CSG have two
+        // parallel constraints there)
+        float gab[3], gac[3], gbc[3];
+        psi_grad<kShape>(g, a, b, q[0], q[1], q[2], gab);
+        psi_grad<kShape>(g, a, c, q[0], q[1], q[2], gac);
+        psi_grad<kShape>(g, b, c, q[0], q[1], q[2], gbc);
+        const float xa[3] = { gab[1] * gac[2] - gab[2] * gac[1], gab[2] * gac[0] - gab[0] * gac[2],
+                              gab[0] * gac[1] - gab[1] * gac[0] };
+        const float xb[3] = { gab[1] * gbc[2] - gab[2] * gbc[1], gab[2] * gbc[0] - gab[0] * gbc[2],
+                              gab[0] * gbc[1] - gab[1] * gbc[0] };
+        const float xc[3] = { gac[1] * gbc[2] - gac[2] * gbc[1], gac[2] * gbc[0] - gac[0] * gbc[2],
+                              gac[0] * gbc[1] - gac[1] * gbc[0] };
+        const float na = xa[0] * xa[0] + xa[1] * xa[1] + xa[2] * xa[2];
+        const float nb = xb[0] * xb[0] + xb[1] * xb[1] + xb[2] * xb[2];
+        const float nc = xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2];
+        if (nb > na && nb >= nc) {   // pivot b: psi_ba, psi_bc
+            const int t = a;
+            a = b;
+            b = t;
+        } else if (nc > na && nc > nb) {   // pivot c: psi_ca, psi_cb
+            const int t = a;
+            a = c;
+            c = b;
+            b = t;
+        }
+    }
     for (int it = 0; it < 3; ++it) {
         float g1[3], g2[3];
-        if (!project1(g, a, b, q, rad)) {
+        if (!project1<kShape>(g, a, b, q, rad)) {
             return make_float4(px, py, pz, 0.0f);
         }
-        psi_grad(g, a, b, q[0], q[1], q[2], g1);
-        const float v2 = psi_grad(g, a, c, q[0], q[1], q[2], g2);
+        psi_grad<kShape>(g, a, b, q[0], q[1], q[2], g1);
+        const float v2 = psi_grad<kShape>(g, a, c, q[0], q[1], q[2], g2);
         const float a11 = g1[0] * g1[0] + g1[1] * g1[1] + g1[2] * g1[2];
         if (a11 < 1e-18f) {
             return make_float4(px, py, pz, 0.0f);
@@ -604,11 +691,11 @@ __device__ __noinline__ float4 project2v(const DGrid& g, int a, int b, int c, fl
         u[0] /= un;
         u[1] /= un;
         u[2] /= un;
-        if (!bisect_dir(g, a, c, q, u, v2, rad, 1.5f * fabsf(v2) / un)) {
+        if (!bisect_dir<kShape>(g, a, c, q, u, v2, rad, 1.5f * fabsf(v2) / un)) {
             return make_float4(px, py, pz, 0.0f);
         }
     }
-    if (!project1(g, a, b, q, rad)) {
+    if (!project1<kShape>(g, a, b, q, rad)) {
         return make_float4(px, py, pz, 0.0f);
     }
     const float m2 = (q[0] - p[0]) * (q[0] - p[0]) + (q[1] - p[1]) * (q[1] - p[1]) + (q[2] - p[2]) * (q[2] - p[2]);
@@ -618,8 +705,9 @@ __device__ __noinline__ float4 project2v(const DGrid& g, int a, int b, int c, fl
     return make_float4(q[0], q[1], q[2], 1.0f);
 }
 
+template <bool kShape>
 __device__ __forceinline__ int project2(const DGrid& g, int a, int b, int c, float* p, float rad) {
-    const float4 r = project2v(g, a, b, c, p[0], p[1], p[2], rad);
+    const float4 r = project2v<kShape>(g, a, b, c, p[0], p[1], p[2], rad);
     p[0] = r.x;
     p[1] = r.y;
     p[2] = r.z;
@@ -627,16 +715,17 @@ __device__ __forceinline__ int project2(const DGrid& g, int a, int b, int c, flo
 }
 
 // Crossing of p -> q with psi_ab = 0: 6 bisections and a secant (src/opencl/v2m_particle_body.cl:188-212)
+template <bool kShape>
 __device__ __noinline__ float4 crossingv(const DGrid& g, int a, int b, float px, float py, float pz, float qx,
                                          float qy, float qz) {
     const float p[3] = { px, py, pz }, q[3] = { qx, qy, qz };
     PsiCache pc = psi_cache_empty();
     float t0 = 0.0f, t1 = 1.0f;
-    float v0 = psi_c(g, a, b, p[0], p[1], p[2], pc);
-    float v1 = psi_c(g, a, b, q[0], q[1], q[2], pc);
+    float v0 = psi_c<kShape>(g, a, b, p[0], p[1], p[2], pc);
+    float v1 = psi_c<kShape>(g, a, b, q[0], q[1], q[2], pc);
     for (int it = 0; it < 6; ++it) {
         const float tm = 0.5f * (t0 + t1);
-        const float vm = psi_c(g, a, b, p[0] + tm * (q[0] - p[0]), p[1] + tm * (q[1] - p[1]), p[2] + tm * (q[2] - p[2]), pc);
+        const float vm = psi_c<kShape>(g, a, b, p[0] + tm * (q[0] - p[0]), p[1] + tm * (q[1] - p[1]), p[2] + tm * (q[2] - p[2]), pc);
         if (vm > 0.0f) {
             t0 = tm;
             v0 = vm;
@@ -649,17 +738,19 @@ __device__ __noinline__ float4 crossingv(const DGrid& g, int a, int b, float px,
     return make_float4(p[0] + t * (q[0] - p[0]), p[1] + t * (q[1] - p[1]), p[2] + t * (q[2] - p[2]), 0.0f);
 }
 
+template <bool kShape>
 __device__ __forceinline__ void crossing(const DGrid& g, int a, int b, const float* p, const float* q, float* c) {
-    const float4 r = crossingv(g, a, b, p[0], p[1], p[2], q[0], q[1], q[2]);
+    const float4 r = crossingv<kShape>(g, a, b, p[0], p[1], p[2], q[0], q[1], q[2]);
     c[0] = r.x;
     c[1] = r.y;
     c[2] = r.z;
 }
 
 // Drop v's component along psi_ab's normal at p (src/opencl/v2m_particle_body.cl:215-229)
+template <bool kShape>
 __device__ __forceinline__ void tangential(const DGrid& g, int a, int b, const float* p, float* v) {
     float gr[3];
-    psi_grad(g, a, b, p[0], p[1], p[2], gr);
+    psi_grad<kShape>(g, a, b, p[0], p[1], p[2], gr);
     const float gn2 = gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2];
     if (gn2 < 1e-12f) {
         return;
@@ -671,6 +762,7 @@ __device__ __forceinline__ void tangential(const DGrid& g, int a, int b, const f
 }
 
 // A third label competing at q (phi_c > 0.5 phi_a), or NOLAB (src/opencl/v2m_particle_body.cl:232-260)
+template <bool kShape>
 __device__ __noinline__ int third_labelv(const DGrid& g, int a, int b, float qx, float qy, float qz) {
     const float q[3] = { qx, qy, qz };
     LabList ll;
@@ -688,14 +780,14 @@ __device__ __noinline__ int third_labelv(const DGrid& g, int a, int b, float qx,
     }
     Cell cl;
     cell_at(g, q[0], q[1], q[2], cl);
-    const float pa = cell_phi(g, cl, a);
+    const float pa = field_phi<kShape>(g, cl, a, q[0], q[1], q[2]);
     int c = V2M_NOLAB;
     float pc = 0.5f * pa;
 #pragma unroll 1
     for (int s = 0; s < n; ++s) {
         const int l = ll.get(s);
         if (l != a && l != b) {
-            const float w = cell_phi(g, cl, l);
+            const float w = field_phi<kShape>(g, cl, l, q[0], q[1], q[2]);
             if (w > pc) {
                 pc = w;
                 c = l;
@@ -705,11 +797,13 @@ __device__ __noinline__ int third_labelv(const DGrid& g, int a, int b, float qx,
     return c;
 }
 
+template <bool kShape>
 __device__ __forceinline__ int third_label(const DGrid& g, int a, int b, const float* q) {
-    return third_labelv(g, a, b, q[0], q[1], q[2]);
+    return third_labelv<kShape>(g, a, b, q[0], q[1], q[2]);
 }
 
 // Do the node's labels dominate at q? (src/opencl/v2m_particle_body.cl:266-291)
+template <bool kShape>
 __device__ __noinline__ int valid_onv(const DGrid& g, int a, int b, int c, float qx, float qy, float qz) {
     const float q[3] = { qx, qy, qz };
     LabList ll;
@@ -727,27 +821,29 @@ __device__ __noinline__ int valid_onv(const DGrid& g, int a, int b, int c, float
     }
     Cell cl;
     cell_at(g, q[0], q[1], q[2], cl);
-    float mine = fminf(cell_phi(g, cl, a), cell_phi(g, cl, b));
+    float mine = fminf(field_phi<kShape>(g, cl, a, q[0], q[1], q[2]), field_phi<kShape>(g, cl, b, q[0], q[1], q[2]));
     if (c != V2M_NOLAB) {
-        mine = fminf(mine, cell_phi(g, cl, c));
+        mine = fminf(mine, field_phi<kShape>(g, cl, c, q[0], q[1], q[2]));
     }
 #pragma unroll 1
     for (int s = 0; s < n; ++s) {
         const int l = ll.get(s);
-        if (l != a && l != b && l != c && cell_phi(g, cl, l) > mine + 0.02f) {
+        if (l != a && l != b && l != c && field_phi<kShape>(g, cl, l, q[0], q[1], q[2]) > mine + 0.02f) {
             return 0;
         }
     }
     return 1;
 }
 
+template <bool kShape>
 __device__ __forceinline__ int valid_on(const DGrid& g, int a, int b, int c, const float* q) {
-    return valid_onv(g, a, b, c, q[0], q[1], q[2]);
+    return valid_onv<kShape>(g, a, b, c, q[0], q[1], q[2]);
 }
 
 // third_label(a, b, q) and valid_on(a, b, NOLAB, q) together: one label list,
 // one cell and one phi evaluation per label serve both (the same values as
 // the two calls). Returns (third label or NOLAB, valid).
+template <bool kShape>
 __device__ __noinline__ int2 third_and_valid(const DGrid& g, int a, int b, float qx, float qy, float qz) {
     LabList ll;
     const int n = labels_near(g, qx, qy, qz, ll);
@@ -764,15 +860,15 @@ __device__ __noinline__ int2 third_and_valid(const DGrid& g, int a, int b, float
     }
     Cell cl;
     cell_at(g, qx, qy, qz, cl);
-    const float pa = cell_phi(g, cl, a);
-    const float mine = fminf(pa, cell_phi(g, cl, b));
+    const float pa = field_phi<kShape>(g, cl, a, qx, qy, qz);
+    const float mine = fminf(pa, field_phi<kShape>(g, cl, b, qx, qy, qz));
     int c = V2M_NOLAB, valid = 1;
     float pc = 0.5f * pa;
 #pragma unroll 1
     for (int s = 0; s < n; ++s) {
         const int l = ll.get(s);
         if (l != a && l != b) {
-            const float w = cell_phi(g, cl, l);
+            const float w = field_phi<kShape>(g, cl, l, qx, qy, qz);
             if (w > pc) {
                 pc = w;
                 c = l;
@@ -1056,6 +1152,7 @@ __device__ __noinline__ float move_voxel(const DGrid& g, int hmode, float h, flo
 // The trapped move with the (capped) step s (src/opencl/v2m_particle_body.cl:659-833).
 // ty0 is the type before the move; st is updated in place exactly where the
 // reference writes the node's arrays.
+template <bool kShape>
 __device__ __noinline__ float move_step(const DGrid& g, int hmode, float h, float* s, float maxstep, float snap,
                                         int voxmode, NodeState& st) {
     float p[3], q[3];
@@ -1077,20 +1174,20 @@ __device__ __noinline__ float move_step(const DGrid& g, int hmode, float h, floa
         int sec, ranked = 0;
         float mg;
         Cell oc;
-        const int l = g.gm > 0 ? owner_label(g, 0, q[0], q[1], q[2], &sec, &mg)
-                               : owner_on_cell(g, q[0], q[1], q[2], &sec, oc, &ranked);
+        const int l = (kShape || g.gm > 0) ? owner_label<kShape>(g, 0, q[0], q[1], q[2], &sec, &mg)
+                                           : owner_on_cell(g, q[0], q[1], q[2], &sec, oc, &ranked);
         if (l != a) {
             b = l;
             float x[3], r[3];
-            crossing(g, a, b, p, q, x);
+            crossing<kShape>(g, a, b, p, q, x);
             for (int k = 0; k < 3; ++k) {
                 r[k] = q[k] - x[k];
             }
-            tangential(g, a, b, x, r);
+            tangential<kShape>(g, a, b, x, r);
             for (int k = 0; k < 3; ++k) {
                 q[k] = x[k] + r[k];
             }
-            if (!project1(g, a, b, q, 0.5f * h)) {
+            if (!project1<kShape>(g, a, b, q, 0.5f * h)) {
                 q[0] = x[0];
                 q[1] = x[1];
                 q[2] = x[2];
@@ -1099,11 +1196,11 @@ __device__ __noinline__ float move_step(const DGrid& g, int hmode, float h, floa
             st.pb = b;
         } else if (sec != V2M_NOLAB && snap > 0.0f) {
             // psi_grad(a, sec) at q; on the cell the ranking located (the same cell psi_grad4 finds)
-            const float4 r = ranked ? psi_grad_on(g, oc, a, sec) : psi_grad4(g, a, sec, q[0], q[1], q[2]);
+            const float4 r = ranked ? psi_grad_on(g, oc, a, sec) : psi_grad4<kShape>(g, a, sec, q[0], q[1], q[2]);
             const float gq[3] = { r.x, r.y, r.z };
             const float v = r.w;
             const float gn = sqrtf(gq[0] * gq[0] + gq[1] * gq[1] + gq[2] * gq[2]);
-            if (gn > 1e-9f && v / gn < snap * h && project1(g, a, sec, q, 1.2f * snap * h)) {
+            if (gn > 1e-9f && v / gn < snap * h && project1<kShape>(g, a, sec, q, 1.2f * snap * h)) {
                 ty = V2M_INTERFACE;
                 b = sec;
                 st.pb = sec;
@@ -1113,7 +1210,7 @@ __device__ __noinline__ float move_step(const DGrid& g, int hmode, float h, floa
         // tangential(p, s), then project1(q, h / 2) through one psi cache
         PsiCache pc = psi_cache_empty();
         {
-            const float4 r4 = psi_grad4_c(g, a, b, p[0], p[1], p[2], pc);
+            const float4 r4 = psi_grad4_c<kShape>(g, a, b, p[0], p[1], p[2], pc);
             const float gr[3] = { r4.x, r4.y, r4.z };
             const float gn2 = gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2];
             if (!(gn2 < 1e-12f)) {
@@ -1126,7 +1223,7 @@ __device__ __noinline__ float move_step(const DGrid& g, int hmode, float h, floa
         for (int k = 0; k < 3; ++k) {
             q[k] = p[k] + s[k];
         }
-        const float4 pr = project1v(g, a, b, q[0], q[1], q[2], 0.5f * h, pc);
+        const float4 pr = project1v<kShape>(g, a, b, q[0], q[1], q[2], 0.5f * h, pc);
         if (pr.w == 0.0f) {
             return 0.0f;
         }
@@ -1135,8 +1232,8 @@ __device__ __noinline__ float move_step(const DGrid& g, int hmode, float h, floa
         q[2] = pr.z;
     } else {
         float g1[3], g2[3], td[3];
-        psi_grad(g, a, b, p[0], p[1], p[2], g1);
-        psi_grad(g, a, c, p[0], p[1], p[2], g2);
+        psi_grad<kShape>(g, a, b, p[0], p[1], p[2], g1);
+        psi_grad<kShape>(g, a, c, p[0], p[1], p[2], g2);
         td[0] = g1[1] * g2[2] - g1[2] * g2[1];
         td[1] = g1[2] * g2[0] - g1[0] * g2[2];
         td[2] = g1[0] * g2[1] - g1[1] * g2[0];
@@ -1145,7 +1242,7 @@ __device__ __noinline__ float move_step(const DGrid& g, int hmode, float h, floa
         for (int k = 0; k < 3; ++k) {
             q[k] = p[k] + stp * td[k];
         }
-        if (!project2(g, a, b, c, q, 0.5f * h)) {
+        if (!project2<kShape>(g, a, b, c, q, 0.5f * h)) {
             return 0.0f;
         }
     }
@@ -1153,12 +1250,12 @@ __device__ __noinline__ float move_step(const DGrid& g, int hmode, float h, floa
     // (third_and_valid also gives valid_on's answer for q as an INTERFACE node)
     int valid_here = -1;
     if (ty == V2M_INTERFACE) {
-        const int2 tv = third_and_valid(g, a, b, q[0], q[1], q[2]);
+        const int2 tv = third_and_valid<kShape>(g, a, b, q[0], q[1], q[2]);
         const int cc = tv.x;
         valid_here = tv.y;
         if (cc != V2M_NOLAB) {
             float r[3] = { q[0], q[1], q[2] };
-            if (project2(g, a, b, cc, r, 0.5f * h)) {
+            if (project2<kShape>(g, a, b, cc, r, 0.5f * h)) {
                 q[0] = r[0];
                 q[1] = r[1];
                 q[2] = r[2];
@@ -1181,11 +1278,11 @@ __device__ __noinline__ float move_step(const DGrid& g, int hmode, float h, floa
     // refuse a move onto an invalid branch of the constraint
     if (ty != V2M_INTERIOR &&
         !(ty == V2M_INTERFACE && valid_here >= 0 ? valid_here
-                                                  : valid_on(g, a, st.pb, ty >= V2M_JUNCTION ? st.pc : V2M_NOLAB, q))) {
+                                                  : valid_on<kShape>(g, a, st.pb, ty >= V2M_JUNCTION ? st.pc : V2M_NOLAB, q))) {
         if (ty == V2M_INTERFACE || ty_in == V2M_INTERIOR) {
-            const int cc = third_label(g, a, st.pb, q);
+            const int cc = third_label<kShape>(g, a, st.pb, q);
             float r[3] = { q[0], q[1], q[2] };
-            if (cc != V2M_NOLAB && project2(g, a, st.pb, cc, r, 0.5f * h) && valid_on(g, a, st.pb, cc, r)) {
+            if (cc != V2M_NOLAB && project2<kShape>(g, a, st.pb, cc, r, 0.5f * h) && valid_on<kShape>(g, a, st.pb, cc, r)) {
                 q[0] = r[0];
                 q[1] = r[1];
                 q[2] = r[2];

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -158,10 +159,35 @@ void validate(const v2m_grid_view* g, const v2m_relax_params* p, const v2m_nodes
         throw ArgError("grid array missing");
     }
     if (g->gm < 0) {
-        throw ArgError("analytic shape fields (gm < 0) are not supported by the CUDA relaxation");
+        // the analytic shape program: its header and code offsets (the device
+        // also bounds-checks every read of it)
+        if (!g->gTW || g->ngTW < 9 || g->ngTW > (int64_t)INT_MAX) {
+            throw ArgError("analytic shape fields need the program gTW and its length ngTW");
+        }
+        const float nf = g->gTW[0];
+        if (!(nf >= 1.0f && nf <= 65535.0f)) {
+            throw ArgError("shape program: label count out of range");
+        }
+        const int nl = (int)nf;
+        if ((int64_t)9 + nl > g->ngTW) {
+            throw ArgError("shape program shorter than its header");
+        }
+        if (!(g->gTW[1] > 0.0f)) {
+            throw ArgError("shape program: the field width must be positive");
+        }
+        for (int l = 0; l < nl; ++l) {
+            const float o = g->gTW[5 + l];
+            if (!(o >= 0.0f && o < (float)g->ngTW)) {
+                throw ArgError("shape program: code offset out of range");
+            }
+        }
+        const float T = g->gTW[8 + nl];
+        if (!(T == 0.0f || (T > 0.0f && (int64_t)T + 4 <= g->ngTW))) {
+            throw ArgError("shape program: brick table out of range");
+        }
     }
-    if (g->gm > 0 && (!g->gI || !g->gTW)) {
-        throw ArgError("gray-scale fields need gI and gTW");
+    if (g->gm > 0 && (!g->gI || !g->gTW || (g->ngTW != 0 && g->ngTW < 2 * (int64_t)g->gm))) {
+        throw ArgError("gray-scale fields need gI and gTW (2 gm floats)");
     }
     if (!(g->hmin > 0.0f) || !(g->hmax >= g->hmin)) {
         throw ArgError("need 0 < hmin <= hmax");
@@ -343,6 +369,10 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         s->refresh_blocks = sms * 4;
         s->d.sms = sms;
+        s->d.shape_any = 0;
+        for (int v = 0; v < nvol; ++v) {
+            s->d.shape_any |= gv[v].gm < 0;
+        }
         static const int env_div = std::getenv("V2M_REBUILD_DIV") ? std::atoi(std::getenv("V2M_REBUILD_DIV")) : 300;
         // layout
         int64_t N = 0, KT = 0;
@@ -442,9 +472,15 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
             if (g->gm > 0) {
                 V.g.gI = upload(s, g->gI, nvox);
                 V.g.gTW = upload(s, g->gTW, 2 * (size_t)g->gm);
+                V.g.ntw = 2 * (int64_t)g->gm;
+            } else if (g->gm < 0) {
+                V.g.gI = nullptr;
+                V.g.gTW = upload(s, g->gTW, (size_t)g->ngTW);
+                V.g.ntw = g->ngTW;
             } else {
                 V.g.gI = nullptr;
                 V.g.gTW = s->alloc<float>(4);
+                V.g.ntw = 0;
             }
             build_corner_tables(s, V.g, nb);
             V.nofs = I.nofs;

@@ -986,13 +986,18 @@ __global__ void __launch_bounds__(kMoveThreads) k_move_pre(const DVol* __restric
 // kMainThreads with no block-wide barrier: a warp's statistics are combined
 // with warp votes and flushed by one lane per (volume, bin), so a finished warp
 // never waits for a slower one.
+// Two instances: kShape = false moves the nodes of volumes with sampled fields,
+// kShape = true (launched only when some volume has them) those with analytic
+// shape fields; with both present each skips the other's nodes.
+template <bool kShape>
 __global__ void __launch_bounds__(kMainThreads, 8) k_move_main(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl,
                                                            const uint16_t* __restrict__ nodevol, float4* __restrict__ Pq,
                                                            float4* __restrict__ Vel, uint8_t* __restrict__ typ,
                                                            const uint16_t* __restrict__ lab, uint32_t* __restrict__ part,
                                                            float* __restrict__ mvout, const float4* __restrict__ P0,
                                                            const float4* __restrict__ S, const int* __restrict__ queue,
-                                                           int* __restrict__ rlist, Global* G, int64_t N) {
+                                                           int* __restrict__ rlist, Global* G, int64_t N,
+                                                           int shape_any) {
     // the three queues laid end to end -- trapped [0, qa), junction [qa, qa+qj),
     // interior [qa+qj, qa+qj+qb) -- over at most N threads: a warp holds nodes of
     // one kind (a junction move costs several interface moves), save the two warps
@@ -1011,7 +1016,10 @@ __global__ void __launch_bounds__(kMainThreads, 8) k_move_main(const DVol* __res
     } else if (q < tot) {
         i = queue[N - 1 - (q - qa - qj)];
     }
-    const int v = i >= 0 ? nodevol[i] : -1;
+    int v = i >= 0 ? nodevol[i] : -1;
+    if (shape_any && v >= 0 && (vols[v].g.gm < 0) != kShape) {
+        v = -1;   // the other instance moves it
+    }
     const unsigned lane = threadIdx.x & 31u;
     const unsigned act = __ballot_sync(0xffffffffu, v >= 0);
     if (v < 0) {
@@ -1034,7 +1042,7 @@ __global__ void __launch_bounds__(kMainThreads, 8) k_move_main(const DVol* __res
     st.pc = (int)(pp >> 16);
     const int ty0 = st.ty;
     float s[3] = { s4.x, s4.y, s4.z };
-    const float m = move_step(g, Vd.hmode, s4.w, s, Vd.maxstep, Vd.snap, Vd.voxmode, st);
+    const float m = move_step<kShape>(g, Vd.hmode, s4.w, s, Vd.maxstep, Vd.snap, Vd.voxmode, st);
     if (Vd.fire) {
         const float fdt = c.fdt;
         Vel[i] = (m > 0.0f && st.ty == ty0)
@@ -1506,8 +1514,14 @@ void launch_move(cudaStream_t s, const Dev& d) {
     k_move_pre<<<nblk(d.N, kMoveThreads), kMoveThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.F, d.Vel, d.typ,
                                                                 d.mv, d.pw, d.P0, d.S, d.queue, d.psum, d.rlist, d.G,
                                                                 d.N);
-    k_move_main<<<nblk(d.N, kMainThreads), kMainThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.Vel, d.typ, d.lab,
-                                                                 d.part, d.mv, d.P0, d.S, d.queue, d.rlist, d.G, d.N);
+    k_move_main<false><<<nblk(d.N, kMainThreads), kMainThreads, 0, s>>>(
+        d.vols, d.ctl, d.nodevol, d.Pq, d.Vel, d.typ, d.lab, d.part, d.mv, d.P0, d.S, d.queue, d.rlist, d.G, d.N,
+        d.shape_any);
+    if (d.shape_any) {
+        k_move_main<true><<<nblk(d.N, kMainThreads), kMainThreads, 0, s>>>(
+            d.vols, d.ctl, d.nodevol, d.Pq, d.Vel, d.typ, d.lab, d.part, d.mv, d.P0, d.S, d.queue, d.rlist, d.G, d.N,
+            d.shape_any);
+    }
 }
 
 void launch_xcount(cudaStream_t s, const DGrid& g, uint4* xbrick, int* xn, int nb) {

@@ -21,6 +21,7 @@ constexpr int kNodeAlign = kMoveThreads;
 struct Dev {
     int nvol = 0;
     int sms = 148;       // multiprocessors: the grid of the grid-stride kernels
+    int shape_any = 0;   // some volume has analytic shape fields (gm < 0)
     int64_t N = 0;       // nodes incl. per-volume padding
     int64_t KT = 0;      // bin-start entries incl. padding
     int ntile_key = 0;

@@ -33,8 +33,9 @@ struct DGrid {
     const float* phi;
     const float* hvox;
     const float* gI;
-    const float* gTW;
+    const float* gTW;       // gray: thresholds and widths; gm < 0: the analytic shape program
     int gm;
+    int64_t ntw;            // floats in gTW
     // Corner tables (built once per session): for every brick, the labels met by
     // a trilinear cell based in it (its own, its + neighbours' and, past the
     // grid's edge, label 0) and, per label, the 9x9x9 voxel values of the brick

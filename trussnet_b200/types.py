@@ -33,7 +33,7 @@ class GridView(C.Structure):
                 ("L", C.c_void_p), ("bl_cnt", C.c_void_p), ("bl_lab", C.c_void_p), ("bl_slot", C.c_void_p),
                 ("phi", C.c_void_p), ("nslots", C.c_int64), ("h", C.c_void_p),
                 ("hmin", C.c_float), ("hmax", C.c_float),
-                ("gI", C.c_void_p), ("gTW", C.c_void_p), ("gm", C.c_int32)]
+                ("gI", C.c_void_p), ("gTW", C.c_void_p), ("gm", C.c_int32), ("ngTW", C.c_int64)]
 
 
 class RelaxParamsC(C.Structure):
@@ -129,8 +129,8 @@ class Grid:
     hmin: float
     hmax: float
     gI: np.ndarray | None = None
-    gTW: np.ndarray | None = None
-    gm: int = 0
+    gTW: np.ndarray | None = None   # gray: thresholds, widths; gm < 0: the analytic shape program
+    gm: int = 0                     # gray thresholds; 0: label volume; < 0: analytic shape fields
     R: int = 6
 
     @property
@@ -163,8 +163,11 @@ class Grid:
         v.h = self.h.ctypes.data
         v.hmin, v.hmax = float(self.hmin), float(self.hmax)
         v.gI = self.gI.ctypes.data if self.gI is not None else None
+        if self.gTW is not None:
+            assert self.gTW.dtype == np.float32 and self.gTW.flags.c_contiguous
         v.gTW = self.gTW.ctypes.data if self.gTW is not None else None
         v.gm = int(self.gm)
+        v.ngTW = int(self.gTW.size) if self.gTW is not None else 0
         return v
 
     @classmethod
@@ -186,12 +189,16 @@ class Grid:
         if v.gm > 0:
             g.gI = arr(v.gI, np.float32, nv)
             g.gTW = arr(v.gTW, np.float32, 2 * v.gm)
+        elif v.gm < 0:
+            g.gTW = arr(v.gTW, np.float32, v.ngTW)
         return g
 
     def nbytes(self) -> int:
         n = sum(getattr(self, a).nbytes for a in ("L", "bl_cnt", "bl_lab", "bl_slot", "phi", "h"))
         if self.gI is not None:
-            n += self.gI.nbytes + self.gTW.nbytes
+            n += self.gI.nbytes
+        if self.gTW is not None:
+            n += self.gTW.nbytes
         return n
 
 
