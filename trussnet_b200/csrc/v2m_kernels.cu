@@ -700,18 +700,24 @@ __global__ void __launch_bounds__(256, 4) k_force(const DVol* __restrict__ vols,
     const int n = nnb[i];
     float fx = 0.0f, fy = 0.0f, fz = 0.0f, fa = 0.0f;
     const int* row = nbr + i;
-    // loads in batches of kForceBatch (ids, then positions) so that many gathers
-    // are in flight per thread; the bars are still added one by one in list order
-    for (int k0 = 0; k0 < n; k0 += kForceBatch) {
-        int jj[kForceBatch];
+    // every id first (one round trip: the slot-major rows are coalesced), then
+    // the positions in batches of kForceBatch, so that a node's dependent chain
+    // is 1 + ceil(nnb / 4) memory round trips rather than 2 ceil(nnb / 4); the
+    // bars are still added one by one in list order
+    int jj[V2M_K];
+#pragma unroll
+    for (int k = 0; k < V2M_K; ++k) {
+        jj[k] = k < n ? __ldg(row + (int64_t)k * N) : (int)i;
+    }
+#pragma unroll
+    for (int k0 = 0; k0 < V2M_K; k0 += kForceBatch) {
+        if (k0 >= n) {
+            break;
+        }
         float4 qq[kForceBatch];
 #pragma unroll
         for (int u = 0; u < kForceBatch; ++u) {
-            jj[u] = k0 + u < n ? __ldg(row + (int64_t)(k0 + u) * N) : (int)i;
-        }
-#pragma unroll
-        for (int u = 0; u < kForceBatch; ++u) {
-            qq[u] = __ldg(Pq + jj[u]);
+            qq[u] = __ldg(Pq + (k0 + u < V2M_K ? jj[k0 + u] : (int)i));
         }
 #pragma unroll
         for (int u = 0; u < kForceBatch; ++u) {
