@@ -68,6 +68,7 @@ typedef struct {
                                     else NULL */
     int32_t gm;                  /* number of gray thresholds; 0 = label volume; < 0 = analytic shape fields */
     int64_t ngTW;                /* floats in gTW (tn::Grid::gTW.size()); 0 = 2 gm (gray-scale) */
+    const uint8_t* grade;        /* nx*ny*nz size grades (tn::Grid::grade): seeding only, may be NULL */
 } v2m_grid_view;
 
 /*
@@ -127,6 +128,23 @@ int v2m_cuda_device_count(void);
  */
 int v2m_relax_cuda(const v2m_grid_view* g, const v2m_relax_params* prm, v2m_nodes_view* nd, v2m_relax_stats* st,
                    int device);
+
+/*
+ * Seeding on CUDA device `device` (-1 = device 0): tn::seed_cpu
+ * (src/v2m_particles.cpp:625-726) without its shape-feature pass -- the graded
+ * HCP lattice of the grid's size grades (g->grade is required), each node
+ * classified onto its interface or junction curve, the junction-line seeds
+ * (params->jseed > 0) with the lattice nodes near them dropped, and the CORNER
+ * nodes (params->corners), in the reference's order and bit for bit. Uses
+ * nseed, jseed, corners and voxel_trap of the parameters. *n receives the node
+ * count and *out a result to copy out (v2m_seed_copy: P 3n floats, lab n,
+ * typ n, part 2n, part3 n or NULL) and free (v2m_seed_free).
+ */
+typedef struct v2m_seed_result v2m_seed_result;
+int v2m_seed_cuda(const v2m_grid_view* g, const v2m_relax_params* prm, int device, v2m_seed_result** out,
+                  int64_t* n);
+int v2m_seed_copy(const v2m_seed_result* r, float* P, uint16_t* lab, uint8_t* typ, uint16_t* part, uint16_t* part3);
+void v2m_seed_free(v2m_seed_result* r);
 
 /*
  * Many independent volumes in one set of launches (one per stage for all of

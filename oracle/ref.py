@@ -56,6 +56,7 @@ class RefLib:
         L.ref_seed.argtypes = [vp, vp, C.POINTER(C.c_int64)]
         L.ref_seed_copy.argtypes = [vp, vp, vp, vp, vp]
         L.ref_seed_free.argtypes = [vp]
+        L.ref_seed_part3.argtypes = [vp, vp]
         L.ref_state_create.restype = vp
         L.ref_state_create.argtypes = [C.POINTER(GridView), vp, C.POINTER(NodesView)]
         L.ref_state_free.argtypes = [vp]
@@ -138,6 +139,8 @@ class RefLib:
             nd = Nodes(P=np.zeros((n, 3), np.float32), lab=np.zeros(n, np.uint16), typ=np.zeros(n, np.uint8),
                        part=np.zeros((n, 2), np.uint16))
             self.L.ref_seed_copy(sh, nd.P.ctypes.data, nd.lab.ctypes.data, nd.typ.ctypes.data, nd.part.ctypes.data)
+            nd.part3 = np.zeros(n, np.uint16)   # (a CORNER node's fourth label)
+            self.L.ref_seed_part3(sh, nd.part3.ctypes.data)
             self.L.ref_seed_free(sh)
         finally:
             self.L.ref_grid_free(h)

@@ -346,6 +346,7 @@ int ref_grid_view(void* h, v2m_grid_view* v) {
     v->gTW = g.gTW.empty() ? nullptr : g.gTW.data();
     v->gm = g.gm;
     v->ngTW = static_cast<int64_t>(g.gTW.size());
+    v->grade = g.grade.empty() ? nullptr : g.grade.data();
     return 0;
 }
 
@@ -373,6 +374,13 @@ int ref_seed_copy(void* h, float* P, uint16_t* lab, uint8_t* typ, uint16_t* part
     std::memcpy(lab, nd->lab.data(), nd->lab.size() * 2);
     std::memcpy(typ, nd->typ.data(), nd->typ.size());
     std::memcpy(part, nd->part.data(), nd->part.size() * 2);
+    return 0;
+}
+
+// The seeds' third partner labels (part3: a CORNER node's fourth label).
+int ref_seed_part3(void* h, uint16_t* part3) {
+    tn::Nodes* nd = static_cast<tn::Nodes*>(h);
+    std::memcpy(part3, nd->part3.data(), nd->part3.size() * 2);
     return 0;
 }
 

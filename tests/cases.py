@@ -163,3 +163,43 @@ def shape_opcodes(prog: np.ndarray):
             else:
                 pc += 1
     return prims, ops
+
+
+# ---- seeding --------------------------------------------------------------------------
+def phantom_labels(dim=40):
+    """Three nested spheres with a slab cut (the ref_phantom volume)."""
+    c = (dim - 1) / 2.0
+    z, y, x = np.mgrid[0:dim, 0:dim, 0:dim].astype(np.float32)
+    r = np.sqrt((x - c) ** 2 + (y - c) ** 2 + (z - c) ** 2)
+    L = np.zeros((dim, dim, dim), np.uint16)
+    L[r < 0.45 * dim] = 1
+    L[r < 0.32 * dim] = 2
+    L[(r < 0.45 * dim) & (x > c + 3)] = 3
+    L[r < 0.15 * dim] = 4
+    return L
+
+
+def noise_labels(dim=36, nlab=5, seed=3):
+    """argmax of smoothed seeded noise fields inside a ball: many junction lines
+    and 4-label corners."""
+    rng = np.random.default_rng(seed)
+    f = rng.standard_normal((nlab, dim, dim, dim)).astype(np.float32)
+    for _ in range(3):   # cheap smoothing: box filters along each axis
+        for ax in (1, 2, 3):
+            f = (np.roll(f, 1, ax) + f + np.roll(f, -1, ax)) / 3.0
+    L = (np.argmax(f, axis=0) + 1).astype(np.uint16)
+    c = (dim - 1) / 2.0
+    z, y, x = np.mgrid[0:dim, 0:dim, 0:dim].astype(np.float32)
+    L[np.sqrt((x - c) ** 2 + (y - c) ** 2 + (z - c) ** 2) > 0.46 * dim] = 0
+    return L
+
+
+def seed_case(ref, name, prm):
+    """A reference-built grid (with its size grades) and the reference's own
+    seed_cpu on it for params prm (the seeds carry part3)."""
+    if name == "phantom":
+        return ref.build_and_seed(phantom_labels(), sigma=1.0, hbase=2.5, hmin=1.5, hmax=3.0, prm=prm)
+    if name == "noise":
+        return ref.build_and_seed(noise_labels(), sigma=1.0, hbase=2.0, hmin=1.2, hmax=3.0, prm=prm)
+    scene, kw = SHAPE_SCENES[name]
+    return ref.shape_and_seed(scene, voxel=1.0, hbase=2.5, hmin=1.5, hmax=3.5, prm=prm, **kw)

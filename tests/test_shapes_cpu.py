@@ -72,3 +72,25 @@ def test_oracle_restatement_declines_shapes():
     g, nd = shape_grid(sphere_program((16.0, 16.0, 16.0), 10.0))
     with pytest.raises(Exception):
         Oracle("f32").relax(g, RelaxParams(max_iters=1), nd)
+
+
+def test_seed_checked_before_any_device():
+    from trussnet_b200 import seed_cl
+    g, _ = cases.sphere_small()            # (synthetic grids carry no size grades)
+    assert g.grade is None
+    with pytest.raises(V2mError) as e:
+        seed_cl(g, RelaxParams())
+    assert e.value.code == _lib.V2M_ERR_ARG and "grade" in str(e.value)
+    g2 = type(g)(**{**g.__dict__, "grade": np.zeros((g.nz, g.ny, g.nx), np.uint8)})
+    with pytest.raises(V2mError) as e:
+        seed_cl(g2, RelaxParams(nseed=0))
+    assert e.value.code == _lib.V2M_ERR_ARG and "nseed" in str(e.value)
+
+
+def test_seed_cases_build(ref):
+    """The seeding cases' reference seeds: every node type present."""
+    for name, types in (("phantom", {0, 1, 2}), ("noise", {0, 1, 2, 3})):
+        g, nd = cases.seed_case(ref, name, RelaxParams())
+        assert g.grade is not None and g.grade.shape == (g.nz, g.ny, g.nx)
+        assert set(np.unique(nd.typ)) == types, name
+        assert nd.part3.shape == (nd.size(),)

@@ -27,6 +27,7 @@ EXPORTS = [
     "v2m_unroll_loss", "v2m_unroll_loss_backward", "v2m_unroll_backward", "v2m_unroll_tape", "v2m_unroll_timing",
     "v2m_unroll_last_error", "v2m_session_autotune", "v2m_session_shapes",
     "v2m_session_profile_stages", "v2m_session_queue_sizes", "v2m_bin_sort_noalloc", "v2m_bin_sort_noalloc_error",
+    "v2m_seed_cuda", "v2m_seed_copy", "v2m_seed_free",
 ]
 
 _lock = threading.Lock()
@@ -79,6 +80,10 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.v2m_session_queue_sizes.argtypes = [vp, P(C.c_int32), P(C.c_int32)]
         L.v2m_bin_sort_noalloc.argtypes = [vp, C.c_int64, C.c_int64, vp, vp, vp]
         L.v2m_bin_sort_noalloc_error.restype = C.c_char_p
+        L.v2m_seed_cuda.argtypes = [P(GridView), P(RelaxParamsC), C.c_int, P(vp), P(C.c_int64)]
+        L.v2m_seed_copy.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.v2m_seed_free.argtypes = [vp]
+        L.v2m_seed_free.restype = None
         L.v2m_unroll_create.argtypes = [C.c_int64, vp, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_int,
                                         C.c_int, C.c_int, P(vp)]
         L.v2m_unroll_destroy.argtypes = [vp]

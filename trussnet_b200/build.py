@@ -25,8 +25,8 @@ REF = "/root/reference"
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "--fmad=false", "-prec-div=true",
               "-prec-sqrt=true", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
-SOURCES = ["v2m_kernels.cu", "v2m_host.cu", "v2m_adjoint.cu", "v2m_noalloc.cu"]
-HEADERS = ["v2m_kernels.h", "v2m_types.cuh", "v2m_field.cuh"]
+SOURCES = ["v2m_kernels.cu", "v2m_host.cu", "v2m_adjoint.cu", "v2m_noalloc.cu", "v2m_seed.cu"]
+HEADERS = ["v2m_kernels.h", "v2m_types.cuh", "v2m_field.cuh", "v2m_sdf.cuh"]
 
 
 def nvcc() -> str:

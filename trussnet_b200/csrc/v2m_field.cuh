@@ -21,6 +21,8 @@
 #include "v2m_types.cuh"
 
 namespace v2m {
+// (internal linkage: the header is compiled into more than one source)
+namespace {
 
 // ---- grid lookups ---------------------------------------------------------------
 __device__ __forceinline__ int label_at(const DGrid& g, int i, int j, int k) {
@@ -1308,4 +1310,5 @@ __device__ __noinline__ float move_step(const DGrid& g, int hmode, float h, floa
     return mv / h;
 }
 
+}  // namespace
 }  // namespace v2m

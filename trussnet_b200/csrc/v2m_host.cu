@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <sys/stat.h>
 #include <stdexcept>
@@ -302,6 +303,46 @@ void build_corner_tables(v2m_session* s, DGrid& g, size_t nb) {
     g.xphi = xphi;
 }
 
+// One volume's fields on the device: the caller's arrays uploaded, and the
+// corner tables built from them.
+DGrid upload_grid(v2m_session* s, const v2m_grid_view* g) {
+    DGrid G;
+    std::memset(&G, 0, sizeof(G));
+    const size_t nvox = (size_t)g->nx * g->ny * g->nz;
+    const size_t nb = (size_t)g->nbx * g->nby * g->nbz;
+    G.nx = g->nx;
+    G.ny = g->ny;
+    G.nz = g->nz;
+    G.nbx = g->nbx;
+    G.nby = g->nby;
+    G.nbz = g->nbz;
+    G.vx = g->vs[0];
+    G.vy = g->vs[1];
+    G.vz = g->vs[2];
+    G.L = upload(s, g->L, nvox);
+    G.bl_cnt = upload(s, g->bl_cnt, nb);
+    G.bl_lab = upload(s, g->bl_lab, nb * V2M_BL);
+    G.bl_slot = upload(s, g->bl_slot, nb);
+    G.phi = upload(s, g->phi, (size_t)g->nslots * V2M_SLOT);
+    G.hvox = upload(s, g->h, nvox);
+    G.gm = g->gm;
+    if (g->gm > 0) {
+        G.gI = upload(s, g->gI, nvox);
+        G.gTW = upload(s, g->gTW, 2 * (size_t)g->gm);
+        G.ntw = 2 * (int64_t)g->gm;
+    } else if (g->gm < 0) {
+        G.gI = nullptr;
+        G.gTW = upload(s, g->gTW, (size_t)g->ngTW);
+        G.ntw = g->ngTW;
+    } else {
+        G.gI = nullptr;
+        G.gTW = s->alloc<float>(4);
+        G.ntw = 0;
+    }
+    build_corner_tables(s, G, nb);
+    return G;
+}
+
 void init_ctl(v2m_session* s) {
     std::vector<VolCtl> c(s->nvol);
     for (int v = 0; v < s->nvol; ++v) {
@@ -451,38 +492,7 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
             const v2m_grid_view* g = gv + v;
             const v2m_relax_params* p = pv + v;
             DVol& V = s->hvols[v];
-            const size_t nvox = (size_t)g->nx * g->ny * g->nz;
-            const size_t nb = (size_t)g->nbx * g->nby * g->nbz;
-            V.g.nx = g->nx;
-            V.g.ny = g->ny;
-            V.g.nz = g->nz;
-            V.g.nbx = g->nbx;
-            V.g.nby = g->nby;
-            V.g.nbz = g->nbz;
-            V.g.vx = g->vs[0];
-            V.g.vy = g->vs[1];
-            V.g.vz = g->vs[2];
-            V.g.L = upload(s, g->L, nvox);
-            V.g.bl_cnt = upload(s, g->bl_cnt, nb);
-            V.g.bl_lab = upload(s, g->bl_lab, nb * V2M_BL);
-            V.g.bl_slot = upload(s, g->bl_slot, nb);
-            V.g.phi = upload(s, g->phi, (size_t)g->nslots * V2M_SLOT);
-            V.g.hvox = upload(s, g->h, nvox);
-            V.g.gm = g->gm;
-            if (g->gm > 0) {
-                V.g.gI = upload(s, g->gI, nvox);
-                V.g.gTW = upload(s, g->gTW, 2 * (size_t)g->gm);
-                V.g.ntw = 2 * (int64_t)g->gm;
-            } else if (g->gm < 0) {
-                V.g.gI = nullptr;
-                V.g.gTW = upload(s, g->gTW, (size_t)g->ngTW);
-                V.g.ntw = g->ngTW;
-            } else {
-                V.g.gI = nullptr;
-                V.g.gTW = s->alloc<float>(4);
-                V.g.ntw = 0;
-            }
-            build_corner_tables(s, V.g, nb);
+            V.g = upload_grid(s, g);
             V.nofs = I.nofs;
             V.n = I.n;
             V.kofs = I.kofs;
@@ -783,7 +793,21 @@ int guard(F&& f) {
     }
 }
 
+// tn::seed_cpu's spacing of seed level L (src/opencl/v2m_seed_body.cl:441-443),
+// with the same float operations and the host's float pow
+float seed_spacing(int L, int nseed, float hmin, float hmax) {
+    return nseed <= 1 ? hmin : hmin * std::pow(hmax / hmin, (float)L / (float)(nseed - 1));
+}
+
 }  // namespace
+
+// Seeds made on the device, held on the host until copied out.
+struct v2m_seed_result {
+    std::vector<float> P;
+    std::vector<uint16_t> lab;
+    std::vector<uint8_t> typ;
+    std::vector<uint16_t> part, part3;
+};
 
 extern "C" {
 
@@ -1392,6 +1416,115 @@ int v2m_session_clear_counters(v2m_session* s) {
         s->force_launches = 0;
         s->force_ms = 0.0;
     });
+}
+
+int v2m_seed_cuda(const v2m_grid_view* g, const v2m_relax_params* prm, int device, v2m_seed_result** out,
+                  int64_t* n) {
+    return guard([&] {
+        if (!out || !n) {
+            throw ArgError("null argument");
+        }
+        *out = nullptr;
+        *n = 0;
+        v2m_nodes_view none{};
+        validate(g, prm, &none);
+        if (!g->grade) {
+            throw ArgError("seeding needs the grid's size grades (grade)");
+        }
+        if (prm->nseed < 1 || prm->nseed > 256) {
+            throw ArgError("nseed must be in [1, 256]");
+        }
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+            cudaGetLastError();
+            throw CudaError("no CUDA device available");
+        }
+        const int dev = device < 0 ? 0 : device;
+        if (dev >= ndev) {
+            throw ArgError("device index out of range");
+        }
+        ck(cudaSetDevice(dev), "cudaSetDevice");
+        v2m_session tmp;   // (an allocation context: the grid's device copy)
+        tmp.device = dev;
+        ck(cudaStreamCreateWithFlags(&tmp.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        SeedArgs A;
+        A.g = upload_grid(&tmp, g);
+        const size_t nvox = (size_t)g->nx * g->ny * g->nz;
+        A.grade = upload(&tmp, g->grade, nvox);
+        std::vector<float> sp(prm->nseed);
+        for (int L = 0; L < prm->nseed; ++L) {
+            sp[L] = seed_spacing(L, prm->nseed, g->hmin, g->hmax);
+        }
+        A.spacing = upload(&tmp, sp.data(), sp.size());
+        A.nseed = prm->nseed;
+        A.voxmode = prm->voxel_trap ? 1 : 0;
+        A.jseed = prm->jseed;
+        A.corners = prm->corners ? 1 : 0;
+        A.hmax = g->hmax;
+        cudaDeviceGetAttribute(&A.sms, cudaDevAttrMultiProcessorCount, dev);
+        A.stream = tmp.stream;
+        SeedBuffers B;
+        std::string err;
+        const cudaError_t e = seed_run(A, B, err);
+        auto release = [&] {
+            cudaStreamSynchronize(tmp.stream);
+            for (void* p : B.tmp) {
+                cudaFree(p);
+            }
+            B.tmp.clear();
+        };
+        if (e != cudaSuccess) {
+            release();
+            cudaGetLastError();
+            if (!err.empty()) {
+                throw ArgError("seeding: " + err);
+            }
+            throw CudaError(std::string("seeding: ") + cudaGetErrorString(e));
+        }
+        std::unique_ptr<v2m_seed_result> r(new v2m_seed_result());
+        const size_t m = (size_t)B.n;
+        r->P.resize(3 * m);
+        r->lab.resize(m);
+        r->typ.resize(m);
+        r->part.resize(2 * m);
+        r->part3.resize(m);
+        if (m) {
+            ck(cudaMemcpyAsync(r->P.data(), B.P, 12 * m, cudaMemcpyDeviceToHost, tmp.stream), "seeds");
+            ck(cudaMemcpyAsync(r->lab.data(), B.lab, 2 * m, cudaMemcpyDeviceToHost, tmp.stream), "seeds");
+            ck(cudaMemcpyAsync(r->typ.data(), B.typ, m, cudaMemcpyDeviceToHost, tmp.stream), "seeds");
+            ck(cudaMemcpyAsync(r->part.data(), B.part, 4 * m, cudaMemcpyDeviceToHost, tmp.stream), "seeds");
+            ck(cudaMemcpyAsync(r->part3.data(), B.part3, 2 * m, cudaMemcpyDeviceToHost, tmp.stream), "seeds");
+        }
+        release();
+        ck(cudaGetLastError(), "seeding");
+        *n = (int64_t)m;
+        *out = r.release();
+    });
+}
+
+int v2m_seed_copy(const v2m_seed_result* r, float* P, uint16_t* lab, uint8_t* typ, uint16_t* part, uint16_t* part3) {
+    return guard([&] {
+        if (!r) {
+            throw ArgError("null argument");
+        }
+        const size_t m = r->lab.size();
+        if (m && (!P || !lab || !typ || !part)) {
+            throw ArgError("null output array");
+        }
+        if (m) {
+            std::memcpy(P, r->P.data(), 12 * m);
+            std::memcpy(lab, r->lab.data(), 2 * m);
+            std::memcpy(typ, r->typ.data(), m);
+            std::memcpy(part, r->part.data(), 4 * m);
+            if (part3) {
+                std::memcpy(part3, r->part3.data(), 2 * m);
+            }
+        }
+    });
+}
+
+void v2m_seed_free(v2m_seed_result* r) {
+    delete r;
 }
 
 int v2m_relax_cuda(const v2m_grid_view* g, const v2m_relax_params* prm, v2m_nodes_view* nd, v2m_relax_stats* st,

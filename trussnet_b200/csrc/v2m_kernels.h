@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <string>
+#include <vector>
 
 #include "v2m_types.cuh"
 
@@ -78,5 +80,34 @@ void launch_float4_to3(cudaStream_t s, const float4* a, int64_t nofs, int n, flo
 void launch_float3_to4(cudaStream_t s, const float* in, int64_t nofs, int n, float4* a);
 void launch_local_ids(cudaStream_t s, const int* a, int64_t nofs, int n, int* out);
 void launch_local_cstart(cudaStream_t s, const int* a, int64_t kofs, int cnt, int64_t nofs, int* out);
+
+// Seeding on the device (v2m_seed.cu): one grid, its size grades and the
+// seed-level spacings (computed on the host with the reference's float pow).
+struct SeedArgs {
+    DGrid g;
+    const uint8_t* grade = nullptr;
+    const float* spacing = nullptr;   // per seed level
+    int nseed = 1;
+    int voxmode = 0;
+    float jseed = 0.0f;
+    int corners = 1;
+    float hmax = 0.0f;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+};
+
+// The seeds (device arrays in `tmp`, freed by the caller): n nodes, P xyz, lab,
+// typ, part pairs and part3 in tn::Nodes' layout.
+struct SeedBuffers {
+    std::vector<void*> tmp;
+    float* P = nullptr;
+    uint16_t* lab = nullptr;
+    uint8_t* typ = nullptr;
+    uint16_t* part = nullptr;
+    uint16_t* part3 = nullptr;
+    int n = 0;
+};
+
+cudaError_t seed_run(const SeedArgs& A, SeedBuffers& B, std::string& err);
 
 }  // namespace v2m

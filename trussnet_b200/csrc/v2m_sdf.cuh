@@ -23,6 +23,8 @@
 #include "v2m_types.cuh"
 
 namespace v2m {
+// (internal linkage: the header is compiled into more than one source)
+namespace {
 
 enum SdfOp : int {
     kSdfEnd = 0,
@@ -421,4 +423,5 @@ __device__ __forceinline__ float sdf_psi(const DGrid& g, int a, int b, float px,
     return (sa.v - sb.v) / w;
 }
 
+}  // namespace
 }  // namespace v2m

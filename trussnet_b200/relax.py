@@ -9,6 +9,9 @@
       (src/v2m_pipeline.cpp:492-526).
   relax_cl_batch(grids, prms, nodes, device=-1)
       many independent volumes in one set of launches (no reference counterpart).
+  seed_cl(g, prm, device=-1)
+      tn::seed_cpu (src/v2m_particles.cpp:625-726) on a CUDA device, without its
+      shape-feature pass: the seeds as Nodes, and their part3 labels.
   Session
       the relaxation state kept on the device: the stages one at a time, repeated
       runs from the same seeds, internal arrays for checks.
@@ -65,6 +68,28 @@ def relax_cl_batch(grids: Sequence[Grid], prms: Sequence[RelaxParams], nodes: Se
     sv = (RelaxStatsC * len(grids))()
     _lib.check(L.v2m_relax_cuda_batch(len(grids), gv, pv, nv, sv, device))
     return [RelaxStats.from_c(s) for s in sv]
+
+
+def seed_cl(g: Grid, prm: RelaxParams, device: int = -1) -> tuple[Nodes, np.ndarray]:
+    """Seed grid g on a CUDA device (g.grade is required): the nodes of
+    tn::seed_cpu in its order (the shape-feature nodes excepted), and part3 (a
+    CORNER node's fourth label, else V2M_NOLAB)."""
+    L = _lib.load()
+    gv = g.view()
+    pv = prm.to_c()
+    h = C.c_void_p()
+    n = C.c_int64()
+    _lib.check(L.v2m_seed_cuda(C.byref(gv), C.byref(pv), device, C.byref(h), C.byref(n)))
+    try:
+        m = n.value
+        nd = Nodes(P=np.zeros((m, 3), np.float32), lab=np.zeros(m, np.uint16), typ=np.zeros(m, np.uint8),
+                   part=np.zeros((m, 2), np.uint16))
+        part3 = np.zeros(m, np.uint16)
+        _lib.check(L.v2m_seed_copy(h, nd.P.ctypes.data, nd.lab.ctypes.data, nd.typ.ctypes.data, nd.part.ctypes.data,
+                                   part3.ctypes.data))
+    finally:
+        L.v2m_seed_free(h)
+    return nd, part3
 
 
 class Session:

@@ -33,7 +33,8 @@ class GridView(C.Structure):
                 ("L", C.c_void_p), ("bl_cnt", C.c_void_p), ("bl_lab", C.c_void_p), ("bl_slot", C.c_void_p),
                 ("phi", C.c_void_p), ("nslots", C.c_int64), ("h", C.c_void_p),
                 ("hmin", C.c_float), ("hmax", C.c_float),
-                ("gI", C.c_void_p), ("gTW", C.c_void_p), ("gm", C.c_int32), ("ngTW", C.c_int64)]
+                ("gI", C.c_void_p), ("gTW", C.c_void_p), ("gm", C.c_int32), ("ngTW", C.c_int64),
+                ("grade", C.c_void_p)]
 
 
 class RelaxParamsC(C.Structure):
@@ -132,6 +133,7 @@ class Grid:
     gTW: np.ndarray | None = None   # gray: thresholds, widths; gm < 0: the analytic shape program
     gm: int = 0                     # gray thresholds; 0: label volume; < 0: analytic shape fields
     R: int = 6
+    grade: np.ndarray | None = None  # uint8 [nz, ny, nx] size grades (seeding only)
 
     @property
     def nbx(self):
@@ -168,6 +170,10 @@ class Grid:
         v.gTW = self.gTW.ctypes.data if self.gTW is not None else None
         v.gm = int(self.gm)
         v.ngTW = int(self.gTW.size) if self.gTW is not None else 0
+        if self.grade is not None:
+            assert self.grade.dtype == np.uint8 and self.grade.flags.c_contiguous
+            assert self.grade.size == self.nx * self.ny * self.nz
+        v.grade = self.grade.ctypes.data if self.grade is not None else None
         return v
 
     @classmethod
@@ -191,6 +197,8 @@ class Grid:
             g.gTW = arr(v.gTW, np.float32, 2 * v.gm)
         elif v.gm < 0:
             g.gTW = arr(v.gTW, np.float32, v.ngTW)
+        if v.grade:
+            g.grade = arr(v.grade, np.uint8, nv).reshape(v.nz, v.ny, v.nx)
         return g
 
     def nbytes(self) -> int:
