@@ -11,6 +11,7 @@ trigger. One step = one whole relaxation from the seeds (first list build +
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
   python bench.py --workload batch64   (the batched form against sequential runs)
   python bench.py --workload adjoint   (the unroll's backward against its forward)
+  python bench.py --workload seed_tpm182   (seeding on the device against seed_cpu)
 
 --workload batch64: 64 independent volumes of seeded sizes 32^3..160^3 with
 2..18 nested-shell labels (~4M nodes in all), 200 FIRE iterations each. One
@@ -343,6 +344,65 @@ def run_adjoint(args):
     print(json.dumps(line), flush=True)
 
 
+def run_seed(args):
+    """Seeding of the tpm182 grid (182x218x182, argmax of six smoothed noise
+    fields: interfaces, junction lines and 4-label corners everywhere; h = 1.3)
+    with the reference's default parameters (8 seed levels, junction-line seeds,
+    corners):
+    seeds per second through seed_cl, a whole call from host arrays (grid upload,
+    corner tables, the seeding stages, the copy back), against the reference's
+    seed_cpu on the same grid, whose result it must equal bit for bit."""
+    world, rank, local = dist_setup(args)
+    if rank != 0:
+        return
+    import torch
+    from trussnet_b200 import seed_cl, synth
+    from trussnet_b200.types import RelaxParams
+    torch.cuda.set_device(local)
+    g, _ = synth.tpm()
+    g.grade = synth.size_grades(g.h, g.hmin, g.hmax)
+    prm = RelaxParams()
+    for _ in range(args.warmup):
+        nd, p3 = seed_cl(g, prm, device=local)
+    ts = []
+    clk = ClockSampler(local)
+    clk.start()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        nd, p3 = seed_cl(g, prm, device=local)
+        ts.append(time.perf_counter() - t0)
+    clocks = clk.stop()
+    dt = statistics.mean(ts)
+    n = nd.size()
+    h2d = g.nbytes() + g.grade.nbytes
+    d2h = n * (12 + 2 + 1 + 4 + 2)
+    cb, same = None, None
+    if not args.no_cpu_baseline:
+        from oracle.ref import RefLib, available
+        if available():
+            lib = RefLib()
+            t0 = time.perf_counter()
+            rnd = lib.seed(g, prm)
+            tc = time.perf_counter() - t0
+            same = bool(rnd.size() == n and all(np.array_equal(getattr(rnd, a), getattr(nd, a))
+                                                for a in ("P", "lab", "typ", "part")) and np.array_equal(rnd.part3, p3))
+            cores = os.cpu_count() or 1
+            cap = int(os.environ.get("V2M_OMP_MAX_THREADS", "64"))
+            cores = min(cores, cap) if cap > 0 else cores
+            cb = {"value": rnd.size() / tc, "unit": "seeds/s", "cores": cores, "kind": "reference",
+                  "sample": f"seed_cpu on the same grid, one whole seeding, {tc:.2f} s"}
+    line = {"metric": "seeding seeds/s", "value": n / dt, "unit": "seeds/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "seed_tpm182: the tpm182 grid (182x218x182, argmax of 6 smoothed noise fields, "
+                                   "h = 1.3), nseed 8, jseed 0.8, corners on", "nodes": n,
+                       "types": np.bincount(nd.typ, minlength=4).tolist(), "timed": "whole seed_cl calls from host "
+                       "arrays (upload, corner tables, seeding, copy back)"},
+            "e2e": {"value": n / dt, "unit": "seeds/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "cpu_baseline": cb, "results_identical": same, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
 def run_cuda(args):
     import torch
     world, rank, local = dist_setup(args)
@@ -464,6 +524,8 @@ def main():
         run_batch(args)
     elif args.workload == "adjoint":
         run_adjoint(args)
+    elif args.workload == "seed_tpm182":
+        run_seed(args)
     else:
         run_cuda(args)
 

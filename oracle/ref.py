@@ -57,6 +57,8 @@ class RefLib:
         L.ref_seed_copy.argtypes = [vp, vp, vp, vp, vp]
         L.ref_seed_free.argtypes = [vp]
         L.ref_seed_part3.argtypes = [vp, vp]
+        L.ref_seed_view.restype = vp
+        L.ref_seed_view.argtypes = [C.POINTER(GridView), vp, C.POINTER(C.c_int64)]
         L.ref_state_create.restype = vp
         L.ref_state_create.argtypes = [C.POINTER(GridView), vp, C.POINTER(NodesView)]
         L.ref_state_free.argtypes = [vp]
@@ -99,8 +101,22 @@ class RefLib:
         return g
 
     def seed(self, g: Grid, prm: RelaxParams) -> Nodes:
-        """tn::seed_cpu on a reference-built grid (needs its grade field: rebuilt here)."""
-        raise NotImplementedError
+        """tn::seed_cpu on grid g (g.grade required); the nodes carry part3."""
+        gv, pv = g.view(), prm.to_c()
+        n = C.c_int64()
+        sh = self.L.ref_seed_view(C.byref(gv), C.byref(pv), C.byref(n))
+        if not sh:
+            raise RuntimeError(self.err())
+        try:
+            m = n.value
+            nd = Nodes(P=np.zeros((m, 3), np.float32), lab=np.zeros(m, np.uint16), typ=np.zeros(m, np.uint8),
+                       part=np.zeros((m, 2), np.uint16))
+            self.L.ref_seed_copy(sh, nd.P.ctypes.data, nd.lab.ctypes.data, nd.typ.ctypes.data, nd.part.ctypes.data)
+            nd.part3 = np.zeros(m, np.uint16)
+            self.L.ref_seed_part3(sh, nd.part3.ctypes.data)
+        finally:
+            self.L.ref_seed_free(sh)
+        return nd
 
     def build_and_seed(self, L, vs=(1.0, 1.0, 1.0), sigma=1.0, hbase=0.0, hmin=0.0, hmax=0.0,
                        prm: RelaxParams | None = None):

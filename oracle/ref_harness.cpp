@@ -115,6 +115,9 @@ void grid_from_view(const v2m_grid_view* v, OwnedGrid& o) {
         g.gI = nullptr;
         g.gTW.assign(1, 0.0f);
     }
+    if (v->grade) {
+        g.grade.assign(v->grade, v->grade + nv);
+    }
 }
 
 tn::RelaxParams params_from(const v2m_relax_params* p) {
@@ -375,6 +378,25 @@ int ref_seed_copy(void* h, float* P, uint16_t* lab, uint8_t* typ, uint16_t* part
     std::memcpy(typ, nd->typ.data(), nd->typ.size());
     std::memcpy(part, nd->part.data(), nd->part.size() * 2);
     return 0;
+}
+
+// seed_cpu on a grid given as a view (its grade array required); a handle for
+// ref_seed_copy / ref_seed_part3 / ref_seed_free.
+void* ref_seed_view(const v2m_grid_view* gv, const v2m_relax_params* pv, int64_t* n) {
+    try {
+        if (!gv->grade) {
+            throw std::runtime_error("seed_cpu needs the grid's size grades");
+        }
+        OwnedGrid og;
+        grid_from_view(gv, og);
+        tn::Nodes* nd = new tn::Nodes();
+        tn::seed_cpu(og.g, params_from(pv), *nd);
+        *n = static_cast<int64_t>(nd->size());
+        return nd;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return nullptr;
+    }
 }
 
 // The seeds' third partner labels (part3: a CORNER node's fourth label).

@@ -229,6 +229,15 @@ def shells(dim=256, nshell=6, rmin=60.0, rmax=120.0, amp=6.0, hlo=1.5, hhi=6.0, 
     return g, nd
 
 
+def size_grades(h: np.ndarray, hmin: float, hmax: float) -> np.ndarray:
+    """Per-voxel size grades (tn::Grid::grade, the seeding's input): h mapped
+    logarithmically onto 0..255 over [hmin, hmax]."""
+    if not hmax > hmin:
+        return np.zeros(h.shape, np.uint8)
+    t = np.log(np.maximum(h, hmin) / hmin) / np.log(hmax / hmin)
+    return np.clip(np.rint(255.0 * t), 0, 255).astype(np.uint8)
+
+
 def tpm(shape=(182, 218, 182), nch=6, sigma=4.0, h=1.3, density=1.0, seed=0):
     """Argmax of `nch` Gaussian-smoothed (sigma voxels) seeded noise fields (the
     labels of a tissue-probability map whose softmax at any temperature has the
