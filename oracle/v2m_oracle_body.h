@@ -29,6 +29,7 @@ typedef struct {
     const float* gI;
     const float* gTW;
     int gm;
+    int64_t ntw;            /* floats in gTW (the analytic shape program when gm < 0) */
     float hmin, hmax;
     /* parameters */
     v2m_relax_params prm;
@@ -94,7 +95,287 @@ static REAL FN(blend)(const REAL* c, REAL fx, REAL fy, REAL fz) {
     return y0 + fz * (y1 - y0);
 }
 
+/* ---- analytic shape fields, gm < 0 (src/opencl/v2m_sdf_body.cl:75-478) -------------
+ * One postfix program per label over nine primitive types, min / max with the
+ * crease blend and the gap closing, complement, sums and scales, bounding-box
+ * culling and per-brick programs; a values-only pass, then one with the
+ * gradients (central differences of each primitive) only where a min / max
+ * needs them. Every program read is bounds-checked. */
+typedef struct {
+    REAL v, x, y, z;
+} FN(sv);
+
+static REAL FN(pg)(const FN(state)* s, int64_t k) {
+    return (k >= 0 && k < s->ntw) ? (REAL)s->gTW[k] : K(0.0);
+}
+
+static int FN(sdf_np)(int t) {
+    switch (t) {
+    case 1: return 4;
+    case 2: case 4: return 6;
+    case 3: case 9: return 7;
+    case 5: case 6: case 8: return 8;
+    case 7: return 15;
+    default: return 0;
+    }
+}
+
+static REAL FN(sdf_prim)(int t, const float* q, REAL x, REAL y, REAL z) {
+    if (t == 1) { /* sphere c r */
+        REAL dx = x - q[0], dy = y - q[1], dz = z - q[2];
+        return q[3] - SQRT(dx * dx + dy * dy + dz * dz);
+    }
+    if (t == 2) { /* box lo hi */
+        REAL cx = K(0.5) * (q[0] + q[3]), cy = K(0.5) * (q[1] + q[4]), cz = K(0.5) * (q[2] + q[5]);
+        REAL ux = FABS(x - cx) - K(0.5) * FABS(q[3] - q[0]), uy = FABS(y - cy) - K(0.5) * FABS(q[4] - q[1]),
+             uz = FABS(z - cz) - K(0.5) * FABS(q[5] - q[2]);
+        REAL ox = FMAX(ux, K(0.0)), oy = FMAX(uy, K(0.0)), oz = FMAX(uz, K(0.0));
+        REAL out = SQRT(ox * ox + oy * oy + oz * oz), in = FMIN(FMAX(ux, FMAX(uy, uz)), K(0.0));
+        return -(out + in);
+    }
+    if (t == 4) return -((x - q[0]) * q[3] + (y - q[1]) * q[4] + (z - q[2]) * q[5]); /* half-space */
+    if (t == 5) { /* slab */
+        REAL tt = (x - q[0]) * q[3] + (y - q[1]) * q[4] + (z - q[2]) * q[5];
+        return FMIN(tt - q[6], q[7] - tt);
+    }
+    if (t == 9) { /* infinite cylinder */
+        REAL dx = x - q[0], dy = y - q[1], dz = z - q[2];
+        REAL tt = dx * q[3] + dy * q[4] + dz * q[5];
+        REAL rx = dx - tt * q[3], ry = dy - tt * q[4], rz = dz - tt * q[5];
+        return q[6] - SQRT(rx * rx + ry * ry + rz * rz);
+    }
+    if (t == 6) { /* torus */
+        REAL dx = x - q[0], dy = y - q[1], dz = z - q[2];
+        REAL h = dx * q[3] + dy * q[4] + dz * q[5];
+        REAL rx = dx - h * q[3], ry = dy - h * q[4], rz = dz - h * q[5];
+        REAL a = SQRT(rx * rx + ry * ry + rz * rz) - q[6];
+        return q[7] - SQRT(a * a + h * h);
+    }
+    if (t == 3) { /* capped cylinder */
+        REAL bx = q[3] - q[0], by = q[4] - q[1], bz = q[5] - q[2];
+        REAL px = x - q[0], py = y - q[1], pz = z - q[2];
+        REAL baba = bx * bx + by * by + bz * bz, paba = px * bx + py * by + pz * bz;
+        REAL ex = px * baba - bx * paba, ey = py * baba - by * paba, ez = pz * baba - bz * paba;
+        REAL u = SQRT(ex * ex + ey * ey + ez * ez) - q[6] * baba;
+        REAL v = FABS(paba - baba * K(0.5)) - baba * K(0.5);
+        REAL u2 = u * u, v2 = v * v * baba;
+        REAL dd = FMAX(u, v) < K(0.0) ? -FMIN(u2, v2) : ((u > K(0.0) ? u2 : K(0.0)) + (v > K(0.0) ? v2 : K(0.0)));
+        return -(dd < K(0.0) ? K(-1.0) : K(1.0)) * SQRT(FABS(dd)) / baba;
+    }
+    if (t == 8) { /* capped frustum */
+        REAL bx = q[3] - q[0], by = q[4] - q[1], bz = q[5] - q[2];
+        REAL px = x - q[0], py = y - q[1], pz = z - q[2];
+        REAL ra = q[6], rb = q[7];
+        REAL rba = rb - ra, baba = bx * bx + by * by + bz * bz;
+        REAL papa = px * px + py * py + pz * pz, paba = (px * bx + py * by + pz * bz) / baba;
+        REAL xr = SQRT(FMAX(papa - paba * paba * baba, K(0.0)));
+        REAL cax = FMAX(K(0.0), xr - ((paba < K(0.5)) ? ra : rb)), cay = FABS(paba - K(0.5)) - K(0.5);
+        REAL k = rba * rba + baba;
+        REAL f = FMIN(FMAX((rba * (xr - ra) + paba * baba) / k, K(0.0)), K(1.0));
+        REAL cbx = xr - ra - f * rba, cby = paba - f;
+        REAL sg = (cbx < K(0.0) && cay < K(0.0)) ? K(-1.0) : K(1.0);
+        REAL d2 = FMIN(cax * cax + cay * cay * baba, cbx * cbx + cby * cby * baba);
+        return -sg * SQRT(d2);
+    }
+    if (t == 7) { /* ellipsoid bound */
+        REAL dx = x - q[0], dy = y - q[1], dz = z - q[2];
+        REAL lx = q[6] * dx + q[7] * dy + q[8] * dz, ly = q[9] * dx + q[10] * dy + q[11] * dz,
+             lz = q[12] * dx + q[13] * dy + q[14] * dz;
+        REAL ax = lx / q[3], ay = ly / q[4], az = lz / q[5];
+        REAL bx = ax / q[3], by = ay / q[4], bz = az / q[5];
+        REAL k0 = SQRT(ax * ax + ay * ay + az * az), k1 = SQRT(bx * bx + by * by + bz * bz);
+        if (k1 < K(1e-20)) return FMIN((REAL)q[3], FMIN((REAL)q[4], (REAL)q[5]));
+        return -k0 * (k0 - K(1.0)) / k1;
+    }
+    return K(-1e30);
+}
+
+static FN(sv) FN(sdf_minmax)(FN(sv) a, FN(sv) b, REAL sgn, REAL k, REAL kgap, int grad, int* near) {
+    REAL va = sgn * a.v, vb = sgn * b.v;
+    int sliver = kgap > K(0.0) && va > -kgap && vb > -kgap && va + vb < kgap;
+    if (sliver && !grad) *near = 1;
+    REAL pen = K(0.0), dpen = K(0.0);
+    if (sliver && grad) {
+        REAL ga = SQRT(a.x * a.x + a.y * a.y + a.z * a.z), gb = SQRT(b.x * b.x + b.y * b.y + b.z * b.z);
+        if (ga > K(0.0) && gb > K(0.0)) {
+            REAL c = (a.x * b.x + a.y * b.y + a.z * b.z) / (ga * gb);
+            REAL wg = FMIN(K(1.0), FMAX(K(0.0), (-c - K(0.7)) / K(0.25)));
+            REAL u = FMAX(K(0.0), K(1.0) - (va + vb) / kgap);
+            pen = kgap * wg * u * u;
+            dpen = K(2.0) * wg * u;
+        }
+    }
+    FN(sv) r = a;
+    if (k > K(0.0) && FABS(va - vb) < k) {
+        if (!grad) {
+            *near = 1;
+        } else {
+            REAL ga = SQRT(a.x * a.x + a.y * a.y + a.z * a.z), gb = SQRT(b.x * b.x + b.y * b.y + b.z * b.z);
+            REAL c = ga > K(0.0) && gb > K(0.0) ? (a.x * b.x + a.y * b.y + a.z * b.z) / (ga * gb) : K(0.0);
+            k *= FMIN(K(1.0), FMAX(K(0.0), (K(0.995) - c) / K(0.095)));
+        }
+    }
+    if (k > K(0.0) && FABS(va - vb) < k) {
+        REAL h = K(0.5) + K(0.5) * (vb - va) / k;
+        r.v = sgn * (vb * (K(1.0) - h) + va * h - k * h * (K(1.0) - h));
+        r.x = h * a.x + (K(1.0) - h) * b.x;
+        r.y = h * a.y + (K(1.0) - h) * b.y;
+        r.z = h * a.z + (K(1.0) - h) * b.z;
+    } else if (vb < va) {
+        r = b;
+    }
+    r.v -= sgn * pen;
+    if (dpen > K(0.0)) {
+        r.x += dpen * (a.x + b.x);
+        r.y += dpen * (a.y + b.y);
+        r.z += dpen * (a.z + b.z);
+    }
+    return r;
+}
+
+static int FN(is_mm)(int op) {
+    return op == 2 || op == 3 || op == 10 || op == 11;
+}
+
+/* s_l at grid-mm point p, and (wantg) its gradient */
+static FN(sv) FN(sdf)(const FN(state)* s, int l, const REAL* p, int wantg) {
+    const FN(sv) zero = { K(0.0), K(0.0), K(0.0), K(0.0) };
+    FN(sv) none = zero;
+    none.v = K(-1e30);
+    int N = (int)FN(pg)(s, 0);
+    if (l < 0 || l >= N) return none;
+    REAL x = p[0] + FN(pg)(s, 2), y = p[1] + FN(pg)(s, 3), z = p[2] + FN(pg)(s, 4);
+    int start = (int)FN(pg)(s, 5 + l);
+    int T = (int)FN(pg)(s, 8 + N);
+    if (T > 0) {
+        int nbx = (int)FN(pg)(s, T), nby = (int)FN(pg)(s, T + 1), nbz = (int)FN(pg)(s, T + 2);
+        REAL vx = FN(pg)(s, T + 3);
+        int bi = (int)FLOOR(p[0] / vx + K(0.5)) >> 3, bj = (int)FLOOR(p[1] / vx + K(0.5)) >> 3,
+            bk = (int)FLOOR(p[2] / vx + K(0.5)) >> 3;
+        bi = bi < 0 ? 0 : (bi >= nbx ? nbx - 1 : bi);
+        bj = bj < 0 ? 0 : (bj >= nby ? nby - 1 : bj);
+        bk = bk < 0 ? 0 : (bk >= nbz ? nbz - 1 : bk);
+        int64_t e = (int64_t)T + 4 + bi + (int64_t)nbx * (bj + (int64_t)nby * bk);
+        start = (int)FN(pg)(s, (int64_t)(int)FN(pg)(s, e) + l);
+    }
+    REAL kblend = FN(pg)(s, 5 + N), kgap = FN(pg)(s, 6 + N), m = FN(pg)(s, 7 + N);
+    FN(sv) st[12];
+    int sp = 0, grad = wantg != 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        int pc = start, near = 0;
+        sp = 0;
+        for (int guard = 0; guard < 100000; ++guard) {
+            int op = (int)FN(pg)(s, pc);
+            if (op == 0) break;
+            if (FN(is_mm)(op)) {
+                if (sp > 1) {
+                    st[sp - 2] = FN(sdf_minmax)(st[sp - 2], st[sp - 1], op == 2 || op == 10 ? K(-1.0) : K(1.0), kblend,
+                                                op >= 10 ? K(0.0) : kgap, grad, &near);
+                    --sp;
+                }
+                pc += 1;
+                continue;
+            }
+            if (op == 4) {
+                if (sp > 0) {
+                    st[sp - 1].v = -st[sp - 1].v;
+                    st[sp - 1].x = -st[sp - 1].x;
+                    st[sp - 1].y = -st[sp - 1].y;
+                    st[sp - 1].z = -st[sp - 1].z;
+                }
+                pc += 1;
+                continue;
+            }
+            if (op == 8) {
+                if (sp > 1) {
+                    FN(sv) t0 = st[sp - 1], t1 = st[sp - 2];
+                    t0.v += t1.v;
+                    t0.x += t1.x;
+                    t0.y += t1.y;
+                    t0.z += t1.z;
+                    st[sp - 2] = t0;
+                    --sp;
+                }
+                pc += 1;
+                continue;
+            }
+            if (op == 9) {
+                REAL f = FN(pg)(s, pc + 1);
+                if (sp > 0) {
+                    st[sp - 1].v *= f;
+                    st[sp - 1].x *= f;
+                    st[sp - 1].y *= f;
+                    st[sp - 1].z *= f;
+                }
+                pc += 2;
+                continue;
+            }
+            FN(sv) nv = zero;
+            if (op == 1) {
+                int type = (int)FN(pg)(s, pc + 1), np = FN(sdf_np)(type);
+                if ((int64_t)pc + 2 + np > s->ntw) break;
+                const float* q = s->gTW + pc + 2;
+                REAL e = FMAX(K(1e-4) * (FABS((REAL)q[0]) + FABS((REAL)q[1]) + FABS((REAL)q[2]) + K(1.0)), K(1e-5));
+                int ne = grad ? 7 : 1;
+                REAL fv[7];
+                for (int k = 0; k < ne; ++k) {
+                    REAL dd = k == 0 ? K(0.0) : ((k & 1) ? e : -e);
+                    int ax = (k - 1) >> 1;
+                    fv[k] = FN(sdf_prim)(type, q, x + (ax == 0 ? dd : K(0.0)), y + (ax == 1 ? dd : K(0.0)),
+                                         z + (ax == 2 ? dd : K(0.0)));
+                }
+                nv.v = fv[0];
+                if (grad) {
+                    nv.x = (fv[1] - fv[2]) / (K(2.0) * e);
+                    nv.y = (fv[3] - fv[4]) / (K(2.0) * e);
+                    nv.z = (fv[5] - fv[6]) / (K(2.0) * e);
+                }
+                pc += 2 + np;
+            } else if (op == 6) {
+                if (!(x < FN(pg)(s, pc + 1) - m || y < FN(pg)(s, pc + 2) - m || z < FN(pg)(s, pc + 3) - m ||
+                      x > FN(pg)(s, pc + 4) + m || y > FN(pg)(s, pc + 5) + m || z > FN(pg)(s, pc + 6) + m)) {
+                    pc += 9;
+                    continue;
+                }
+                nv.v = FN(pg)(s, pc + 8) * m;
+                pc += 9 + (int)FN(pg)(s, pc + 7);
+            } else if (op == 7) {
+                nv.v = FN(pg)(s, pc + 1) * m;
+                pc += 2;
+            } else if (op == 5) {
+                nv.v = FN(pg)(s, pc + 1);
+                pc += 2;
+            } else {
+                break;
+            }
+            {
+                int op1 = (int)FN(pg)(s, pc), neg = op1 == 4;
+                int op2 = neg ? (int)FN(pg)(s, pc + 1) : op1;
+                if (sp > 0 && FN(is_mm)(op2)) {
+                    if (neg) {
+                        nv.v = -nv.v;
+                        nv.x = -nv.x;
+                        nv.y = -nv.y;
+                        nv.z = -nv.z;
+                    }
+                    st[sp - 1] = FN(sdf_minmax)(st[sp - 1], nv, op2 == 2 || op2 == 10 ? K(-1.0) : K(1.0), kblend,
+                                                op2 >= 10 ? K(0.0) : kgap, grad, &near);
+                    pc += 1 + neg;
+                    continue;
+                }
+            }
+            if (sp < 12) st[sp++] = nv;
+        }
+        if (grad || !near) break;
+        grad = 1;
+    }
+    return sp > 0 ? st[sp - 1] : none;
+}
+
 static REAL FN(phi_at)(const FN(state)* s, int l, const REAL* p) {
+    if (s->gm < 0) {
+        return FMIN(K(1.0), FMAX(K(0.0), K(0.5) + FN(sdf)(s, l, p, 0).v / (REAL)s->gTW[1]));
+    }
     REAL u = p[0] / s->vx, v = p[1] / s->vy, w = p[2] / s->vz;
     int i0 = (int)FLOOR(u), j0 = (int)FLOOR(v), k0 = (int)FLOOR(w);
     REAL c[8];
@@ -141,6 +422,19 @@ static REAL FN(gray)(const FN(state)* s, const REAL* p, REAL* g) {
 }
 
 static int FN(gray_psi)(const FN(state)* s, int a, int b, const REAL* p, REAL* val, REAL* g) {
+    if (s->gm < 0) { /* analytic shape fields: (s_a - s_b) / w */
+        REAL w = (REAL)s->gTW[1];
+        if (!g) {
+            *val = (FN(sdf)(s, a, p, 0).v - FN(sdf)(s, b, p, 0).v) / w;
+            return 1;
+        }
+        FN(sv) sa = FN(sdf)(s, a, p, 1), sb = FN(sdf)(s, b, p, 1);
+        g[0] = (sa.x - sb.x) / w;
+        g[1] = (sa.y - sb.y) / w;
+        g[2] = (sa.z - sb.z) / w;
+        *val = (sa.v - sb.v) / w;
+        return 1;
+    }
     if (s->gm <= 0 || (a - b != 1 && b - a != 1)) return 0;
     int k = a < b ? a : b;
     REAL sg = (a > b ? K(2.0) : K(-2.0)) / (REAL)s->gTW[s->gm + k];
@@ -167,13 +461,14 @@ static int FN(owner)(const FN(state)* s, const REAL* p, int* second) {
     int lab[V2M_BL];
     int n = FN(labels_near)(s, p, lab);
     int best = lab[0], sec = V2M_NOLAB;
-    REAL pb = K(-1.0), ps = pb;
+    REAL pb = s->gm < 0 ? K(-1e30) : K(-1.0), ps = pb;
     if (n == 1) {
         *second = V2M_NOLAB;
         return best;
     }
     for (int q = 0; q < n; ++q) {
-        REAL v = FN(phi_at)(s, lab[q], p);
+        /* (analytic fields: ranked by s itself) */
+        REAL v = s->gm < 0 ? FN(sdf)(s, lab[q], p, 0).v : FN(phi_at)(s, lab[q], p);
         if (v > pb) {
             ps = pb;
             sec = best;
@@ -273,9 +568,30 @@ static int FN(project1)(const FN(state)* s, int a, int b, REAL* p, REAL rad) {
     return FN(bisect)(s, a, b, p, u, v, rad, K(1.5) * FABS(v) / gn);
 }
 
-/* src/opencl/v2m_seed_body.cl:342-420 (sampled fields) */
+/* src/opencl/v2m_seed_body.cl:342-420 */
 static int FN(project2)(const FN(state)* s, int a, int b, int c, REAL* p, REAL rad) {
     REAL q[3] = { p[0], p[1], p[2] };
+    if (s->gm < 0) { /* the pair of constraints with the most independent gradients, pivot first */
+        REAL gab[3], gac[3], gbc[3];
+        FN(psi_grad)(s, a, b, q, gab);
+        FN(psi_grad)(s, a, c, q, gac);
+        FN(psi_grad)(s, b, c, q, gbc);
+        REAL xa[3] = { gab[1] * gac[2] - gab[2] * gac[1], gab[2] * gac[0] - gab[0] * gac[2], gab[0] * gac[1] - gab[1] * gac[0] };
+        REAL xb[3] = { gab[1] * gbc[2] - gab[2] * gbc[1], gab[2] * gbc[0] - gab[0] * gbc[2], gab[0] * gbc[1] - gab[1] * gbc[0] };
+        REAL xc[3] = { gac[1] * gbc[2] - gac[2] * gbc[1], gac[2] * gbc[0] - gac[0] * gbc[2], gac[0] * gbc[1] - gac[1] * gbc[0] };
+        REAL na = xa[0] * xa[0] + xa[1] * xa[1] + xa[2] * xa[2], nb = xb[0] * xb[0] + xb[1] * xb[1] + xb[2] * xb[2],
+             nc = xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2];
+        if (nb > na && nb >= nc) {
+            int t = a;
+            a = b;
+            b = t;
+        } else if (nc > na && nc > nb) {
+            int t = a;
+            a = c;
+            c = b;
+            b = t;
+        }
+    }
     for (int it = 0; it < 3; ++it) {
         REAL g1[3], g2[3];
         if (!FN(project1)(s, a, b, q, rad)) return 0;
@@ -815,15 +1131,13 @@ static void FN(free)(FN(state)* s) {
 }
 
 static FN(state)* FN(create)(const v2m_grid_view* g, const v2m_relax_params* p, const v2m_nodes_view* nd) {
-    /* analytic shape fields (gm < 0) are not restated here: the compiled
-       reference (oracle/_ref) is their checker */
-    if (g->gm < 0) return NULL;
     FN(state)* s = (FN(state)*)calloc(1, sizeof(FN(state)));
     if (!s) return NULL;
     s->nx = g->nx; s->ny = g->ny; s->nz = g->nz; s->nbx = g->nbx; s->nby = g->nby; s->nbz = g->nbz;
     s->vx = (REAL)g->vs[0]; s->vy = (REAL)g->vs[1]; s->vz = (REAL)g->vs[2];
     s->L = g->L; s->bl_cnt = g->bl_cnt; s->bl_lab = g->bl_lab; s->bl_slot = g->bl_slot; s->phi = g->phi;
     s->hv = g->h; s->gI = g->gI; s->gTW = g->gTW; s->gm = g->gm; s->hmin = g->hmin; s->hmax = g->hmax;
+    s->ntw = g->gm < 0 ? g->ngTW : (g->gm > 0 ? 2 * (int64_t)g->gm : 0);
     s->prm = *p;
     s->fire = p->fire && !p->voxel_trap;
     s->voxmode = p->voxel_trap != 0;

@@ -67,11 +67,30 @@ def test_shape_program_checked_before_any_device():
         assert "shape" in str(e.value) or "analytic" in str(e.value), (what, str(e.value))
 
 
-def test_oracle_restatement_declines_shapes():
+@pytest.mark.parametrize("name", list(cases.SHAPE_SCENES))
+def test_oracle_restatement_equals_reference_on_shapes(name, ref):
+    """The plain-C restatement's analytic fields (FP32) against the compiled
+    reference: 15 relaxation iterations, bit for bit."""
     from oracle.oracle import Oracle
-    g, nd = shape_grid(sphere_program((16.0, 16.0, 16.0), 10.0))
-    with pytest.raises(Exception):
-        Oracle("f32").relax(g, RelaxParams(max_iters=1), nd)
+    g, nd = cases.shape_case(ref, name)
+    prm = cases.params(15)
+    a, b = nd.copy(), nd.copy()
+    ra = ref.relax_cpu(g, prm, a)
+    rb = Oracle("f32").relax(g, prm, b)
+    for f in ("P", "typ", "part"):
+        d = cases.first_diff(getattr(b, f), getattr(a, f))
+        assert d is None, f"{f}: {d}"
+    assert (rb.iters, rb.rebuilds) == (ra.iters, ra.rebuilds)
+
+
+def test_oracle_restatement_handmade_program(ref):
+    from oracle.oracle import Oracle
+    g, nd = shape_grid(sphere_program((23.5, 23.5, 23.5), 17.6))
+    prm = cases.params(15)
+    a, b = nd.copy(), nd.copy()
+    ref.relax_cpu(g, prm, a)
+    Oracle("f32").relax(g, prm, b)
+    assert cases.first_diff(b.P, a.P) is None and cases.first_diff(b.typ, a.typ) is None
 
 
 def test_seed_checked_before_any_device():
