@@ -104,6 +104,10 @@ def test_seed_checked_before_any_device():
     with pytest.raises(V2mError) as e:
         seed_cl(g2, RelaxParams(nseed=0))
     assert e.value.code == _lib.V2M_ERR_ARG and "nseed" in str(e.value)
+    g3 = type(g2)(**{**g2.__dict__, "hmin": 0.01})   # more lattice points than int32 counts hold
+    with pytest.raises(V2mError) as e:
+        seed_cl(g3, RelaxParams())
+    assert e.value.code == _lib.V2M_ERR_ARG and "int32" in str(e.value)
 
 
 def test_seed_cases_build(ref):

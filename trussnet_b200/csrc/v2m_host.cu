@@ -1434,6 +1434,19 @@ int v2m_seed_cuda(const v2m_grid_view* g, const v2m_relax_params* prm, int devic
         if (prm->nseed < 1 || prm->nseed > 256) {
             throw ArgError("nseed must be in [1, 256]");
         }
+        {
+            // the counts and offsets are int32, as the reference's: bound the
+            // lattice points of the finest level (spacing hmin) over all voxels,
+            // and the grid vertices
+            const double s0 = seed_spacing(0, prm->nseed, g->hmin, g->hmax);
+            const double per = (g->vs[0] / s0 + 2.0) * (g->vs[1] / (0.8660254 * s0) + 2.0) *
+                               (g->vs[2] / (0.8164966 * s0) + 2.0);
+            const double nvox = (double)g->nx * g->ny * g->nz;
+            const double nvert = (double)(g->nx + 1) * (g->ny + 1) * (g->nz + 1);
+            if (!(s0 > 0.0) || per * nvox >= 2147483647.0 || nvert >= 2147483647.0) {
+                throw ArgError("seeding: the grid could hold more seeds than int32 counts allow");
+            }
+        }
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
             cudaGetLastError();
