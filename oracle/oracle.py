@@ -37,6 +37,8 @@ def load():
             getattr(L, f"orc_read_{suf}").argtypes = [vp, C.c_int, vp, C.c_int64]
             getattr(L, f"orc_write_{suf}").argtypes = [vp, C.c_int, vp, C.c_int64]
         L.orc_relax_f32.argtypes = [C.POINTER(GridView), vp, C.POINTER(NodesView), C.POINTER(RelaxStatsC)]
+        L.orc_seed_f32.restype = C.c_int64
+        L.orc_seed_f32.argtypes = [C.POINTER(GridView), vp, C.c_int64, vp, vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -63,6 +65,22 @@ class Oracle:
         if self.L.orc_relax_f32(C.byref(gv), C.byref(pv), C.byref(nv), C.byref(sv)) != 0:
             raise RuntimeError("oracle relax failed")
         return RelaxStats.from_c(sv)
+
+    def seed(self, g: Grid, prm: RelaxParams) -> Nodes:
+        """tn::seed_cpu restated (float; g.grade required); the nodes carry part3."""
+        assert self.v == "f32"
+        gv, pv = g.view(), prm.to_c()
+        n = self.L.orc_seed_f32(C.byref(gv), C.byref(pv), 0, None, None, None, None, None)
+        if n < 0:
+            raise RuntimeError("oracle seeding failed")
+        nd = Nodes(P=np.zeros((n, 3), np.float32), lab=np.zeros(n, np.uint16), typ=np.zeros(n, np.uint8),
+                   part=np.zeros((n, 2), np.uint16))
+        nd.part3 = np.zeros(n, np.uint16)
+        m = self.L.orc_seed_f32(C.byref(gv), C.byref(pv), n, nd.P.ctypes.data, nd.lab.ctypes.data,
+                                nd.typ.ctypes.data, nd.part.ctypes.data, nd.part3.ctypes.data)
+        if m != n:
+            raise RuntimeError("oracle seeding failed")
+        return nd
 
     def state(self, g: Grid, prm: RelaxParams, nd: Nodes) -> "OracleState":
         return OracleState(self, g, prm, nd)

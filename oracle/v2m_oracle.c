@@ -28,6 +28,9 @@
 #define FMIN fminf
 #define FMAX fmaxf
 #include "v2m_oracle_body.h"
+#define POW powf
+#include "v2m_seed_oracle_body.h"
+#undef POW
 #undef REAL
 #undef K
 #undef FN
@@ -176,4 +179,28 @@ int orc_relax_f32(const v2m_grid_view* g, const v2m_relax_params* p, v2m_nodes_v
     }
     orcf_free(s);
     return 0;
+}
+
+/* tn::seed_cpu restated (v2m_seed_oracle_body.h), in float. Returns the node
+   count; the arrays (P 3n, lab n, typ n, part 2n, part3 n) are written when
+   cap >= the count. -1 on failure. */
+int64_t orc_seed_f32(const v2m_grid_view* g, const v2m_relax_params* p, int64_t cap, float* P, uint16_t* lab,
+                     uint8_t* typ, uint16_t* part, uint16_t* part3) {
+    if (!g || !p || !g->grade) return -1;
+    v2m_nodes_view none;
+    memset(&none, 0, sizeof(none));
+    orcf_state* s = orcf_create(g, p, &none);
+    if (!s) return -1;
+    orcf_seeds o;
+    int n = orcf_seed(s, g->grade, p, &o);
+    if (n >= 0 && cap >= n && n > 0) {
+        memcpy(P, o.P, sizeof(float) * 3 * (size_t)n);
+        memcpy(lab, o.lab, 2 * (size_t)n);
+        memcpy(typ, o.typ, (size_t)n);
+        memcpy(part, o.part, 4 * (size_t)n);
+        memcpy(part3, o.part3, 2 * (size_t)n);
+    }
+    orcf_seeds_free(&o);
+    orcf_free(s);
+    return n;
 }

@@ -117,3 +117,28 @@ def test_seed_cases_build(ref):
         assert g.grade is not None and g.grade.shape == (g.nz, g.ny, g.nx)
         assert set(np.unique(nd.typ)) == types, name
         assert nd.part3.shape == (nd.size(),)
+
+
+@pytest.mark.parametrize("name", ["phantom", "noise", "mcx", "csg"])
+def test_oracle_seeding_equals_reference(name, ref):
+    """The plain-C restatement of seed_cpu against the compiled reference."""
+    from oracle.oracle import Oracle
+    prm = RelaxParams()
+    g, rnd = cases.seed_case(ref, name, prm)
+    nd = Oracle("f32").seed(g, prm)
+    assert nd.size() == rnd.size()
+    for f in ("P", "lab", "typ", "part", "part3"):
+        d = cases.first_diff(getattr(nd, f), getattr(rnd, f))
+        assert d is None, f"{f}: {d}"
+
+
+@pytest.mark.parametrize("prm", [RelaxParams(jseed=0.0), RelaxParams(corners=False),
+                                 RelaxParams(voxel_trap=True, fire=False), RelaxParams(nseed=1)],
+                         ids=["no_junction_seeds", "no_corners", "voxel_trap", "one_level"])
+def test_oracle_seeding_variants(prm, ref):
+    from oracle.oracle import Oracle
+    g, rnd = cases.seed_case(ref, "noise", prm)
+    nd = Oracle("f32").seed(g, prm)
+    assert nd.size() == rnd.size()
+    for f in ("P", "lab", "typ", "part", "part3"):
+        assert cases.first_diff(getattr(nd, f), getattr(rnd, f)) is None, f
