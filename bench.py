@@ -184,9 +184,55 @@ def dist_setup(args):
     return world, rank, local
 
 
+def run_seed_reference(args):
+    """The reference arm of seed_tpm182: seed_cpu on the host cores, W + K whole
+    seedings of the same grid."""
+    from oracle.ref import RefLib, available
+    from trussnet_b200 import synth
+    from trussnet_b200.types import RelaxParams
+    if not available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libv2m_ref.so is not built"}))
+        return
+    g, _ = synth.tpm()
+    g.grade = synth.size_grades(g.h, g.hmin, g.hmax)
+    prm = RelaxParams()
+    lib = RefLib()
+    for _ in range(args.warmup):
+        lib.seed(g, prm)
+    ts = []
+    n = 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        n = lib.seed(g, prm).size()
+        ts.append(time.perf_counter() - t0)
+    dt = statistics.mean(ts)
+    cores = os.cpu_count() or 1
+    cap = int(os.environ.get("V2M_OMP_MAX_THREADS", "64"))
+    cores = min(cores, cap) if cap > 0 else cores
+    v = n / dt
+    print(json.dumps({"metric": "seeding seeds/s", "value": v, "unit": "seeds/s", "n_gpus": args.gpus,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                      "impl": "reference",
+                      "config": {"workload": "seed_tpm182: the tpm182 grid, nseed 8, jseed 0.8, corners on",
+                                 "nodes": n},
+                      "cpu_baseline": {"value": v, "unit": "seeds/s", "cores": cores, "kind": "reference",
+                                       "sample": f"seed_cpu, whole seedings of the grid, {dt:.2f} s each"},
+                      "e2e": {"value": v, "unit": "seeds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+          flush=True)
+
+
 def run_reference(args):
     world, rank, _ = dist_setup(args)
     if rank != 0:
+        return
+    if args.workload == "seed_tpm182":
+        run_seed_reference(args)
+        return
+    if args.workload in ("batch64", "adjoint"):
+        why = {"batch64": "the reference relaxes one volume per call; its arm is the default workload's",
+               "adjoint": "the reference has no adjoint of the relaxation"}[args.workload]
+        print(json.dumps({"impl": "reference", "unavailable": why}))
         return
     g, nd, prm, desc = workload(args.workload)
     from oracle.ref import available
