@@ -94,3 +94,33 @@ def test_session_create_rejects_bad_volume_count():
     assert L.v2m_session_create(0, None, None, None, 0, C.byref(h)) == _lib.V2M_ERR_ARG
     nv = NodesView()
     assert isinstance(nv, C.Structure)
+
+
+def test_python_views_match_the_c_header(tmp_path):
+    """The ctypes mirrors of the C ABI's structs have the header's size and
+    field offsets (compiled with the system C compiler)."""
+    import shutil
+    import subprocess
+    from trussnet_b200.types import GridView, NodesView, RelaxParamsC, RelaxStatsC
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not cc:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    structs = {"v2m_grid_view": GridView, "v2m_nodes_view": NodesView, "v2m_relax_params": RelaxParamsC,
+               "v2m_relax_stats": RelaxStatsC}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "v2m_cuda.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'    printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f in py._fields_:
+            lines.append(f'    printf("{cname} {f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    lines += ["    return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for f in py._fields_:
+            assert got[(cname, f[0])] == getattr(py, f[0]).offset, (cname, f[0])
