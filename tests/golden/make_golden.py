@@ -7,7 +7,7 @@ determinism and mesh conformity only), so these fixtures are outputs of the
 reference itself, run here on small seeded inputs; the inputs are stored too,
 so the fixtures do not depend on the generator's numpy/scipy versions.
 
-  python tests/golden/make_golden.py      (needs oracle/_ref built)
+  python tests/golden/make_golden.py [NAME ...]   (needs oracle/_ref built; default: all)
 
 Each fixture <name>.npz holds
   grid_*            the grid arrays (v2m_grid_view) and node seeds
@@ -15,6 +15,10 @@ Each fixture <name>.npz holds
   F                 after the first force pass
   it1_P, it1_typ, it1_part, it1_mv       after one whole iteration
   run_P, run_typ, run_part, run_stats    after relax_cpu with the stored parameters
+  grid_gTW, grid_gm (shape input only)    the compiled shape program
+
+and each seeding fixture seed_<name>.npz holds the grid (with grid_grade), the
+seeding parameters and seed_cpu's nodes (P, lab, typ, part, part3).
 """
 import os
 import sys
@@ -24,12 +28,15 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 from oracle.ref import RefLib  # noqa: E402
 from trussnet_b200 import synth  # noqa: E402
 from trussnet_b200.types import RelaxParams  # noqa: E402
+import cases as test_cases  # noqa: E402
 
 PARAM_FIELDS = ("max_iters", "dt", "dptol", "fire", "voxel_trap")
+SEED_FIELDS = ("nseed", "jseed", "corners", "voxel_trap")
 
 
 def cases(ref):
@@ -41,18 +48,50 @@ def cases(ref):
                                           density=1.0, seed=13) + (RelaxParams(max_iters=30, fire=False),)
     out["shells32_voxel"] = synth.shells(dim=32, nshell=2, rmin=7.0, rmax=13.0, amp=1.0, hlo=1.5, hhi=3.0,
                                          density=1.0, seed=14) + (RelaxParams(max_iters=15, voxel_trap=True),)
+    # shape input: the CSG scene of the tests, compiled and seeded by the reference
+    out["shape_csg"] = test_cases.shape_case(ref, "csg") + (RelaxParams(max_iters=15),)
     return out
+
+
+def seed_cases(ref):
+    """Seeding fixtures: a reference-built 5-label noise volume (every node kind)."""
+    prm = RelaxParams()
+    g, nd = test_cases.seed_case(ref, "noise", prm)
+    return {"seed_noise": (g, nd, prm)}
+
+
+def grid_arrays(g):
+    d = {}
+    for a in ("L", "bl_cnt", "bl_lab", "bl_slot", "phi", "h"):
+        d["grid_" + a] = getattr(g, a)
+    d["grid_dims"] = np.array([g.nx, g.ny, g.nz], np.int32)
+    d["grid_vs"] = np.array(g.vs, np.float32)
+    d["grid_hrange"] = np.array([g.hmin, g.hmax], np.float32)
+    if g.gm < 0:
+        d["grid_gTW"], d["grid_gm"] = g.gTW, np.array([g.gm], np.int32)
+    if g.grade is not None:
+        d["grid_grade"] = g.grade
+    return d
 
 
 def main():
     ref = RefLib()
+    only = set(sys.argv[1:])
+    for name, (g, nd, prm) in seed_cases(ref).items():
+        if only and name not in only:
+            continue
+        d = grid_arrays(g)
+        d["seed_params"] = np.array([float(getattr(prm, f)) for f in SEED_FIELDS], np.float64)
+        for a in ("P", "lab", "typ", "part", "part3"):
+            d["seeds_" + a] = getattr(nd, a)
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, **d)
+        print(f"{name}: {nd.size()} seeds -> {os.path.getsize(path)} B")
     for name, (g, nd, prm) in cases(ref).items():
-        d = {}
-        for a in ("L", "bl_cnt", "bl_lab", "bl_slot", "phi", "h"):
-            d["grid_" + a] = getattr(g, a)
-        d["grid_dims"] = np.array([g.nx, g.ny, g.nz], np.int32)
-        d["grid_vs"] = np.array(g.vs, np.float32)
-        d["grid_hrange"] = np.array([g.hmin, g.hmax], np.float32)
+        if only and name not in only:
+            continue
+        d = grid_arrays(g)
+        d.pop("grid_grade", None)
         d["seed_P"], d["seed_lab"], d["seed_typ"], d["seed_part"] = nd.P, nd.lab, nd.typ, nd.part
         d["params"] = np.array([float(getattr(prm, f)) for f in PARAM_FIELDS], np.float64)
         s = ref.state(g, prm, nd.copy())

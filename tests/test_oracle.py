@@ -144,3 +144,14 @@ def test_fp32_within_tolerance_of_fp64(name, record_property):
     assert perr.max() <= REL_TOL, f"position error {perr.max():.3g}"
     assert proj.max() <= PROJ_TOL, f"trapped position error {proj.max():.3g}"
     assert nact <= len(nd.P) // 1000 and ntyp <= len(nd.P) // 1000
+
+
+@pytest.mark.parametrize("name", golden_io.seed_names())
+def test_golden_seeding(name, f32):
+    """The seeding restatement against seed_cpu's stored nodes."""
+    g, prm, ref_nd = golden_io.load_seed(name)
+    nd = f32.seed(g, prm)
+    assert nd.size() == ref_nd.size()
+    for a in ("P", "lab", "typ", "part", "part3"):
+        diff = first_diff(getattr(nd, a), getattr(ref_nd, a))
+        assert diff is None, f"{a}: {diff}"
