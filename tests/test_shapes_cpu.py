@@ -142,3 +142,14 @@ def test_oracle_seeding_variants(prm, ref):
     assert nd.size() == rnd.size()
     for f in ("P", "lab", "typ", "part", "part3"):
         assert cases.first_diff(getattr(nd, f), getattr(rnd, f)) is None, f
+
+
+@pytest.mark.skipif(_lib.load().v2m_cuda_device_count() > 0, reason="a CUDA device is present")
+def test_seed_without_device_fails_loudly():
+    """No CPU fallback inside the library: seeding without a device is a CUDA error."""
+    from trussnet_b200 import seed_cl
+    g, _ = cases.sphere_small()
+    g = type(g)(**{**g.__dict__, "grade": np.zeros((g.nz, g.ny, g.nx), np.uint8)})
+    with pytest.raises(V2mError) as e:
+        seed_cl(g, RelaxParams())
+    assert e.value.code == _lib.V2M_ERR_CUDA
