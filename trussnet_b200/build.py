@@ -21,7 +21,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libv2m_cuda.so")
 SHIM = os.path.join(HERE, "libv2m_relax_cl.so")
-REF = "/root/reference"
+REF = os.environ.get("V2M_REFERENCE", "/root/reference")   # the reference tree (its headers, for the shim)
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "--fmad=false", "-prec-div=true",
               "-prec-sqrt=true", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
