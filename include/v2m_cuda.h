@@ -88,7 +88,9 @@ typedef struct {
     /* extensions */
     int32_t h_mode;          /* 0: h at the nearest voxel (reference); 1: trilinear h */
     int32_t rebuild_div;     /* Verlet trigger divisor; 0: V2M_REBUILD_DIV or 300 (src/v2m_gpu.cpp:119) */
-    int32_t rebuild_policy;  /* 0: reference Verlet trigger; 1: rebuild when max |dp| since the build > 0.1 h */
+    int32_t rebuild_policy;  /* 0: reference Verlet trigger; 1: rebuild when max |dp| since the build > 0.1 h;
+                                2: fixed lists -- the first build's lists for the whole run (no rebuild, no
+                                self-refresh) */
 } v2m_relax_params;
 
 /* tn::Nodes (src/v2m_particles.h:78-87): the node arrays, caller-owned host memory. */
@@ -147,6 +149,39 @@ int v2m_seed_copy(const v2m_seed_result* r, float* P, uint16_t* lab, uint8_t* ty
 void v2m_seed_free(v2m_seed_result* r);
 
 /*
+ * tn::GridParams (src/v2m_grid.h:21-43) for the device grid build, same names
+ * and meaning; label input only: no interface sizes, no user sizing field.
+ */
+typedef struct {
+    float sigma, sigma_thin, thin_lo, thin_hi, thick, thin_floor, preserve, sigma_curv, hbase, hmin, hmax, K, g;
+    const float* hlab;   /* per-label size (mm), index = label, 0 = hbase; NULL (nhlab = 0): none */
+    int32_t nhlab;
+} v2m_grid_params;
+
+/* The reference's GridParams defaults (src/v2m_grid.h:22-37). */
+void v2m_grid_params_default(v2m_grid_params* p);
+
+/*
+ * The relaxation's fields built on CUDA device `device` (-1 = device 0) from a
+ * label volume: tn::build_grid_cpu (src/v2m_grid.cpp:47-722) for label input,
+ * bit for bit -- the labels within R of each brick, one slot per (mixed brick,
+ * label), the smoothed indicators (sigma, blended with sigma_thin by the local
+ * thickness), the sizing field (label sizes, curvature bound, gradient limit)
+ * and the size grades. L: nx*ny*nz labels (host, x fastest); vs: voxel size
+ * (mm). *out receives the grid, read through v2m_grid_result_view (host arrays
+ * owned by the result; the view's L is the result's copy of the labels) and
+ * freed by v2m_grid_free. The steps that call the C library's logf in the
+ * reference (the thickness's erfinv, the grades) evaluate it on the host.
+ */
+typedef struct v2m_grid_result v2m_grid_result;
+int v2m_grid_build_cuda(const uint16_t* L, int32_t nx, int32_t ny, int32_t nz, const float* vs,
+                        const v2m_grid_params* p, int device, v2m_grid_result** out);
+int v2m_grid_result_view(const v2m_grid_result* r, v2m_grid_view* g);
+/* hbase (mm), the brick label radius R, the slot count and the gradient-limit sweeps of a built grid */
+int v2m_grid_result_info(const v2m_grid_result* r, float* hbase, int32_t* R, int64_t* nslots, int32_t* limit_sweeps);
+void v2m_grid_free(v2m_grid_result* r);
+
+/*
  * Many independent volumes in one set of launches (one per stage for all of
  * them), the iteration loop captured in a CUDA graph. Each volume keeps its own
  * hash, lists, FIRE state and stop / rebuild decisions, so volume v's result is
@@ -201,6 +236,8 @@ int v2m_session_stats(v2m_session* s, int vol, v2m_relax_stats* st);
 #define V2M_ARR_PW 11        /* float [n]   FIRE power a.v of the last move */
 #define V2M_ARR_P0 12        /* float [3n]  positions at the last list build */
 #define V2M_ARR_HIST 13      /* int32 [34]  log2 histogram, max |dp|/h bits, half-skin count */
+#define V2M_ARR_SERIAL_SUMS 14 /* int32 [1] iterations whose FIRE power was within rounding of zero, so that
+                                  its sign was taken from relax_cpu's serial order */
 int v2m_session_read_array(v2m_session* s, int vol, int what, void* host, int64_t bytes);
 /* Overwrite an internal array of volume `vol` from host memory (P, typ, part, nbr, nnb, V, hn). */
 int v2m_session_write_array(v2m_session* s, int vol, int what, const void* host, int64_t bytes);
@@ -281,6 +318,22 @@ int v2m_unroll_timing(v2m_unroll* u, float* ms_forward, float* ms_backward);
 const char* v2m_unroll_last_error(void);
 
 /*
+ * Host-side check of truss lists (no device is used): row-major nbr[i*V2M_K+k]
+ * (local ids) and nnb[i] of n nodes, held to the rules of the reference's list
+ * build (v2m_neighbors, src/opencl/v2m_particle_body.cl:73-151): 0 <= nnb <=
+ * V2M_K, ids in [0, n), no self-edge, no repeated id, and entries in strictly
+ * ascending (distance, id) order, the distance recomputed with the list build's
+ * float expression from the positions the lists were built from -- pi (3n
+ * floats): each node's position at its last build (V2M_ARR_P0); pj (3n floats):
+ * each node's position in the bin-order snapshot of the last full build (Ps by
+ * way of the sorted ids). Returns V2M_OK, or V2M_ERR_KERNEL with the first
+ * violation in `report` (and v2m_cuda_last_error). No counterpart in the
+ * reference, which has no list checker.
+ */
+int v2m_validate_lists(int64_t n, const int32_t* nbr, const int32_t* nnb, const float* pi, const float* pj,
+                       char* report, int64_t report_len);
+
+/*
  * The hash's stable counting sort with no device allocation, for callers that
  * cannot call cudaMalloc: a process whose GPU memory belongs to its own pool (a
  * framework's caching allocator, a host application that reserved most of the
@@ -292,15 +345,19 @@ const char* v2m_unroll_last_error(void);
  * caller: sorted int32[n] (node ids by (key, id)) and cstart int32[nbins + 1]
  * (bin starts) -- what the hash build produces (v2m_session_read_array's
  * V2M_ARR_SORTED / V2M_ARR_CSTART). stream: a cudaStream_t, NULL for the legacy
- * default stream; the call returns when the sort is done.
+ * default stream. The call is synchronous: it waits on `stream` and returns
+ * when the sort is done. A key outside [0, nbins) returns V2M_ERR_ARG.
  *
- * Scratch is a fixed array in the library's device memory (about 8 MB, on every
+ * Scratch is a fixed array in the library's device memory (about 24 MB, on every
  * GPU that loads the library, until exit): nbins is limited to
- * V2M_NOALLOC_MAX_BINS, larger requests return V2M_ERR_ARG. Its device address
- * is looked up on the first call made on each device (call once before any
- * stream capture). Calls share the array: calls that overlap on the GPU race.
+ * V2M_NOALLOC_MAX_BINS and n to V2M_NOALLOC_MAX_KEYS, larger requests return
+ * V2M_ERR_ARG. Its device address is looked up on the first call made on each
+ * device; a cudaDeviceReset of that device makes it stale (do not call again on
+ * that device in the same process). Calls share the array: calls that overlap
+ * on the GPU race. Bins of any size cost work linear in their size.
  */
 #define V2M_NOALLOC_MAX_BINS (1 << 20)
+#define V2M_NOALLOC_MAX_KEYS (1 << 22)
 int v2m_bin_sort_noalloc(const int32_t* key, int64_t n, int64_t nbins, int32_t* sorted, int32_t* cstart,
                          void* stream);
 const char* v2m_bin_sort_noalloc_error(void);

@@ -48,6 +48,8 @@ class RefLib:
         L.ref_grid_build.restype = vp
         L.ref_grid_build.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, C.c_float, C.c_float, C.c_float, C.c_float]
         L.ref_grid_view.argtypes = [vp, C.POINTER(GridView)]
+        L.ref_grid_build_p.restype = vp
+        L.ref_grid_build_p.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp]
         L.ref_shape_grid.restype = vp
         L.ref_shape_grid.argtypes = [C.c_char_p, C.c_char_p, C.c_double, C.c_double, C.c_double, C.c_int, C.c_float,
                                      C.c_float, C.c_float, C.c_float]
@@ -90,6 +92,32 @@ class RefLib:
         nz, ny, nx = L.shape
         vsa = np.array(vs, np.float32)
         h = self.L.ref_grid_build(L.ctypes.data, nx, ny, nz, vsa.ctypes.data, sigma, hbase, hmin, hmax)
+        if not h:
+            raise RuntimeError(self.err())
+        try:
+            gv = GridView()
+            self.L.ref_grid_view(h, C.byref(gv))
+            g = Grid.from_view(gv)
+        finally:
+            self.L.ref_grid_free(h)
+        return g
+
+    def build_grid_p(self, L: np.ndarray, vs=(1.0, 1.0, 1.0), prm=None) -> Grid:
+        """tn::build_grid_cpu of label volume L [nz, ny, nx] with every field of
+        GridParams (trussnet_b200.types.GridParams, hlab included)."""
+        from trussnet_b200.types import GridParams, GridParamsC
+        prm = prm or GridParams()
+        L = np.ascontiguousarray(L, np.uint16)
+        nz, ny, nx = L.shape
+        pc = GridParamsC()
+        for f in ("sigma", "sigma_thin", "thin_lo", "thin_hi", "thick", "thin_floor", "preserve", "sigma_curv",
+                  "hbase", "hmin", "hmax", "K", "g"):
+            setattr(pc, f, float(getattr(prm, f)))
+        hl = np.ascontiguousarray(prm.hlab, np.float32)
+        pc.hlab = hl.ctypes.data if hl.size else None
+        pc.nhlab = int(hl.size)
+        vsa = np.array(vs, np.float32)
+        h = self.L.ref_grid_build_p(L.ctypes.data, nx, ny, nz, vsa.ctypes.data, C.byref(pc))
         if not h:
             raise RuntimeError(self.err())
         try:

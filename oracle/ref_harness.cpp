@@ -324,6 +324,46 @@ void* ref_shape_grid(const char* json, const char* overlap, double voxel, double
 }
 
 // Pointers into the reference grid (valid until ref_grid_free).
+// tn::build_grid_cpu with every GridParams field of the C ABI's v2m_grid_params
+// (the device grid build's parameters), hlab included.
+void* ref_grid_build_p(const uint16_t* labels, int nx, int ny, int nz, const float* vs, const v2m_grid_params* p) {
+    try {
+        RefGrid* r = new RefGrid();
+        r->lv.nx = nx;
+        r->lv.ny = ny;
+        r->lv.nz = nz;
+        r->lv.voxelsize = { { vs[0], vs[1], vs[2] } };
+        r->lv.data.assign(labels, labels + static_cast<size_t>(nx) * ny * nz);
+        int m = 0;
+        for (uint16_t l : r->lv.data) {
+            m = std::max<int>(m, l);
+        }
+        r->lv.maxlabel = m;
+        tn::GridParams gp;
+        gp.sigma = p->sigma;
+        gp.sigma_thin = p->sigma_thin;
+        gp.thin_lo = p->thin_lo;
+        gp.thin_hi = p->thin_hi;
+        gp.thick = p->thick;
+        gp.thin_floor = p->thin_floor;
+        gp.preserve = p->preserve;
+        gp.sigma_curv = p->sigma_curv;
+        gp.hbase = p->hbase;
+        gp.hmin = p->hmin;
+        gp.hmax = p->hmax;
+        gp.K = p->K;
+        gp.g = p->g;
+        if (p->nhlab > 0) {
+            gp.hlab.assign(p->hlab, p->hlab + p->nhlab);
+        }
+        tn::build_grid_cpu(r->lv, gp, r->g);
+        return r;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return nullptr;
+    }
+}
+
 int ref_grid_view(void* h, v2m_grid_view* v) {
     RefGrid* r = static_cast<RefGrid*>(h);
     tn::Grid& g = r->g;

@@ -1308,13 +1308,19 @@ static int FN(tail)(FN(state)* s) {
     }
     int nhalf = 0, nref = 0;
     const REAL skin = (REAL)s->prm.skin;
+    const int policy = s->prm.rebuild_policy;   /* extensions: 1 max displacement, 2 fixed lists */
+    REAL maxd = K(0.0);
     FN(cand)* buf = NULL;
     int cap = 0;
     for (int i = 0; i < n; ++i) {
         REAL ex = s->P[3 * i] - s->P0[3 * i], ey = s->P[3 * i + 1] - s->P0[3 * i + 1], ez = s->P[3 * i + 2] - s->P0[3 * i + 2];
         REAL h = FN(h_at)(s, s->P + 3 * i);
         REAL m2 = ex * ex + ey * ey + ez * ez, s2 = skin * skin * h * h;
-        if (m2 > s2) {
+        if (policy == 1) {
+            const REAL d = SQRT(m2) / h;
+            maxd = d > maxd ? d : maxd;
+        }
+        if (m2 > s2 && policy != 2) {
             FN(neighbors)(s, i, &buf, &cap);
             s->P0[3 * i] = s->P[3 * i];
             s->P0[3 * i + 1] = s->P[3 * i + 1];
@@ -1327,6 +1333,11 @@ static int FN(tail)(FN(state)* s) {
     free(buf);
     s->nhalf = nhalf;
     s->nrefresh = nref;
+    if (policy == 1) {
+        if (maxd > K(0.1)) FN(rebuild)(s);
+        return 0;
+    }
+    if (policy == 2) return 0;   /* the first build's lists for the whole run */
     int endgame = it >= s->prm.max_iters * 4 / 5 || s->p99 < K(4.0) * (REAL)s->prm.dptol;
     int div = endgame ? (s->rebuild_div > 1000 ? s->rebuild_div : 1000) : s->rebuild_div;
     if (nhalf > n / div) FN(rebuild)(s);

@@ -3,8 +3,9 @@ pipeline's own dispatch over the reference's types (tests/dropin_driver.cpp).
 
 CPU: without a device relax_cl throws std::runtime_error and the pipeline's
 fallback (restore the seeds, relax_cpu) produces the reference result.
-GPU: relax_cl runs on the device and its nodes equal relax_cpu's bit for bit
-(FIRE power summed in the CPU's serial order).
+GPU: relax_cl runs on the device and its nodes equal relax_cpu's bit for bit;
+and a failure injected on the host in the middle of a run (V2M_CUDA_FAIL_AT)
+takes the pipeline's fallback with the seeds restored.
 """
 import os
 import subprocess
@@ -40,8 +41,24 @@ def test_fallback_without_device():
 @needs_driver
 @pytest.mark.gpu
 def test_dropin_on_device_equals_relax_cpu():
-    f, err = run({"V2M_CUDA_SERIAL_POWER": "1"})
+    f, err = run()
     assert f["path"] == "cuda", err
     assert f["identical"] == "1"
     a, b = f["iters"].split("/")
     assert a == b
+
+
+@needs_driver
+@pytest.mark.gpu
+@pytest.mark.parametrize("where", ["create", "rebuild", "iterate:10", "readback"])
+def test_injected_fault_restores_seeds_and_falls_back(where):
+    """A failure of the library in the middle of a run on a live device
+    (V2M_CUDA_FAIL_AT: the host code fails as a CUDA call would; nothing is done
+    to the GPU) reaches the pipeline's dispatch as std::runtime_error; it
+    restores the seeds and runs relax_cpu, so the result equals relax_cpu's.
+    At readback the positions were already written into the pipeline's nodes
+    when the failure came: the restore is what makes the result right."""
+    f, err = run({"V2M_CUDA_FAIL_AT": where})
+    assert f["path"] == "cpu-fallback", err
+    assert "injected fault at " + where.split(":")[0] in err
+    assert f["identical"] == "1"

@@ -98,9 +98,10 @@ def test_one_iteration_bit_exact(name, fire, ref, cuda_lib):
 
 
 @pytest.mark.parametrize("name", CASES)
-def test_full_relax_bit_exact_serial_power(name, ref, cuda_lib, monkeypatch):
-    """Whole loop, FIRE power summed in the CPU's serial order: identical to relax_cpu."""
-    monkeypatch.setenv("V2M_CUDA_SERIAL_POWER", "1")
+def test_full_relax_bit_exact(name, ref, cuda_lib):
+    """Whole loop in the production mode (the FIRE power's sign from the block
+    tree when it is clear of rounding, else from the serial order): identical to
+    relax_cpu."""
     g, nd = load_case(name, ref)
     prm = cases.params(60)
     a = nd.copy()
@@ -117,10 +118,9 @@ def test_full_relax_bit_exact_serial_power(name, ref, cuda_lib, monkeypatch):
 
 
 @pytest.mark.parametrize("name", ["sphere64", "shells_small", "ref_phantom"])
-def test_full_relax_tree_power(name, ref, cuda_lib):
-    """Production FIRE sum (fixed-shape double tree): same trajectory as the
-    CPU unless the power's sign differs from the serial sum's; the graph and the
-    plain launches agree bit for bit, and two runs are identical."""
+def test_full_relax_graph_and_plain(name, ref, cuda_lib):
+    """Longer runs: the graph and the plain launches agree bit for bit, and both
+    equal relax_cpu."""
     g, nd = load_case(name, ref)
     prm = RelaxParams(max_iters=200, dt=0.2, dptol=0.0) if name == "sphere64" else cases.params(80)
     a = nd.copy()
@@ -134,9 +134,54 @@ def test_full_relax_tree_power(name, ref, cuda_lib):
         c = s.read_nodes(nd.copy())
     for f in ("P", "typ", "part"):
         assert same_bits(getattr(b, f), getattr(c, f)), f"graph vs plain launches differ in {f}"
-    assert st.iters == st_ref.iters
-    d = first_diff(b.P, a.P)
-    assert d is None, f"P vs relax_cpu: {d}"
+    assert st.iters == st_ref.iters and st.fire_resets == st_ref.fire_resets
+    for f in ("P", "typ", "part"):
+        d = first_diff(getattr(b, f), getattr(a, f))
+        assert d is None, f"{f} vs relax_cpu: {d}"
+
+
+def two_pairs():
+    """Four interior nodes in a uniform label-1 volume (h = 1.25): two pairs of
+    nodes one voxel apart along x, each pair's bar compressed, the pairs out of
+    each other's reach. Equal and opposite forces +-f."""
+    from trussnet_b200 import synth
+    from trussnet_b200.types import Nodes
+    L = np.ones((32, 32, 32), np.uint16)
+    g = synth.build_grid(L, np.full(L.shape, 1.25, np.float32), 1.25, 1.25)
+    P = np.array([[15, 16, 16], [16, 16, 16], [15, 16, 24], [16, 16, 24]], np.float32)
+    nd = Nodes(P=P, lab=np.ones(4, np.uint16), typ=np.zeros(4, np.uint8), part=np.full((4, 2), 0xFFFF, np.uint16))
+    return g, nd
+
+
+def test_fire_power_within_rounding_of_zero(ref, cuda_lib):
+    """Velocities planted so that the powers are f 2^61, -f 2^61, -2f, 0: the
+    serial double sum is -2f (uphill: FIRE resets), while a pairwise tree
+    rounds f 2^61 - 2f to f 2^61 and gives 0 (downhill). The sum is within the
+    rounding bound of zero, so the kernel takes the serial order: the same reset
+    as relax_cpu, and the fallback is counted."""
+    g, nd = two_pairs()
+    prm = cases.params(5, dptol=0.0)
+    V = np.array([[-2.0 ** 61, 0, 0], [-2.0 ** 61, 0, 0], [2, 0, 0], [0, 0, 0]], np.float32)
+    rs = ref.state(g, prm, nd.copy())
+    rs.rebuild()
+    rs.write("V", V.reshape(-1))
+    rs.force()
+    with Session(g, prm, nd.copy()) as s:
+        s.rebuild()
+        s.write("V", V.reshape(-1))
+        s.force()
+        F = s.read("F").reshape(-1, 4)
+        assert F[0, 0] == -F[1, 0] and F[2, 0] == -F[3, 0] and F[0, 0] < 0
+        rs.tail()
+        s.step_tail()
+        pw = s.read("pw").astype(np.float64)
+        assert pw[0] == -pw[1] and pw[2] < 0 and pw[3] == 0
+        assert sum(pw.tolist()) < 0 and (pw[0] + pw[2]) + (pw[1] + pw[3]) == 0.0
+        assert s.read("serial_sums")[0] == 1
+        assert s.stats().fire_resets == rs.counts()["fire_resets"] == 1
+        for a in ("P", "typ", "V", "pw"):
+            d = first_diff(s.read(a), rs.read(a))
+            assert d is None, f"{a}: {d}"
 
 
 def test_relax_cl_deterministic(cuda_lib):
@@ -175,8 +220,7 @@ def test_corners_stay(ref, cuda_lib):
     assert same_bits(b.P, a.P) and same_bits(b.typ, a.typ)
 
 
-def test_batch_equals_single(cuda_lib, monkeypatch):
-    monkeypatch.setenv("V2M_CUDA_SERIAL_POWER", "1")
+def test_batch_equals_single(cuda_lib):
     vols = [cases.sphere_small(), cases.shells_small(), cases.tpm_small()]
     prms = [cases.params(40), cases.params(25), cases.params(30)]
     singles = []
@@ -224,12 +268,7 @@ def test_trilinear_h_matches_oracle(cuda_lib):
     a = nd.copy()
     Oracle("f32").relax(g, prm, a)
     b = nd.copy()
-    import os
-    os.environ["V2M_CUDA_SERIAL_POWER"] = "1"
-    try:
-        relax_cl(g, prm, b)
-    finally:
-        del os.environ["V2M_CUDA_SERIAL_POWER"]
+    relax_cl(g, prm, b)
     for f in ("P", "typ", "part"):
         d = first_diff(getattr(b, f), getattr(a, f))
         assert d is None, f"{f}: {d}"
@@ -274,3 +313,70 @@ def test_step_within_tolerance_of_fp64(name, cuda_lib, record_property):
     assert ferr.max() <= 1e-6 and perr.max() <= 1e-6
     assert proj.size == 0 or proj.max() <= 1e-2
     assert (~same).sum() <= n // 1000
+
+
+def test_crowded_bin_rebuild_bit_exact(ref, cuda_lib):
+    """3,000 nodes packed into one hash bin (sphere_small's bins are 3.2 voxels
+    wide; this cube lies inside bin (7, 7, 7)): the in-bin order is sorted by
+    the whole block instead of one thread, and keys, sorted ids, bin starts,
+    bin-order positions and lists still equal relax_cpu's rebuild."""
+    g, nd = cases.sphere_small()
+    nd = nd.copy()
+    rng = np.random.default_rng(21)
+    idx = rng.choice(nd.size(), 3000, replace=False)
+    nd.P[idx] = rng.uniform(22.0, 25.0, (3000, 3)).astype(np.float32)
+    nd.typ[idx] = 0
+    prm = cases.params(3)
+    rs = ref.state(g, prm, nd.copy())
+    rs.rebuild()
+    cs = rs.read("cstart")
+    assert np.diff(cs).max() >= 3000
+    with Session(g, prm, nd.copy()) as s:
+        s.rebuild()
+        for a in ("key", "sorted", "cstart", "nnb"):
+            d = first_diff(s.read(a), rs.read(a))
+            assert d is None, f"{a}: {d}"
+        assert same_bits(s.read("Ps"), rs.read("Ps"))
+        n = nd.size()
+        nnb = rs.read("nnb")
+        d = first_diff(rowmajor_lists(s.read("nbr"), nnb, n), rowmajor_lists(rs.read("nbr"), nnb, n))
+        assert d is None, f"nbr: {d}"
+        rs.force()
+        s.force()
+        assert first_diff(s.read("F"), rs.read("F")) is None
+
+
+@pytest.mark.parametrize("name", ["shells_small", "tpm_small", "ref_phantom"])
+def test_session_lists_pass_the_host_checker(name, ref, cuda_lib):
+    """The session's truss lists obey the list build's rules (host checker
+    v2m_validate_lists) after the first build and after iterations in which
+    nodes refreshed their own lists."""
+    g, nd = load_case(name, ref)
+    with Session(g, cases.params(20), nd.copy()) as s:
+        s.rebuild()
+        assert s.validate_lists() == ""
+        s.iterate(12, graph=False)
+        assert s.validate_lists() == ""
+
+
+@pytest.mark.parametrize("policy", [1, 2])
+@pytest.mark.parametrize("name", ["sphere64", "shells_small"])
+def test_rebuild_policy_extensions_match_oracle(name, policy, cuda_lib):
+    """Extensions without a reference counterpart, against the FP32 C
+    restatement (which equals relax_cpu under the reference policy): policy 1
+    rebuilds when some node moved more than 0.1 h since the last build; policy 2
+    keeps the first build's lists for the whole run (the fixed edge list of the
+    64^3 sphere workload)."""
+    from oracle.oracle import Oracle
+    g, nd = getattr(cases, name)()
+    prm = RelaxParams(max_iters=60, dt=0.2, dptol=0.0, rebuild_policy=policy)
+    a = nd.copy()
+    sa = Oracle("f32").relax(g, prm, a)
+    b = nd.copy()
+    sb = relax_cl(g, prm, b)
+    assert sa.iters == sb.iters and sa.rebuilds == sb.rebuilds
+    if policy == 2:
+        assert sb.rebuilds == 1
+    for f in ("P", "typ", "part"):
+        d = first_diff(getattr(b, f), getattr(a, f))
+        assert d is None, f"{f}: {d}"

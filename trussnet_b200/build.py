@@ -21,12 +21,25 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libv2m_cuda.so")
 SHIM = os.path.join(HERE, "libv2m_relax_cl.so")
-REF = os.environ.get("V2M_REFERENCE", "/root/reference")   # the reference tree (its headers, for the shim)
+
+
+def _reference_tree() -> str:
+    """The reference tree whose headers the shim and the drop-in driver compile
+    against: V2M_REFERENCE, else the location oracle/Makefile's recipe names
+    (the one place that names it)."""
+    if os.environ.get("V2M_REFERENCE"):
+        return os.environ["V2M_REFERENCE"]
+    r = subprocess.run(["make", "-s", "--no-print-directory", "-f", os.path.join(ROOT, "oracle", "Makefile"),
+                        "print-ref"], capture_output=True, text=True)
+    return r.stdout.strip() if r.returncode == 0 else ""
+
+
+REF = _reference_tree()
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "--fmad=false", "-prec-div=true",
-              "-prec-sqrt=true", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
-SOURCES = ["v2m_kernels.cu", "v2m_host.cu", "v2m_adjoint.cu", "v2m_noalloc.cu", "v2m_seed.cu"]
-HEADERS = ["v2m_kernels.h", "v2m_types.cuh", "v2m_field.cuh", "v2m_sdf.cuh"]
+              "-prec-sqrt=true", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-Xptxas", "-v"]
+SOURCES = ["v2m_kernels.cu", "v2m_host.cu", "v2m_adjoint.cu", "v2m_noalloc.cu", "v2m_seed.cu", "v2m_grid.cu"]
+HEADERS = ["v2m_kernels.h", "v2m_types.cuh", "v2m_field.cuh", "v2m_sdf.cuh", "v2m_binsort.cuh", "v2m_grid.h"]
 
 
 def nvcc() -> str:

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "../../include/v2m_cuda.h"
+#include "v2m_grid.h"
 #include "v2m_kernels.h"
 
 using namespace v2m;
@@ -43,6 +44,31 @@ struct ArgError : std::runtime_error {
 struct KernelError : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
+
+// Host-side fault injection, for the callers' recovery paths (the pipeline's
+// CPU fallback, src/v2m_pipeline.cpp:497-526 of fangq/trussnet): with
+// V2M_CUDA_FAIL_AT=<stage>[:<k>] the host code fails at that point as if a CUDA
+// call had, with "injected fault at <stage>" -- nothing is done to the GPU.
+// Stages: create (before the first allocation), rebuild (the first list build),
+// iterate:<k> (the first host check at or after iteration k), readback (after
+// the positions have been written into the caller's arrays, before the types
+// and partners: the caller's nodes are left half-updated).
+void inject(const char* stage, int it = -1) {
+    const char* e = std::getenv("V2M_CUDA_FAIL_AT");
+    if (!e || !*e) {
+        return;
+    }
+    const std::string spec(e);
+    const size_t colon = spec.find(':');
+    const std::string name = spec.substr(0, colon);
+    if (name != stage) {
+        return;
+    }
+    if (it >= 0 && colon != std::string::npos && it < std::atoi(spec.c_str() + colon + 1)) {
+        return;
+    }
+    throw CudaError(std::string("injected fault at ") + stage + (it >= 0 ? " (iteration " + std::to_string(it) + ")" : ""));
+}
 
 void ck(cudaError_t e, const char* where) {
     if (e != cudaSuccess) {
@@ -66,6 +92,7 @@ int env_int(const char* name, int dflt) {
     const char* e = std::getenv(name);
     return e ? std::atoi(e) : dflt;
 }
+
 
 // Per-volume host bookkeeping.
 struct VolInfo {
@@ -394,6 +421,7 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
         throw ArgError("device index out of range");
     }
     ck(cudaSetDevice(dev), "cudaSetDevice");
+    inject("create");
     v2m_session* s = new v2m_session();
     try {
         s->device = dev;
@@ -459,6 +487,7 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
         d.pw = s->alloc<float>(N);
         d.key = s->alloc<int>(N);
         d.sorted = s->alloc<int>(N);
+        d.sort_tmp = s->alloc<int>(N);
         d.nbr = s->alloc<int>((size_t)N * V2M_K);
         d.nnb = s->alloc<uint8_t>(N);
         d.rlist = s->alloc<int>(N);
@@ -469,7 +498,7 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
         d.cursor = s->alloc<int>(KT);
         d.tilesum = s->alloc<int>(d.ntile_key);
         d.tileofs = s->alloc<int>(d.ntile_key);
-        d.psum = s->alloc<double>(N / kMoveThreads + 1);
+        d.psum = s->alloc<double2>(N / kMoveThreads + 1);
         d.pser = s->alloc<double>(nvol);
         s->Pq0 = s->alloc<float4>(N);
         s->typ0 = s->alloc<uint8_t>(N);
@@ -671,6 +700,7 @@ void do_iterate(v2m_session* s, int iters, int graph) {
             s->force_launches += G;
             done_it += G;
             read_ctl(s, c);
+            inject("iterate", c[0].it);
             if (s->time_force) {
                 for (int k = 0; k < G; ++k) {
                     float ms = 0.0f;
@@ -700,6 +730,7 @@ void do_iterate(v2m_session* s, int iters, int graph) {
             }
             if ((k + 1) % 25 == 0 || k + 1 == iters) {
                 read_ctl(s, c);
+                inject("iterate", c[0].it);
                 if (all_done(s, c)) {
                     break;
                 }
@@ -716,6 +747,7 @@ void do_iterate(v2m_session* s, int iters, int graph) {
 }
 
 void do_rebuild(v2m_session* s) {
+    inject("rebuild");
     const auto t0 = std::chrono::steady_clock::now();
     launch_set_rebuild(s->stream, s->d, 1);
     s->launches += 1;
@@ -766,6 +798,15 @@ void read_nodes(v2m_session* s, int v, v2m_nodes_view* nd) {
     ck(cudaMallocAsync((void**)&tmp, 12 * (size_t)I.n, s->stream), "cudaMallocAsync");
     launch_unpack_P(s->stream, s->d, I.nofs, I.n, tmp);
     ck(cudaMemcpyAsync(nd->P, tmp, 12 * (size_t)I.n, cudaMemcpyDeviceToHost, s->stream), "P");
+    if (std::getenv("V2M_CUDA_FAIL_AT")) {
+        ck(cudaStreamSynchronize(s->stream), "synchronize");   // (the positions are in the caller's arrays)
+        try {
+            inject("readback");
+        } catch (...) {
+            cudaFreeAsync(tmp, s->stream);
+            throw;
+        }
+    }
     ck(cudaMemcpyAsync(nd->typ, s->d.typ + I.nofs, I.n, cudaMemcpyDeviceToHost, s->stream), "typ");
     ck(cudaMemcpyAsync(nd->part, s->d.part + I.nofs, 4 * (size_t)I.n, cudaMemcpyDeviceToHost, s->stream), "part");
     ck(cudaFreeAsync(tmp, s->stream), "cudaFreeAsync");
@@ -800,6 +841,19 @@ float seed_spacing(int L, int nseed, float hmin, float hmax) {
 }
 
 }  // namespace
+
+// A grid built on the device, held on the host (tn::Grid's arrays).
+struct v2m_grid_result {
+    int32_t nx = 0, ny = 0, nz = 0;
+    float vs[3] = { 1, 1, 1 };
+    std::vector<uint16_t> L, bl_lab;
+    std::vector<int32_t> bl_cnt, bl_slot;
+    std::vector<float> phi, h;
+    std::vector<uint8_t> grade;
+    int64_t nslots = 0;
+    float hbase = 0, hmin = 0, hmax = 0;
+    int32_t R = 0, limit_sweeps = 0;
+};
 
 // Seeds made on the device, held on the host until copied out.
 struct v2m_seed_result {
@@ -1064,6 +1118,13 @@ int v2m_session_read_array(v2m_session* s, int vol, int what, void* host, int64_
             std::memcpy(h, c[vol].hist, 32 * 4);
             std::memcpy(h + 32, &c[vol].maxbits, 4);
             h[33] = c[vol].nhalf;
+            break;
+        }
+        case V2M_ARR_SERIAL_SUMS: {
+            need(4);
+            std::vector<VolCtl> c;
+            read_ctl(s, c);
+            *(int*)host = c[vol].serial_sums;
             break;
         }
         default: throw ArgError("unknown array");
@@ -1538,6 +1599,243 @@ int v2m_seed_copy(const v2m_seed_result* r, float* P, uint16_t* lab, uint8_t* ty
 
 void v2m_seed_free(v2m_seed_result* r) {
     delete r;
+}
+
+void v2m_grid_params_default(v2m_grid_params* p) {
+    std::memset(p, 0, sizeof(*p));
+    const GridParamsH d;
+    p->sigma = d.sigma;
+    p->sigma_thin = d.sigma_thin;
+    p->thin_lo = d.thin_lo;
+    p->thin_hi = d.thin_hi;
+    p->thick = d.thick;
+    p->thin_floor = d.thin_floor;
+    p->preserve = d.preserve;
+    p->sigma_curv = d.sigma_curv;
+    p->hbase = d.hbase;
+    p->hmin = d.hmin;
+    p->hmax = d.hmax;
+    p->K = d.K;
+    p->g = d.g;
+}
+
+int v2m_grid_build_cuda(const uint16_t* L, int32_t nx, int32_t ny, int32_t nz, const float* vs,
+                        const v2m_grid_params* p, int device, v2m_grid_result** out) {
+    return guard([&] {
+        if (!out || !L || !vs || !p) {
+            throw ArgError("null argument");
+        }
+        *out = nullptr;
+        if (nx < 1 || ny < 1 || nz < 1 || (int64_t)nx * ny * nz > (int64_t)0x7FFFFFFF) {
+            throw ArgError("grid dimensions must be positive, at most 2^31 voxels");
+        }
+        if (!(vs[0] > 0.0f && vs[1] > 0.0f && vs[2] > 0.0f)) {
+            throw ArgError("voxel sizes must be positive");
+        }
+        if (!(p->sigma > 0.0f) || !(p->sigma_curv > 0.0f) || p->sigma_thin < 0.0f || !(p->g >= 0.0f) ||
+            !(p->K > 0.0f) || (p->nhlab > 0 && !p->hlab) || p->nhlab < 0) {
+            throw ArgError("grid parameters out of range (sigma, sigma_curv > 0; sigma_thin, g >= 0; K > 0)");
+        }
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+            cudaGetLastError();
+            throw CudaError("no CUDA device available");
+        }
+        const int dev = device < 0 ? 0 : device;
+        if (dev >= ndev) {
+            throw ArgError("device index out of range");
+        }
+        ck(cudaSetDevice(dev), "cudaSetDevice");
+        GridBuildArgs A;
+        A.L = L;
+        A.nx = nx;
+        A.ny = ny;
+        A.nz = nz;
+        A.vs[0] = vs[0];
+        A.vs[1] = vs[1];
+        A.vs[2] = vs[2];
+        GridParamsH& q = A.prm;
+        q.sigma = p->sigma;
+        q.sigma_thin = p->sigma_thin;
+        q.thin_lo = p->thin_lo;
+        q.thin_hi = p->thin_hi;
+        q.thick = p->thick;
+        q.thin_floor = p->thin_floor;
+        q.preserve = p->preserve;
+        q.sigma_curv = p->sigma_curv;
+        q.hbase = p->hbase;
+        q.hmin = p->hmin;
+        q.hmax = p->hmax;
+        q.K = p->K;
+        q.g = p->g;
+        if (p->nhlab > 0) {
+            q.hlab.assign(p->hlab, p->hlab + p->nhlab);
+        }
+        A.device = dev;
+        cudaStream_t st = nullptr;
+        ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+        A.stream = st;
+        GridBuildOut O;
+        std::string err;
+        auto release = [&] {
+            cudaStreamSynchronize(st);
+            for (void* x : O.tmp) {
+                cudaFree(x);
+            }
+            O.tmp.clear();
+            cudaStreamDestroy(st);
+        };
+        const cudaError_t e = grid_build(A, O, err);
+        if (e != cudaSuccess) {
+            release();
+            cudaGetLastError();
+            throw CudaError(std::string("grid build: ") + cudaGetErrorString(e));
+        }
+        std::unique_ptr<v2m_grid_result> r(new v2m_grid_result());
+        const size_t nv = (size_t)nx * ny * nz;
+        const size_t nb = (size_t)((nx + 7) / 8) * ((ny + 7) / 8) * ((nz + 7) / 8);
+        r->nx = nx;
+        r->ny = ny;
+        r->nz = nz;
+        r->vs[0] = vs[0];
+        r->vs[1] = vs[1];
+        r->vs[2] = vs[2];
+        r->L.assign(L, L + nv);
+        r->bl_cnt.resize(nb);
+        r->bl_lab.resize(nb * V2M_BL);
+        r->bl_slot.resize(nb);
+        r->phi.resize((size_t)O.nslots * V2M_SLOT);
+        r->h.resize(nv);
+        r->grade.resize(nv);
+        auto d2h = [&](void* dst, const void* src, size_t bytes) {
+            if (bytes) {
+                ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st), "grid read-back");
+            }
+        };
+        try {
+            d2h(r->bl_cnt.data(), O.bl_cnt, 4 * nb);
+            d2h(r->bl_lab.data(), O.bl_lab, 2 * nb * V2M_BL);
+            d2h(r->bl_slot.data(), O.bl_slot, 4 * nb);
+            d2h(r->phi.data(), O.phi, 4 * r->phi.size());
+            d2h(r->h.data(), O.h, 4 * nv);
+            d2h(r->grade.data(), O.grade, nv);
+            ck(cudaStreamSynchronize(st), "synchronize");
+        } catch (...) {
+            release();
+            throw;
+        }
+        release();
+        r->nslots = O.nslots;
+        r->hbase = O.hbase;
+        r->hmin = O.hmin;
+        r->hmax = O.hmax;
+        r->R = O.R;
+        r->limit_sweeps = O.limit_sweeps;
+        *out = r.release();
+    });
+}
+
+int v2m_grid_result_view(const v2m_grid_result* r, v2m_grid_view* g) {
+    return guard([&] {
+        if (!r || !g) {
+            throw ArgError("null argument");
+        }
+        std::memset(g, 0, sizeof(*g));
+        g->nx = r->nx;
+        g->ny = r->ny;
+        g->nz = r->nz;
+        g->nbx = (r->nx + 7) / 8;
+        g->nby = (r->ny + 7) / 8;
+        g->nbz = (r->nz + 7) / 8;
+        g->vs[0] = r->vs[0];
+        g->vs[1] = r->vs[1];
+        g->vs[2] = r->vs[2];
+        g->L = r->L.data();
+        g->bl_cnt = r->bl_cnt.data();
+        g->bl_lab = r->bl_lab.data();
+        g->bl_slot = r->bl_slot.data();
+        g->phi = r->phi.data();
+        g->nslots = r->nslots;
+        g->h = r->h.data();
+        g->hmin = r->hmin;
+        g->hmax = r->hmax;
+        g->gm = 0;
+        g->grade = r->grade.data();
+    });
+}
+
+int v2m_grid_result_info(const v2m_grid_result* r, float* hbase, int32_t* R, int64_t* nslots, int32_t* limit_sweeps) {
+    return guard([&] {
+        if (!r) {
+            throw ArgError("null argument");
+        }
+        if (hbase) {
+            *hbase = r->hbase;
+        }
+        if (R) {
+            *R = r->R;
+        }
+        if (nslots) {
+            *nslots = r->nslots;
+        }
+        if (limit_sweeps) {
+            *limit_sweeps = r->limit_sweeps;
+        }
+    });
+}
+
+void v2m_grid_free(v2m_grid_result* r) {
+    delete r;
+}
+
+int v2m_validate_lists(int64_t n, const int32_t* nbr, const int32_t* nnb, const float* pi, const float* pj,
+                       char* report, int64_t report_len) {
+    std::string msg;
+    const int rc = guard([&] {
+        if (n < 0 || (n > 0 && (!nbr || !nnb || !pi || !pj))) {
+            throw ArgError("v2m_validate_lists: null array");
+        }
+        auto fail = [&](int64_t i, int k, const std::string& what) {
+            msg = "node " + std::to_string(i) + (k >= 0 ? ", entry " + std::to_string(k) : "") + ": " + what;
+            throw KernelError("truss lists invalid: " + msg);
+        };
+        for (int64_t i = 0; i < n; ++i) {
+            const int c = nnb[i];
+            if (c < 0 || c > V2M_K) {
+                fail(i, -1, "length " + std::to_string(c) + " outside [0, " + std::to_string(V2M_K) + "]");
+            }
+            const float px = pi[3 * i], py = pi[3 * i + 1], pz = pi[3 * i + 2];
+            float dprev = 0.0f;
+            int jprev = -1;
+            for (int k = 0; k < c; ++k) {
+                const int j = nbr[i * V2M_K + k];
+                if (j < 0 || j >= n) {
+                    fail(i, k, "id " + std::to_string(j) + " outside [0, n)");
+                }
+                if (j == i) {
+                    fail(i, k, "self-edge");
+                }
+                for (int q = 0; q < k; ++q) {
+                    if (nbr[i * V2M_K + q] == j) {
+                        fail(i, k, "id " + std::to_string(j) + " repeated");
+                    }
+                }
+                // the distance as v2m_neighbors computes it (src/opencl/v2m_particle_body.cl:104-123)
+                const float ex = pj[3 * (int64_t)j] - px, ey = pj[3 * (int64_t)j + 1] - py,
+                            ez = pj[3 * (int64_t)j + 2] - pz;
+                const float d = std::sqrt(ex * ex + ey * ey + ez * ez);
+                if (k > 0 && !(dprev < d || (dprev == d && jprev < j))) {
+                    fail(i, k, "not after the previous entry in (distance, id) order");
+                }
+                dprev = d;
+                jprev = j;
+            }
+        }
+    });
+    if (report && report_len > 0) {
+        std::snprintf(report, (size_t)report_len, "%s", rc == V2M_OK ? "" : g_err.c_str());
+    }
+    return rc;
 }
 
 int v2m_relax_cuda(const v2m_grid_view* g, const v2m_relax_params* prm, v2m_nodes_view* nd, v2m_relax_stats* st,

@@ -24,6 +24,7 @@
 #include <cstdint>
 #include <cstdio>
 
+#include "v2m_binsort.cuh"
 #include "v2m_field.cuh"
 #include "v2m_kernels.h"
 
@@ -268,43 +269,54 @@ __global__ void k_scatter(const VolCtl* __restrict__ ctl, const DVol* __restrict
     }
 }
 
-// ascending ids within bin e, then the bin's positions and sizes
-__device__ __forceinline__ void bin_order(const int* __restrict__ cstart, int* __restrict__ sorted,
-                                          const float4* __restrict__ Pq, float4* __restrict__ Ps, int64_t e) {
-    const int s0 = cstart[e], s1 = cstart[e + 1];
-    for (int a = s0 + 1; a < s1; ++a) {
-        const int x = sorted[a];
-        int b = a - 1;
-        while (b >= s0 && sorted[b] > x) {
-            sorted[b + 1] = sorted[b];
-            --b;
-        }
-        sorted[b + 1] = x;
-    }
-    for (int s = s0; s < s1; ++s) {
-        const float4 p = Pq[sorted[s]];
-        Ps[s] = make_float4(p.x, p.y, p.z, fabsf(p.w));
-    }
-}
-
 // One thread per bin: the bin's ids ascending (the CPU's stable counting sort,
 // src/v2m_particles.cpp:791-795), then their positions and sizes in bin order.
-__global__ void k_binsort(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl, const int16_t* __restrict__ tilevol,
-                          const int* __restrict__ cstart, int* __restrict__ sorted, const float4* __restrict__ Pq,
-                          float4* __restrict__ Ps, int64_t KT, const Global* G) {
+// A bin of more than kSmallBin ids is handed to the whole block
+// (block_bin_sort, over `tmp` at the same offsets), so the work stays linear in
+// the bin's size: clustered or coincident nodes cannot stall one thread.
+__global__ void __launch_bounds__(kBinSortThreads) k_binsort(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
+                                                          const int16_t* __restrict__ tilevol,
+                                                          const int* __restrict__ cstart, int* __restrict__ sorted,
+                                                          int* __restrict__ tmp, const float4* __restrict__ Pq,
+                                                          float4* __restrict__ Ps, int64_t KT, const Global* G) {
+    __shared__ BinSortSmem sm;
+    __shared__ int64_t big[kBinSortThreads];
+    __shared__ int nbig;
     if (!*((volatile const int*)&G->rebuild_any)) {
         return;
     }
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < KT; e += (int64_t)gridDim.x * blockDim.x) {
-        const int v = tilevol[e / kScanTile];
-        if (v < 0 || !ctl[v].rebuild) {
-            continue;
+    for (int64_t base = blockIdx.x * (int64_t)kBinSortThreads; base < KT; base += (int64_t)gridDim.x * kBinSortThreads) {
+        if (threadIdx.x == 0) {
+            nbig = 0;
         }
-        const DVol& V = vols[v];
-        if (e < V.kofs || e >= V.kofs + V.nkeys) {
-            continue;
+        __syncthreads();
+        const int64_t e = base + threadIdx.x;
+        if (e < KT) {
+            const int v = tilevol[e / kScanTile];
+            if (v >= 0 && ctl[v].rebuild && e >= vols[v].kofs && e < vols[v].kofs + vols[v].nkeys) {
+                const int s0 = cstart[e], s1 = cstart[e + 1];
+                if (s1 - s0 <= kSmallBin) {
+                    small_bin_sort(sorted + s0, s1 - s0);
+                    for (int s = s0; s < s1; ++s) {
+                        const float4 p = Pq[sorted[s]];
+                        Ps[s] = make_float4(p.x, p.y, p.z, fabsf(p.w));
+                    }
+                } else {
+                    big[atomicAdd(&nbig, 1)] = e;
+                }
+            }
         }
-        bin_order(cstart, sorted, Pq, Ps, e);
+        __syncthreads();
+        const int nb = nbig;
+        for (int q = 0; q < nb; ++q) {
+            const int s0 = cstart[big[q]], s1 = cstart[big[q] + 1];
+            block_bin_sort(sorted + s0, tmp + s0, s1 - s0, sm);
+            for (int s = s0 + threadIdx.x; s < s1; s += kBinSortThreads) {
+                const float4 p = Pq[sorted[s]];
+                Ps[s] = make_float4(p.x, p.y, p.z, fabsf(p.w));
+            }
+            __syncthreads();
+        }
     }
 }
 
@@ -675,11 +687,12 @@ constexpr int kForceBatch = 4;
 
 // One thread per node; the lists are slot-major (nbr[k*N + i]) so a warp's k-th
 // entries are one coalesced 128-byte row; neighbour position + signed size is
-// one 16-byte gather. Bars are added in list order, as v2m_force does.
+// one 16-byte gather. Bars are added in list order, as v2m_force does: the
+// deterministic ordered fold of the node's CSR row (no float atomics).
 __global__ void __launch_bounds__(256, 4) k_force(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
                                                const uint16_t* __restrict__ nodevol, const float4* __restrict__ Pq,
                                                const int* __restrict__ nbr, const uint8_t* __restrict__ nnb,
-                                               float4* __restrict__ F, int64_t N) {
+                                               float4* __restrict__ F, int64_t N, Global* G) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= N) {
         return;
@@ -703,25 +716,31 @@ __global__ void __launch_bounds__(256, 4) k_force(const DVol* __restrict__ vols,
     // every id first (one round trip: the slot-major rows are coalesced), then
     // the positions in batches of kForceBatch, so that a node's dependent chain
     // is 1 + ceil(nnb / 4) memory round trips rather than 2 ceil(nnb / 4); the
-    // bars are still added one by one in list order
+    // bars are still added one by one in list order. A list id outside the
+    // node's volume (a corrupted list) is reported and the list cut there.
     int jj[V2M_K];
+    int m = n;
 #pragma unroll
     for (int k = 0; k < V2M_K; ++k) {
         jj[k] = k < n ? __ldg(row + (int64_t)k * N) : (int)i;
+        if (k < m && (jj[k] < V.nofs || jj[k] >= V.nofs + V.n)) {
+            raise_error(G, 3, (int)i);
+            m = k;
+        }
     }
 #pragma unroll
     for (int k0 = 0; k0 < V2M_K; k0 += kForceBatch) {
-        if (k0 >= n) {
+        if (k0 >= m) {
             break;
         }
         float4 qq[kForceBatch];
 #pragma unroll
         for (int u = 0; u < kForceBatch; ++u) {
-            qq[u] = __ldg(Pq + (k0 + u < V2M_K ? jj[k0 + u] : (int)i));
+            qq[u] = __ldg(Pq + (k0 + u < m ? jj[k0 + u] : (int)i));
         }
 #pragma unroll
         for (int u = 0; u < kForceBatch; ++u) {
-            if (k0 + u >= n) {
+            if (k0 + u >= m) {
                 break;
             }
             const float4 q = qq[u];
@@ -786,7 +805,7 @@ __device__ __forceinline__ void node_tail(const DVol& Vd, VolCtl* ctl, int v, in
             atomicMax(reinterpret_cast<unsigned*>(&cv->pad1), __float_as_uint(sqrtf(m2) / hh));
         }
     }
-    if (m2 > s2) {
+    if (m2 > s2 && Vd.policy != 2) {
         const int e = atomicAdd(&G->nrefresh, 1);
         rlist[e] = (int)i;
         atomicAdd(&cv->nrefresh, 1);
@@ -840,11 +859,11 @@ __global__ void __launch_bounds__(kMoveThreads) k_move_pre(const DVol* __restric
                                                           float4* __restrict__ Vel, const uint8_t* __restrict__ typ,
                                                           float* __restrict__ mvout, float* __restrict__ pwout,
                                                           const float4* __restrict__ P0, float4* __restrict__ S,
-                                                          int* __restrict__ queue, double* __restrict__ psum,
+                                                          int* __restrict__ queue, double2* __restrict__ psum,
                                                           int* __restrict__ rlist, Global* G, int64_t N) {
     __shared__ TailAcc acc;
     __shared__ int sh_vol;
-    __shared__ double sh_pw[kMoveThreads / 32];
+    __shared__ double sh_pw[kMoveThreads / 32], sh_pa[kMoveThreads / 32];
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     tail_init(acc);
     if (threadIdx.x == 0) {
@@ -949,12 +968,17 @@ __global__ void __launch_bounds__(kMoveThreads) k_move_pre(const DVol* __restric
             sh_cnt[kind][wid] = __popc(km[kind]);
         }
     }
+    // the block's FIRE power and the sum of its magnitudes (the latter bounds
+    // the rounding error of any order of summation: k_control)
     double pd = active ? (double)pwv : 0.0;
+    double pa = fabs(pd);
     for (int o = 16; o > 0; o >>= 1) {
         pd += __shfl_down_sync(0xffffffffu, pd, o);
+        pa += __shfl_down_sync(0xffffffffu, pa, o);
     }
     if (lane == 0) {
         sh_pw[wid] = pd;
+        sh_pa[wid] = pa;
     }
     __syncthreads();
     if (threadIdx.x < 3) {
@@ -967,7 +991,8 @@ __global__ void __launch_bounds__(kMoveThreads) k_move_pre(const DVol* __restric
     }
     __syncthreads();
     if (qkind >= 0) {
-        int slot = sh_base[qkind] + __popc(km[qkind] & ((1u << lane) - 1u));
+        const unsigned mk = qkind == 0 ? km[0] : (qkind == 1 ? km[1] : km[2]);   // (no local-memory array)
+        int slot = sh_base[qkind] + __popc(mk & ((1u << lane) - 1u));
         for (int w = 0; w < wid; ++w) {
             slot += sh_cnt[qkind][w];
         }
@@ -978,11 +1003,12 @@ __global__ void __launch_bounds__(kMoveThreads) k_move_pre(const DVol* __restric
         return;
     }
     if (threadIdx.x == 0) {
-        double t = 0.0;
+        double t = 0.0, ta = 0.0;
         for (int w = 0; w < kMoveThreads / 32; ++w) {
             t += sh_pw[w];
+            ta += sh_pa[w];
         }
-        psum[blockIdx.x] = t;
+        psum[blockIdx.x] = make_double2(t, ta);
     }
     tail_flush(acc, ctl + bv);
 }
@@ -995,8 +1021,11 @@ __global__ void __launch_bounds__(kMoveThreads) k_move_pre(const DVol* __restric
 // Two instances: kShape = false moves the nodes of volumes with sampled fields,
 // kShape = true (launched only when some volume has them) those with analytic
 // shape fields; with both present each skips the other's nodes.
+#ifndef V2M_MOVE_MIN_BLOCKS
+#define V2M_MOVE_MIN_BLOCKS 8   // resident blocks of k_move_main per multiprocessor (8 x 128 threads: 64 registers)
+#endif
 template <bool kShape>
-__global__ void __launch_bounds__(kMainThreads, 8) k_move_main(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl,
+__global__ void __launch_bounds__(kMainThreads, V2M_MOVE_MIN_BLOCKS) k_move_main(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl,
                                                            const uint16_t* __restrict__ nodevol, float4* __restrict__ Pq,
                                                            float4* __restrict__ Vel, uint8_t* __restrict__ typ,
                                                            const uint16_t* __restrict__ lab, uint32_t* __restrict__ part,
@@ -1073,7 +1102,7 @@ __global__ void __launch_bounds__(kMainThreads, 8) k_move_main(const DVol* __res
     const unsigned gvol = __match_any_sync(act, (unsigned)v);
     const unsigned leader = (unsigned)(__ffs(gvol) - 1);
     const unsigned mx = __reduce_max_sync(gvol, __float_as_uint(m));
-    const bool refresh = m2 > s2;
+    const bool refresh = m2 > s2 && Vd.policy != 2;   // (policy 2: the first build's lists for the whole run)
     const bool half = !refresh && m2 > 0.25f * s2;
     const unsigned nh = __popc(__ballot_sync(act, half) & gvol);
     unsigned md = 0u;
@@ -1219,8 +1248,18 @@ __global__ void k_xfill(DGrid g, const int2* __restrict__ tabs, float* __restric
     }
 }
 
-// Serial FIRE power (the CPU's order: node 0 first, one double accumulator),
-// for bit-exact replays; one thread per volume.
+// The FIRE power in the CPU's order (src/v2m_particles.cpp:849-859: node 0
+// first, one double accumulator), on one thread.
+__device__ __noinline__ double serial_power(const float* __restrict__ pw, int64_t nofs, int n) {
+    double t = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        t += (double)pw[nofs + i];
+    }
+    return t;
+}
+
+// Serial FIRE power of every iteration (V2M_CUDA_SERIAL_POWER=1); one thread per
+// volume.
 __global__ void k_power_serial(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl, const float* __restrict__ pw,
                                double* __restrict__ pser, int nvol) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1231,20 +1270,29 @@ __global__ void k_power_serial(const DVol* __restrict__ vols, const VolCtl* __re
     if (!V.fire || ctl[v].done || ctl[v].it >= V.max_iters) {
         return;
     }
-    double t = 0.0;
-    for (int64_t i = 0; i < V.n; ++i) {
-        t += (double)pw[V.nofs + i];
-    }
-    pser[v] = t;
+    pser[v] = serial_power(pw, V.nofs, V.n);
 }
 
 // ---- the loop's control (one block per volume) ---------------------------------------
-__global__ void k_control(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl, const double* __restrict__ psum,
-                          const double* __restrict__ pser, int serial, int move_threads, Global* G) {
+// Only the sign of the FIRE power matters (FireCtl::update, src/v2m_particles.h:58-73),
+// and relax_cpu takes it from a serial double sum of the float powers. The
+// block sums summed in a fixed tree give a sum P and a sum A of magnitudes.
+// Every summation order of the n terms, the serial one and this tree alike, is
+// within gamma_(n+64) A of the exact sum S (recursive summation error bound,
+// gamma_k = k u / (1 - k u), u = 2^-53; no term passes through more than n + 64
+// additions in either). So when |P| > kPowerGuard (n + 64) u A, S and the serial
+// sum both have P's sign and P decides exactly as relax_cpu would. Otherwise
+// (a sum within rounding of zero) the serial sum is taken on one thread. A = 0
+// means every term is zero: every sum is +0.
+constexpr double kPowerGuard = 2.5;   // 2 gamma_(n+64) A <= 2.0001 (n + 64) u A' for n < 2^31, with margin
+
+__global__ void k_control(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl, const double2* __restrict__ psum,
+                          const double* __restrict__ pser, const float* __restrict__ pw, int serial, int move_threads,
+                          Global* G) {
     const int v = blockIdx.x;
     const DVol& V = vols[v];
     VolCtl& c = ctl[v];
-    __shared__ double red[kCtlThreads];
+    __shared__ double red[kCtlThreads], reda[kCtlThreads];
     __shared__ int s_skip;
     if (threadIdx.x == 0) {
         s_skip = c.done || c.it >= V.max_iters;
@@ -1256,28 +1304,41 @@ __global__ void k_control(const DVol* __restrict__ vols, VolCtl* __restrict__ ct
     if (s_skip) {
         return;
     }
-    double P = 0.0;
+    double P = 0.0, A = 0.0;
     if (V.fire && !serial) {
         const int b0 = (int)(V.nofs / move_threads);
         const int nb = (V.n + move_threads - 1) / move_threads;
-        double t = 0.0;
+        double t = 0.0, ta = 0.0;
         for (int b = threadIdx.x; b < nb; b += kCtlThreads) {
-            t += psum[b0 + b];
+            const double2 q = psum[b0 + b];
+            t += q.x;
+            ta += q.y;
         }
         red[threadIdx.x] = t;
+        reda[threadIdx.x] = ta;
         __syncthreads();
         for (int w = kCtlThreads / 2; w > 0; w >>= 1) {
             if (threadIdx.x < w) {
                 red[threadIdx.x] += red[threadIdx.x + w];
+                reda[threadIdx.x] += reda[threadIdx.x + w];
             }
             __syncthreads();
         }
         P = red[0];
+        A = reda[0];
     } else if (V.fire) {
         P = pser[v];
     }
     if (threadIdx.x != 0) {
         return;
+    }
+    if (V.fire && !serial) {
+        if (A == 0.0) {
+            P = 0.0;
+        } else if (!(fabs(P) > kPowerGuard * ((double)V.n + 64.0) * 0x1p-53 * A)) {
+            P = serial_power(pw, V.nofs, V.n);   // within rounding of zero: the CPU's own order
+            ++c.serial_sums;
+        }
     }
     const int it = c.it;
     if (V.fire) {
@@ -1337,6 +1398,8 @@ __global__ void k_control(const DVol* __restrict__ vols, VolCtl* __restrict__ ct
     int reb;
     if (V.policy == 1) {
         reb = maxd > 0.1f;
+    } else if (V.policy == 2) {
+        reb = 0;
     } else {
         const bool endgame = it >= V.max_iters * 4 / 5 || p99 < 4.0f * V.dptol;
         const int div = endgame ? (V.rebuild_div > 1000 ? V.rebuild_div : 1000) : V.rebuild_div;
@@ -1502,8 +1565,9 @@ void launch_scan(cudaStream_t s, const Dev& d) {
 
 void launch_scatter(cudaStream_t s, const Dev& d) {
     k_scatter<<<gsblocks(d, d.N, 256), 256, 0, s>>>(d.ctl, d.vols, d.nodevol, d.key, d.cursor, d.sorted, d.N, d.G);
-    k_binsort<<<gsblocks(d, d.KT, 256), 256, 0, s>>>(d.vols, d.ctl, d.tilevol, d.cstart, d.sorted, d.Pq, d.Ps, d.KT,
-                                                     d.G);
+    k_binsort<<<gsblocks(d, d.KT, kBinSortThreads), kBinSortThreads, 0, s>>>(d.vols, d.ctl, d.tilevol, d.cstart,
+                                                                             d.sorted, d.sort_tmp, d.Pq, d.Ps, d.KT,
+                                                                             d.G);
 }
 
 void launch_neighbors(cudaStream_t s, const Dev& d, int threads) {
@@ -1513,7 +1577,7 @@ void launch_neighbors(cudaStream_t s, const Dev& d, int threads) {
 }
 
 void launch_force(cudaStream_t s, const Dev& d, int threads) {
-    k_force<<<nblk(d.N, threads), threads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.nbr, d.nnb, d.F, d.N);
+    k_force<<<nblk(d.N, threads), threads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.nbr, d.nnb, d.F, d.N, d.G);
 }
 
 void launch_move(cudaStream_t s, const Dev& d) {
@@ -1544,7 +1608,7 @@ void launch_control(cudaStream_t s, const Dev& d, int serial) {
     if (serial) {
         k_power_serial<<<nblk(d.nvol, 32), 32, 0, s>>>(d.vols, d.ctl, d.pw, d.pser, d.nvol);
     }
-    k_control<<<d.nvol, kCtlThreads, 0, s>>>(d.vols, d.ctl, d.psum, d.pser, serial, kMoveThreads, d.G);
+    k_control<<<d.nvol, kCtlThreads, 0, s>>>(d.vols, d.ctl, d.psum, d.pser, d.pw, serial, kMoveThreads, d.G);
 }
 
 void launch_refresh(cudaStream_t s, const Dev& d, int blocks) {

@@ -44,6 +44,7 @@ struct Dev {
     float* pw = nullptr;
     int* key = nullptr;
     int* sorted = nullptr;
+    int* sort_tmp = nullptr;       // scratch of the large bins' in-block sort (same offsets as sorted)
     int* nbr = nullptr;            // slot-major: nbr[k*N + i]
     uint8_t* nnb = nullptr;
     int* rlist = nullptr;
@@ -54,7 +55,7 @@ struct Dev {
     int* cursor = nullptr;
     int* tilesum = nullptr;
     int* tileofs = nullptr;
-    double* psum = nullptr;        // FIRE power per move block
+    double2* psum = nullptr;       // FIRE power and its sum of magnitudes per move block
     double* pser = nullptr;        // serial FIRE power per volume
 };
 

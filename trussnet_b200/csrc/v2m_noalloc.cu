@@ -9,16 +9,20 @@
 // streams. Such a caller hands in its own input and output buffers; the only
 // other memory this entry point touches is the scratch below.
 //
-// Scratch: a file-scope __device__ array of kBins + 1 bin counters (and as many
-// scatter cursors) plus the scan's tile sums, for at most
-// V2M_NOALLOC_MAX_BINS = 2^20 bins: about 8 MB, held by every GPU that loads
-// the library until the process exits. Host code must not use the array's name
-// as a device address (on the host it is only a stand-in): the address comes
-// from cudaGetSymbolAddress, taken once per device, with that device current,
-// on the first call made on it. Every call shares the array and leaves its
-// contents behind; the counters are cleared at the start of each call. Calls
-// that overlap on the GPU (two streams, or two host threads on one device)
-// race on the array and give wrong results: serialize them.
+// Scratch: a file-scope __device__ array holding kBins + 1 bin counters (and as
+// many scatter cursors), the scan's tile sums and an id segment of kMaxKeys
+// entries (the in-bin sort of crowded bins): at most V2M_NOALLOC_MAX_BINS = 2^20
+// bins and V2M_NOALLOC_MAX_KEYS = 2^22 keys, about 24 MB, held by every GPU that
+// loads the library until the process exits. Host code must not use the array's
+// name as a device address (on the host it is only a stand-in): the address
+// comes from cudaGetSymbolAddress, taken once per device, with that device
+// current, on the first call made on it. A cudaDeviceReset of a device discards
+// its copy of the array, and the address cached for it is then stale: do not
+// call this entry point on that device again in the same process. Every call
+// shares the array and leaves its contents behind; the counters and the error
+// flag are cleared at the start of each call. Calls that overlap on the GPU (two
+// streams, or two host threads on one device) race on the array and give wrong
+// results: serialize them.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -26,10 +30,15 @@
 #include <string>
 
 #include "../../include/v2m_cuda.h"
+#include "v2m_binsort.cuh"
 
 namespace v2m_na {
 
+using v2m::kBinSortThreads;
+using v2m::kSmallBin;
+
 constexpr int kBins = V2M_NOALLOC_MAX_BINS;
+constexpr int kMaxKeys = V2M_NOALLOC_MAX_KEYS;
 constexpr int kTile = 1024;
 constexpr int kTiles = (kBins + 1 + kTile - 1) / kTile;
 constexpr int kThreads = 256;
@@ -41,6 +50,7 @@ struct Scratch {
     int tile[kTiles];
     int tile_ofs[kTiles];
     int err;
+    int ids[kMaxKeys];   // scratch of the in-bin sort of bins above kSmallBin ids (same offsets as sorted)
 };
 
 static __device__ __align__(256) Scratch g_scratch;
@@ -159,21 +169,36 @@ __global__ void k_scatter(Scratch* sc, const int* __restrict__ key, int n, int n
     }
 }
 
-// ascending ids within each bin: the stable order
-__global__ void k_bin_order(const int* __restrict__ cstart, int nbins, int* __restrict__ sorted) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nbins) {
-        return;
-    }
-    const int s0 = cstart[e], s1 = cstart[e + 1];
-    for (int a = s0 + 1; a < s1; ++a) {
-        const int x = sorted[a];
-        int b = a - 1;
-        while (b >= s0 && sorted[b] > x) {
-            sorted[b + 1] = sorted[b];
-            --b;
+// Ascending ids within each bin (the stable order): a bin of at most kSmallBin
+// ids on one thread, larger bins by the whole block over the scratch's id
+// segment at the same offsets -- linear in the bin's size, so a caller's keys
+// that crowd into one bin cannot stall a thread.
+__global__ void __launch_bounds__(kBinSortThreads) k_bin_order(Scratch* sc, const int* __restrict__ cstart, int nbins,
+                                                               int* __restrict__ sorted) {
+    __shared__ v2m::BinSortSmem sm;
+    __shared__ int big[kBinSortThreads];
+    __shared__ int nbig;
+    for (int base = blockIdx.x * kBinSortThreads; base < nbins; base += gridDim.x * kBinSortThreads) {
+        if (threadIdx.x == 0) {
+            nbig = 0;
         }
-        sorted[b + 1] = x;
+        __syncthreads();
+        const int e = base + threadIdx.x;
+        if (e < nbins) {
+            const int s0 = cstart[e], c = cstart[e + 1] - s0;
+            if (c <= kSmallBin) {
+                v2m::small_bin_sort(sorted + s0, c);
+            } else {
+                big[atomicAdd(&nbig, 1)] = e;
+            }
+        }
+        __syncthreads();
+        const int nb = nbig;
+        for (int q = 0; q < nb; ++q) {
+            const int s0 = cstart[big[q]], s1 = cstart[big[q] + 1];
+            v2m::block_bin_sort(sorted + s0, sc->ids + s0, s1 - s0, sm);
+        }
+        __syncthreads();
     }
 }
 
@@ -206,8 +231,13 @@ extern "C" {
 
 int v2m_bin_sort_noalloc(const int32_t* key, int64_t n, int64_t nbins, int32_t* sorted, int32_t* cstart,
                          void* stream) {
-    if (n < 0 || n > 0x7FFFFFFF || nbins < 1) {
-        g_err = "v2m_bin_sort_noalloc: n must be in [0, 2^31) and nbins >= 1";
+    if (n < 0 || nbins < 1) {
+        g_err = "v2m_bin_sort_noalloc: n must be >= 0 and nbins >= 1";
+        return V2M_ERR_ARG;
+    }
+    if (n > V2M_NOALLOC_MAX_KEYS) {
+        g_err = "v2m_bin_sort_noalloc: " + std::to_string(n) + " keys exceed the fixed scratch of " +
+                std::to_string(V2M_NOALLOC_MAX_KEYS) + " keys";
         return V2M_ERR_ARG;
     }
     if (nbins > V2M_NOALLOC_MAX_BINS) {
@@ -242,7 +272,7 @@ int v2m_bin_sort_noalloc(const int32_t* key, int64_t n, int64_t nbins, int32_t* 
     k_apply<<<ntiles, kThreads, 0, s>>>(sc, nb, cstart);
     if (nn > 0) {
         k_scatter<<<(nn + kThreads - 1) / kThreads, kThreads, 0, s>>>(sc, key, nn, nb, sorted);
-        k_bin_order<<<(nb + kThreads - 1) / kThreads, kThreads, 0, s>>>(cstart, nb, sorted);
+        k_bin_order<<<(nb + kBinSortThreads - 1) / kBinSortThreads, kBinSortThreads, 0, s>>>(sc, cstart, nb, sorted);
     }
     int err = 0;
     cudaError_t e = cudaGetLastError();

@@ -90,7 +90,8 @@ struct VolCtl {
     int iters;         // RelaxStats.iters
     float last_move, last_p99;
     double power;      // last FIRE power sum
-    int nhalf_last, nrefresh_last, stop_reason, pad0;
+    int nhalf_last, nrefresh_last, stop_reason;
+    int serial_sums;   // iterations whose FIRE power was within rounding of zero (summed serially)
     // accumulators of the current iteration (cleared by the control stage)
     int hist[32];
     unsigned int maxbits;

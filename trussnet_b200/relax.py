@@ -24,12 +24,12 @@ from typing import Sequence
 import numpy as np
 
 from . import _lib
-from .types import (ARR, V2M_K, Grid, GridView, Nodes, NodesView, RelaxParams, RelaxParamsC, RelaxStats,
+from .types import (ARR, V2M_K, Grid, GridParams, GridParamsC, GridView, Nodes, NodesView, RelaxParams, RelaxParamsC, RelaxStats,
                     RelaxStatsC)
 
 _ARR_DTYPE = {"key": np.int32, "sorted": np.int32, "cstart": np.int32, "Ps": np.float32, "nbr": np.int32,
               "nnb": np.int32, "F": np.float32, "hn": np.float32, "mv": np.float32, "V": np.float32, "pw": np.float32,
-              "P0": np.float32, "hist": np.int32, "P": np.float32, "typ": np.uint8, "part": np.uint16}
+              "P0": np.float32, "hist": np.int32, "serial_sums": np.int32, "P": np.float32, "typ": np.uint8, "part": np.uint16}
 _PER_NODE = {"key": 1, "sorted": 1, "Ps": 4, "nbr": V2M_K, "nnb": 1, "F": 4, "hn": 1, "mv": 1, "V": 3, "pw": 1,
              "P0": 3, "P": 3, "typ": 1, "part": 2}
 
@@ -90,6 +90,66 @@ def seed_cl(g: Grid, prm: RelaxParams, device: int = -1) -> tuple[Nodes, np.ndar
     finally:
         L.v2m_seed_free(h)
     return nd, part3
+
+
+def grid_cl(L: np.ndarray, vs=(1.0, 1.0, 1.0), prm: GridParams | None = None, device: int = -1) -> Grid:
+    """tn::build_grid_cpu of label volume L (uint16 [nz, ny, nx], x fastest) on a
+    CUDA device, bit for bit: bricks, slots, smoothed indicators, sizing field
+    and size grades (the returned grid carries grade, ready for seed_cl)."""
+    lib = _lib.load()
+    L = np.ascontiguousarray(L, np.uint16)
+    nz, ny, nx = L.shape
+    prm = prm or GridParams()
+    pc = GridParamsC()
+    for f in ("sigma", "sigma_thin", "thin_lo", "thin_hi", "thick", "thin_floor", "preserve", "sigma_curv", "hbase",
+              "hmin", "hmax", "K", "g"):
+        setattr(pc, f, float(getattr(prm, f)))
+    hl = np.ascontiguousarray(prm.hlab, np.float32)
+    pc.hlab = hl.ctypes.data if hl.size else None
+    pc.nhlab = int(hl.size)
+    vsa = np.asarray(vs, np.float32)
+    h = C.c_void_p()
+    _lib.check(lib.v2m_grid_build_cuda(L.ctypes.data, nx, ny, nz, vsa.ctypes.data, C.byref(pc), device, C.byref(h)))
+    try:
+        gv = GridView()
+        _lib.check(lib.v2m_grid_result_view(h, C.byref(gv)))
+        g = Grid.from_view(gv)
+        R = C.c_int32()
+        _lib.check(lib.v2m_grid_result_info(h, None, C.byref(R), None, None))
+        g.R = R.value
+    finally:
+        lib.v2m_grid_free(h)
+    return g
+
+
+def validate_lists(nbr: np.ndarray, nnb: np.ndarray, pi: np.ndarray, pj: np.ndarray) -> str:
+    """Host-side check of truss lists (v2m_validate_lists; no device): lengths,
+    ids in range, no self-edges or repeats, and (distance, id) order from the
+    positions the lists were built from (pi: each node's position at its build,
+    pj: the bin-order snapshot's). Returns "" when valid, else the first
+    violation."""
+    L = _lib.load()
+    n = int(nnb.size)
+    nbr = np.ascontiguousarray(nbr, np.int32).reshape(-1)
+    nnb = np.ascontiguousarray(nnb, np.int32)
+    pi = np.ascontiguousarray(pi, np.float32).reshape(-1)
+    pj = np.ascontiguousarray(pj, np.float32).reshape(-1)
+    if nbr.size != n * V2M_K or pi.size != 3 * n or pj.size != 3 * n:
+        raise ValueError("validate_lists: array sizes do not match the node count")
+    rep = C.create_string_buffer(512)
+    rc = L.v2m_validate_lists(n, nbr.ctypes.data, nnb.ctypes.data, pi.ctypes.data, pj.ctypes.data, rep, len(rep))
+    if rc not in (0, _lib.V2M_ERR_KERNEL):
+        _lib.check(rc)
+    return rep.value.decode()
+
+
+def build_positions(Ps: np.ndarray, sorted_ids: np.ndarray) -> np.ndarray:
+    """Each node's position in the bin-order snapshot (Ps, 4 floats per slot,
+    slot s holding node sorted_ids[s]), in node order (3 floats per node)."""
+    n = sorted_ids.size
+    out = np.zeros((n, 3), np.float32)
+    out[sorted_ids] = Ps.reshape(-1, 4)[:n, :3]
+    return out
 
 
 class Session:
@@ -167,6 +227,8 @@ class Session:
             count = self.nkeys[vol] + 1
         elif name == "hist":
             count = 34
+        elif name == "serial_sums":
+            count = 1
         else:
             count = self.n[vol] * _PER_NODE[name]
         out = np.zeros(max(count, 1), dt)
@@ -181,6 +243,11 @@ class Session:
         nbr = np.ascontiguousarray(nbr, np.int32)
         nnb = np.ascontiguousarray(nnb, np.int32)
         _lib.check(self.L.v2m_session_write_lists(self.h, vol, nbr.ctypes.data, nnb.ctypes.data))
+
+    def validate_lists(self, vol: int = 0) -> str:
+        """The session's current truss lists through validate_lists ("" when valid)."""
+        return validate_lists(self.read("nbr", vol), self.read("nnb", vol), self.read("P0", vol),
+                              build_positions(self.read("Ps", vol), self.read("sorted", vol)))
 
     def timed_runs(self, runs: int, graph: bool = True, time_force: bool = False) -> float:
         """Device milliseconds of `runs` whole relaxations from the seeds (CUDA events)."""

@@ -299,8 +299,9 @@ def batch(nvol=64, seed=0, dmin=32, dmax=160, lmin=2, lmax=18, scale=1.55):
 def params_for(name: str) -> RelaxParams:
     """Relaxation parameters of each workload (reference defaults otherwise)."""
     if name == "sphere64":
-        # 200 FP32 iterations, step dt = 0.2 (FIRE's first step sqrt(0.2)), no early stop
-        return RelaxParams(max_iters=200, dt=0.2, dptol=0.0)
+        # 200 FP32 iterations, step dt = 0.2 (FIRE's first step sqrt(0.2)), no early stop, and a
+        # fixed edge list: the first build's truss lists for the whole run (rebuild_policy 2)
+        return RelaxParams(max_iters=200, dt=0.2, dptol=0.0, rebuild_policy=2)
     if name == "shells256":
         return RelaxParams(max_iters=500, dptol=0.0)
     if name == "tpm182":

@@ -22,7 +22,7 @@ V2M_NOLAB = 0xFFFF
 V2M_INTERIOR, V2M_INTERFACE, V2M_JUNCTION, V2M_CORNER = 0, 1, 2, 3
 
 # internal arrays (V2M_ARR_* of include/v2m_cuda.h)
-ARR = dict(key=1, sorted=2, cstart=3, Ps=4, nbr=5, nnb=6, F=7, hn=8, mv=9, V=10, pw=11, P0=12, hist=13,
+ARR = dict(key=1, sorted=2, cstart=3, Ps=4, nbr=5, nnb=6, F=7, hn=8, mv=9, V=10, pw=11, P0=12, hist=13, serial_sums=14,
            P=20, typ=21, part=22)
 
 
@@ -81,7 +81,7 @@ class RelaxParams:
     verbose: bool = False
     h_mode: int = 0          # 0: nearest-voxel h (reference), 1: trilinear h
     rebuild_div: int = 0     # 0: V2M_REBUILD_DIV or 300
-    rebuild_policy: int = 0  # 0: reference Verlet trigger, 1: max |dp| since build > 0.1 h
+    rebuild_policy: int = 0  # 0: reference Verlet trigger, 1: max |dp| since build > 0.1 h, 2: fixed lists
 
     def to_c(self) -> RelaxParamsC:
         c = RelaxParamsC()
@@ -112,6 +112,32 @@ class RelaxStats:
     @classmethod
     def from_c(cls, c: RelaxStatsC) -> "RelaxStats":
         return cls(**{f.name: getattr(c, f.name) for f in fields(cls)})
+
+
+class GridParamsC(C.Structure):
+    """v2m_grid_params: tn::GridParams (src/v2m_grid.h:21-43), label input."""
+    _fields_ = [(f, C.c_float) for f in ("sigma", "sigma_thin", "thin_lo", "thin_hi", "thick", "thin_floor", "preserve",
+                                         "sigma_curv", "hbase", "hmin", "hmax", "K", "g")] + \
+        [("hlab", C.c_void_p), ("nhlab", C.c_int32)]
+
+
+@dataclass
+class GridParams:
+    """tn::GridParams (src/v2m_grid.h:21-43): the reference's defaults."""
+    sigma: float = 1.0
+    sigma_thin: float = 0.35
+    thin_lo: float = 2.0
+    thin_hi: float = 4.0
+    thick: float = 0.0
+    thin_floor: float = 0.5
+    preserve: float = 0.0
+    sigma_curv: float = 2.0
+    hbase: float = 0.0
+    hmin: float = 0.0
+    hmax: float = 0.0
+    K: float = 3.0
+    g: float = 0.3
+    hlab: tuple = ()
 
 
 @dataclass
