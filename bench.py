@@ -12,6 +12,7 @@ trigger. One step = one whole relaxation from the seeds (first list build +
   python bench.py --workload batch64   (the batched form against sequential runs)
   python bench.py --workload adjoint   (the unroll's backward against its forward)
   python bench.py --workload seed_tpm182   (seeding on the device against seed_cpu)
+  python bench.py --workload grid_shells256   (the grid build on the device against build_grid_cpu)
 
 --workload batch64: 64 independent volumes of seeded sizes 32^3..160^3 with
 2..18 nested-shell labels (~4M nodes in all), 200 FIRE iterations each. One
@@ -222,12 +223,43 @@ def run_seed_reference(args):
           flush=True)
 
 
+def run_grid_reference(args):
+    """The reference arm of grid_shells256: build_grid_cpu on the host cores,
+    W + K whole builds of the same labels."""
+    from oracle.ref import RefLib, available
+    if not available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libv2m_ref.so is not built"}))
+        return
+    L, gp = grid_workload()
+    lib = RefLib()
+    for _ in range(args.warmup):
+        lib.build_grid_p(L, prm=gp)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        lib.build_grid_p(L, prm=gp)
+        ts.append(time.perf_counter() - t0)
+    dt = statistics.mean(ts)
+    v = L.size / dt
+    print(json.dumps({"metric": "grid build voxels/s", "value": v, "unit": "voxels/s", "n_gpus": args.gpus,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                      "impl": "reference", "config": {"workload": "grid_shells256", "voxels": int(L.size)},
+                      "cpu_baseline": {"value": v, "unit": "voxels/s", "cores": _cores(), "kind": "reference",
+                                       "sample": f"build_grid_cpu, whole builds, {dt:.2f} s each"},
+                      "e2e": {"value": v, "unit": "voxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+          flush=True)
+
+
 def run_reference(args):
     world, rank, _ = dist_setup(args)
     if rank != 0:
         return
     if args.workload == "seed_tpm182":
         run_seed_reference(args)
+        return
+    if args.workload == "grid_shells256":
+        run_grid_reference(args)
         return
     if args.workload in ("batch64", "adjoint"):
         why = {"batch64": "the reference relaxes one volume per call; its arm is the default workload's",
@@ -277,12 +309,20 @@ def pinned_copy(a: np.ndarray) -> np.ndarray:
 def run_batch(args):
     """The batched form (64 volumes, one graph-captured session) against the same
     relaxations run one volume at a time with plain launches; device time by CUDA
-    events on each session's stream. One GPU."""
+    events on each session's stream. Under torchrun (N > 1) the volumes are
+    sharded over the ranks by node count (shard.assign_volumes: no collective
+    while the loops run), each rank relaxing its share in one session on its
+    GPU; the step time is the max over ranks and the end-to-end leg goes
+    through shard.relax_batch_distributed (every rank ends with every volume)."""
     import torch
     from trussnet_b200 import Session, synth
+    from trussnet_b200.shard import assign_volumes
     world, rank, local = dist_setup(args)
-    if world > 1 and rank != 0:
-        return
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     vols = synth.batch()
     prm = synth.params_for("batch64")
     if args.iters:
@@ -292,57 +332,89 @@ def run_batch(args):
     nodes = [nd for _, nd in vols]
     prms = [prm] * len(vols)
     n = sum(nd.size() for nd in nodes)
-    sess = Session(grids, prms, nodes, device=local)
+    mine = assign_volumes([nd.size() for nd in nodes], world)[rank]
+
+    def barrier():
+        torch.cuda.synchronize(local)
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    sess = Session([grids[v] for v in mine], [prm] * len(mine), [nodes[v] for v in mine], device=local)
     tune = sess.autotune()
     sess.timed_runs(args.warmup, graph=True)
     sess.clear_counters()
-    torch.cuda.synchronize(local)
+    barrier()
     clk = ClockSampler(local)
     clk.start()
     ms = sess.timed_runs(args.steps, graph=True)
     clocks = clk.stop()
+    barrier()
     cnt = sess.counters()
     sess.close()
-    step_ms = ms / args.steps
-    # the same relaxations, one volume at a time, plain launches (each session warmed once)
-    seq_ms = 0.0
-    for g, nd in vols:
-        with Session(g, prm, nd, device=local) as s1:
-            s1.timed_runs(1, graph=False)
-            seq_ms += s1.timed_runs(1, graph=False)
-    torch.cuda.synchronize(local)
-    # end to end through the C ABI: one batch call against one relax_cl call per
-    # volume (host buffers, every upload, set-up and read-back inside), same results
-    from trussnet_b200 import relax_cl, relax_cl_batch
+    step_ms = max_over_ranks(ms / args.steps)
+    seq_ms = None
     e2e = {}
-    for k in range(2):   # the first pass warms the module and the allocator
-        outs_b = [nd.copy() for nd in nodes]
-        t0 = time.perf_counter()
-        relax_cl_batch(grids, prms, outs_b, device=local)
-        tb = time.perf_counter() - t0
-        outs_s = [nd.copy() for nd in nodes]
-        t0 = time.perf_counter()
-        for g, o in zip(grids, outs_s):
-            relax_cl(g, prm, o, device=local)
-        ts_ = time.perf_counter() - t0
-        e2e = {"batch_call_s": tb, "sequential_calls_s": ts_, "speedup": ts_ / tb}
-    e2e["identical"] = all(np.array_equal(a.P.view(np.uint32), b.P.view(np.uint32)) and
-                           np.array_equal(a.typ, b.typ) for a, b in zip(outs_b, outs_s))
-    line = {"metric": "batched relax node-iters/s, 64 volumes", "value": n * iters / (step_ms / 1e3), "unit": UNIT,
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "batch64: 64 volumes 32^3..160^3, 2..18 nested-shell labels, h in [1.55, 6.2] "
-                                   "vox, 200 FIRE iterations, dptol 0", "volumes": len(vols), "nodes": n,
-                       "min_nodes": min(nd.size() for nd in nodes), "max_nodes": max(nd.size() for nd in nodes),
-                       "iters_per_step": iters, "autotune": tune.strip().splitlines()[-1] if tune else None},
-            "sequential_plain_ms": seq_ms, "batched_speedup": seq_ms / step_ms,
-            "e2e": {"value": n * iters / e2e["batch_call_s"], "unit": UNIT,
-                    "h2d_bytes_per_step": int(sum(g.nbytes() for g in grids) + sum(nd.nbytes() for nd in nodes)),
-                    "d2h_bytes_per_step": int(sum(nd.P.nbytes + nd.typ.nbytes + nd.part.nbytes for nd in nodes)),
-                    "batch_call_s": e2e["batch_call_s"], "sequential_relax_cl_calls_s": e2e["sequential_calls_s"],
-                    "speedup": e2e["speedup"], "results_identical": e2e["identical"]},
-            "clocks": clocks, "gpu_launches": int(cnt["launches"])}
-    print(json.dumps(line), flush=True)
+    from trussnet_b200 import relax_cl, relax_cl_batch
+    if world == 1:
+        # the same relaxations, one volume at a time, plain launches (each session warmed once)
+        seq_ms = 0.0
+        for g, nd in vols:
+            with Session(g, prm, nd, device=local) as s1:
+                s1.timed_runs(1, graph=False)
+                seq_ms += s1.timed_runs(1, graph=False)
+        torch.cuda.synchronize(local)
+        # end to end through the C ABI: one batch call against one relax_cl call per
+        # volume (host buffers, every upload, set-up and read-back inside), same results
+        for k in range(2):   # the first pass warms the module and the allocator
+            outs_b = [nd.copy() for nd in nodes]
+            t0 = time.perf_counter()
+            relax_cl_batch(grids, prms, outs_b, device=local)
+            tb = time.perf_counter() - t0
+            outs_s = [nd.copy() for nd in nodes]
+            t0 = time.perf_counter()
+            for g, o in zip(grids, outs_s):
+                relax_cl(g, prm, o, device=local)
+            ts_ = time.perf_counter() - t0
+            e2e = {"batch_call_s": tb, "sequential_calls_s": ts_, "speedup": ts_ / tb}
+        e2e["identical"] = all(np.array_equal(a.P.view(np.uint32), b.P.view(np.uint32)) and
+                               np.array_equal(a.typ, b.typ) for a, b in zip(outs_b, outs_s))
+    else:
+        from trussnet_b200.shard import relax_batch_distributed
+        for k in range(2):
+            outs_b = [nd.copy() for nd in nodes]
+            barrier()
+            t0 = time.perf_counter()
+            relax_batch_distributed(grids, prms, outs_b, device=local)
+            torch.cuda.synchronize(local)
+            tb = max_over_ranks(time.perf_counter() - t0)
+            e2e = {"batch_call_s": tb}
+    if rank == 0:
+        line = {"metric": "batched relax node-iters/s, 64 volumes", "value": n * iters / (step_ms / 1e3),
+                "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+                "higher_is_better": True, "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "batch64: 64 volumes 32^3..160^3, 2..18 nested-shell labels, h in [1.55, 6.2] "
+                                       "vox, 200 FIRE iterations, dptol 0", "volumes": len(vols), "nodes": n,
+                           "min_nodes": min(nd.size() for nd in nodes), "max_nodes": max(nd.size() for nd in nodes),
+                           "iters_per_step": iters, "autotune": tune.strip().splitlines()[-1] if tune else None,
+                           "parallelism": (f"volumes sharded over {world} ranks by node count (LPT), no collective "
+                                           f"in the loop" if world > 1 else "one session")},
+                "sequential_plain_ms": seq_ms, "batched_speedup": (seq_ms / step_ms) if seq_ms else None,
+                "e2e": {"value": n * iters / e2e["batch_call_s"], "unit": UNIT,
+                        "h2d_bytes_per_step": int(sum(g.nbytes() for g in grids) + sum(nd.nbytes() for nd in nodes)),
+                        "d2h_bytes_per_step": int(sum(nd.P.nbytes + nd.typ.nbytes + nd.part.nbytes for nd in nodes)),
+                        **{k: v for k, v in e2e.items()}},
+                "clocks": clocks, "gpu_launches": int(cnt["launches"])}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
 
 
 def adjoint_leg(local, steps=3, warmup=3):
@@ -447,6 +519,68 @@ def run_seed(args):
             "e2e": {"value": n / dt, "unit": "seeds/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "cpu_baseline": cb, "results_identical": same, "clocks": clocks}
     print(json.dumps(line), flush=True)
+
+
+def grid_workload():
+    """The shells256 label volume (256^3, six noisy shells) and grid parameters
+    giving its h range: hbase 4, hmin 1.5, hmax 6 voxels."""
+    from trussnet_b200 import GridParams, synth
+    g, _ = synth.shells(seed=0)
+    return g.L, GridParams(hbase=4.0, hmin=1.5, hmax=6.0)
+
+
+def run_grid(args):
+    """The grid build on the device (grid_cl: labels from host memory in, the
+    grid's arrays to host memory out, the whole call timed) against the
+    reference's build_grid_cpu on the same labels and parameters; results
+    compared bit for bit."""
+    world, rank, local = dist_setup(args)
+    if rank != 0:
+        return
+    import torch
+    from trussnet_b200 import grid_cl
+    torch.cuda.set_device(local)
+    L, gp = grid_workload()
+    nv = L.size
+    for _ in range(args.warmup):
+        gd = grid_cl(L, (1.0, 1.0, 1.0), gp, device=local)
+    clk = ClockSampler(local)
+    clk.start()
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        gd = grid_cl(L, (1.0, 1.0, 1.0), gp, device=local)
+        ts.append(time.perf_counter() - t0)
+    clocks = clk.stop()
+    dt = statistics.mean(ts)
+    cb, same = None, None
+    if not args.no_cpu_baseline:
+        from oracle.ref import RefLib, available
+        if available():
+            t0 = time.perf_counter()
+            gr = RefLib().build_grid_p(L, prm=gp)
+            tc = time.perf_counter() - t0
+            same = all(np.array_equal(getattr(gd, a), getattr(gr, a)) for a in
+                       ("bl_cnt", "bl_lab", "bl_slot", "phi", "h", "grade"))
+            cb = {"value": nv / tc, "unit": "voxels/s", "cores": _cores(), "kind": "reference",
+                  "sample": f"build_grid_cpu on the same labels and parameters, one whole build, {tc:.2f} s"}
+    line = {"metric": "grid build voxels/s", "value": nv / dt, "unit": "voxels/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "grid_shells256: the shells256 label volume (256^3, six noisy shells), "
+                                   "hbase 4, hmin 1.5, hmax 6 voxels, the reference's other GridParams defaults",
+                       "voxels": int(nv), "slots": int(gd.phi.size // 512),
+                       "timed": "whole grid_cl calls from host labels to host grid arrays"},
+            "e2e": {"value": nv / dt, "unit": "voxels/s", "h2d_bytes_per_step": int(L.nbytes),
+                    "d2h_bytes_per_step": int(gd.nbytes() + gd.grade.nbytes - L.nbytes)},
+            "cpu_baseline": cb, "results_identical": same, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
+def _cores():
+    cores = os.cpu_count() or 1
+    cap = int(os.environ.get("V2M_OMP_MAX_THREADS", "64"))
+    return min(cores, cap) if cap > 0 else cores
 
 
 def run_cuda(args):
@@ -572,6 +706,8 @@ def main():
         run_adjoint(args)
     elif args.workload == "seed_tpm182":
         run_seed(args)
+    elif args.workload == "grid_shells256":
+        run_grid(args)
     else:
         run_cuda(args)
 

@@ -182,6 +182,19 @@ int v2m_grid_result_info(const v2m_grid_result* r, float* hbase, int32_t* R, int
 void v2m_grid_free(v2m_grid_result* r);
 
 /*
+ * The pipeline's points mode on the device (run_pipeline with stop_after_relax,
+ * src/v2m_pipeline.cpp:424-565; `v2mesh --mode points`): the label volume is
+ * uploaded once, its grid built (v2m_grid_build_cuda), seeded (v2m_seed_cuda)
+ * and relaxed (v2m_relax_cuda) with every stage reading the previous one's
+ * device arrays, and the relaxed nodes are copied back once: *n nodes in *out
+ * (read with v2m_seed_copy: P, lab, typ, part, part3; freed with
+ * v2m_seed_free), bit for bit build_grid_cpu -> seed_cpu -> relax_cpu. st may
+ * be NULL.
+ */
+int v2m_points_cuda(const uint16_t* L, int32_t nx, int32_t ny, int32_t nz, const float* vs, const v2m_grid_params* gp,
+                    const v2m_relax_params* prm, int device, v2m_seed_result** out, int64_t* n, v2m_relax_stats* st);
+
+/*
  * Many independent volumes in one set of launches (one per stage for all of
  * them), the iteration loop captured in a CUDA graph. Each volume keeps its own
  * hash, lists, FIRE state and stop / rebuild decisions, so volume v's result is

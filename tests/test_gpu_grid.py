@@ -22,11 +22,11 @@ pytestmark = pytest.mark.gpu
 
 
 def thin_layers(dim=32, nlab=20):
-    """Parallel one- and two-voxel layers of nlab labels: more labels within
-    R of a brick than a brick lists (the overflow count)."""
+    """Parallel one-voxel layers of nlab labels: a brick's box (8 + 2R + 1 = 21
+    voxels wide) meets more labels than a brick lists (the overflow count)."""
     L = np.zeros((dim, dim, dim), np.uint16)
     x = np.arange(dim)
-    lab = (x // 1.5).astype(np.int64) % nlab + 1
+    lab = x % nlab + 1
     L[:, :, :] = lab[None, None, :].astype(np.uint16)
     L[:2] = 0
     return L
@@ -110,3 +110,38 @@ def test_device_chain_equals_reference_chain(ref, cuda_lib):
     assert (st_dev.iters, st_dev.rebuilds) == (st_ref.iters, st_ref.rebuilds)
     for f in ("P", "typ", "part"):
         assert first_diff(getattr(nd_dev, f), getattr(nd_ref, f)) is None, f
+
+
+@pytest.mark.parametrize("name", ["phantom", "noise"])
+def test_points_mode_on_device_equals_reference(name, ref, cuda_lib):
+    """points_cl (v2m_points_cuda): one upload of the labels, grid build,
+    seeding and relaxation from device arrays, one copy back -- equals the
+    reference pipeline's points mode (build_grid_cpu -> seed_cpu -> relax_cpu)."""
+    from trussnet_b200 import points_cl
+    L, vs, p = VOLUMES[name]()
+    prm = RelaxParams(max_iters=40)
+    g_ref, nd_ref = ref.build_and_seed(L, sigma=p.sigma, hbase=p.hbase, hmin=p.hmin, hmax=p.hmax, prm=prm)
+    part3_ref = nd_ref.part3.copy()
+    st_ref = ref.relax_cpu(g_ref, prm, nd_ref)
+    nd, part3, st = points_cl(L, vs, p, prm)
+    assert nd.size() == nd_ref.size()
+    for f in ("P", "lab", "typ", "part"):
+        assert first_diff(getattr(nd, f), getattr(nd_ref, f)) is None, f
+    assert np.array_equal(part3, part3_ref)
+    assert (st.iters, st.rebuilds, st.fire_resets) == (st_ref.iters, st_ref.rebuilds, st_ref.fire_resets)
+
+
+def test_pyv2mesh_points_call(cuda_lib):
+    """trussnet_b200.pyv2mesh.points: v2mesh.points' call (vol[x, y, z], size
+    and relaxation options, keys node / label / type / partner / info) on the
+    device path; equals points_cl on the transposed volume."""
+    from trussnet_b200 import points_cl, pyv2mesh
+    L = cases.noise_labels()
+    vol = L.transpose(2, 1, 0)   # vol[x, y, z]
+    out = pyv2mesh.points(vol, size=2.0, hmin=1.2, hmax=3.0, iters=30)
+    nd, part3, st = points_cl(L, (1.0, 1.0, 1.0), GridParams(hbase=2.0, hmin=1.2, hmax=3.0), RelaxParams(max_iters=30))
+    assert np.array_equal(out["node"].astype(np.float32), nd.P)
+    assert np.array_equal(out["type"], nd.typ.astype(np.int64)) and np.array_equal(out["label"], nd.lab)
+    partner = out["partner"]
+    assert partner.shape == (nd.size(), 3) and (partner[nd.typ == 0] == -1).all()
+    assert out["info"]["iters"] == st.iters == 30

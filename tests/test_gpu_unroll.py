@@ -133,3 +133,17 @@ def test_autograd_function(cuda_lib):
     assert torch.equal(x.grad, gx0)
     assert torch.allclose(G.grad, gG1 + gG2, rtol=0, atol=0)
     assert float(L) == pytest.approx(u.loss(xK, Gt), rel=0, abs=0)
+
+
+def test_sizing_by_gradient_lowers_the_loss(cuda_lib):
+    """The adjoint's consumer: descent on the sizing grid through the K-step
+    unroll (adjoint.optimize_sizing) lowers the edge loss after K steps; the
+    same for descent on the starting positions (adjoint.optimize_positions)."""
+    from trussnet_b200.adjoint import optimize_positions, optimize_sizing
+    u, x0, Gt, nd, nbr, nnb, G, cs = setup(48, 16, 12, 5)
+    G1, lg = optimize_sizing(u, x0, Gt, steps=12, step=0.02)
+    assert min(lg[1:]) < lg[0] and lg[-1] < 0.99 * lg[0], lg
+    assert float(G1.min()) >= float(Gt.min()) and float(G1.max()) <= float(Gt.max())
+    x1, lx = optimize_positions(u, x0, Gt, steps=12, step=0.02)
+    assert lx[-1] < lx[0], lx
+    u.close()

@@ -7,9 +7,9 @@ fangq/trussnet src/v2m_gpu.h, src/v2m_particles.h) plus seeded synthetic inputs.
 """
 from .types import (V2M_CORNER, V2M_INTERFACE, V2M_INTERIOR, V2M_JUNCTION, V2M_K, V2M_NOLAB, Grid, GridParams,
                     Nodes, RelaxParams, RelaxStats)
-from .relax import Session, device_count, grid_cl, relax_cl, relax_cl_batch, seed_cl, validate_lists
+from .relax import Session, device_count, grid_cl, points_cl, relax_cl, relax_cl_batch, seed_cl, validate_lists
 from ._lib import V2mError
 
 __all__ = ["Grid", "Nodes", "RelaxParams", "RelaxStats", "Session", "relax_cl", "relax_cl_batch", "seed_cl", "device_count",
-           "validate_lists", "grid_cl", "GridParams",
+           "validate_lists", "grid_cl", "points_cl", "GridParams",
            "V2mError", "V2M_INTERIOR", "V2M_INTERFACE", "V2M_JUNCTION", "V2M_CORNER", "V2M_NOLAB", "V2M_K"]

@@ -28,7 +28,7 @@ EXPORTS = [
     "v2m_unroll_last_error", "v2m_session_autotune", "v2m_session_shapes",
     "v2m_session_profile_stages", "v2m_session_queue_sizes", "v2m_bin_sort_noalloc", "v2m_bin_sort_noalloc_error",
     "v2m_validate_lists", "v2m_grid_params_default", "v2m_grid_build_cuda", "v2m_grid_result_view",
-    "v2m_grid_result_info", "v2m_grid_free",
+    "v2m_grid_result_info", "v2m_grid_free", "v2m_points_cuda",
     "v2m_seed_cuda", "v2m_seed_copy", "v2m_seed_free",
 ]
 
@@ -87,6 +87,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.v2m_grid_build_cuda.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, C.c_int, vp]
         L.v2m_grid_result_view.argtypes = [vp, vp]
         L.v2m_grid_result_info.argtypes = [vp, vp, vp, vp, vp]
+        L.v2m_points_cuda.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, C.c_int, vp, vp, vp]
         L.v2m_grid_free.argtypes = [vp]
         L.v2m_grid_free.restype = None
         L.v2m_bin_sort_noalloc_error.restype = C.c_char_p

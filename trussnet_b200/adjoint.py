@@ -161,3 +161,53 @@ def unrolled_loss(x0, G, unroll):
     import sys
     mod = sys.modules[__name__]
     return mod.EdgeLoss.apply(mod.RelaxUnroll.apply(x0, G, unroll), G, unroll)
+
+
+def optimize_sizing(unroll, x0, G0, steps=20, step=0.05, hmin=None, hmax=None):
+    """Sizing by gradient: descent on the sizing grid G so that the nodes after
+    the K-step unroll from x0 make bars of their target lengths (the unroll's
+    edge loss, sum over list entries of (l_ij / h_ij - 1)^2). Each step
+    evaluates the loss and dL/dG by the hand-written adjoint (RelaxUnroll +
+    EdgeLoss), moves G by `step` times the largest grid value against the
+    gradient normalised by its largest magnitude, and clamps G to
+    [hmin, hmax] (default: G0's range). Returns (G, losses): the final grid
+    and the loss before each step and after the last."""
+    import torch
+    G = G0.detach().clone().contiguous()
+    lo = float(G0.min()) if hmin is None else float(hmin)
+    hi = float(G0.max()) if hmax is None else float(hmax)
+    scale = step * hi
+    losses = []
+    for _ in range(steps):
+        Gv = G.clone().requires_grad_(True)
+        L = unrolled_loss(x0, Gv, unroll)
+        L.backward()
+        losses.append(float(L))
+        g = Gv.grad
+        with torch.no_grad():
+            G = (G - scale * g / g.abs().max().clamp_min(1e-30)).clamp_(lo, hi).contiguous()
+    with torch.no_grad():
+        losses.append(float(unrolled_loss(x0, G, unroll)))
+    return G, losses
+
+
+def optimize_positions(unroll, x0, G, steps=20, step=0.05):
+    """Node positions by gradient: descent on the starting positions x0 of the
+    unroll (the relaxation's state fed to a mesh-quality optimiser) against
+    the same edge loss after K steps, each node moved by at most `step` times
+    its local grid spacing. Returns (x, losses)."""
+    import torch
+    x = x0.detach().clone().contiguous()
+    cell = float(min(unroll.cs))
+    losses = []
+    for _ in range(steps):
+        xv = x.clone().requires_grad_(True)
+        L = unrolled_loss(xv, G, unroll)
+        L.backward()
+        losses.append(float(L))
+        g = xv.grad
+        with torch.no_grad():
+            x = (x - step * cell * g / g.norm(dim=1).max().clamp_min(1e-30)).contiguous()
+    with torch.no_grad():
+        losses.append(float(unrolled_loss(x, G, unroll)))
+    return x, losses

@@ -1155,7 +1155,7 @@ __device__ __noinline__ float move_voxel(const DGrid& g, int hmode, float h, flo
 // ty0 is the type before the move; st is updated in place exactly where the
 // reference writes the node's arrays.
 template <bool kShape>
-__device__ __noinline__ float move_step(const DGrid& g, int hmode, float h, float* s, float maxstep, float snap,
+__device__ __forceinline__ float move_step(const DGrid& g, int hmode, float h, float* s, float maxstep, float snap,
                                         int voxmode, NodeState& st) {
     float p[3], q[3];
     p[0] = st.p[0];

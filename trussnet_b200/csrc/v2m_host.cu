@@ -70,6 +70,47 @@ void inject(const char* stage, int it = -1) {
     throw CudaError(std::string("injected fault at ") + stage + (it >= 0 ? " (iteration " + std::to_string(it) + ")" : ""));
 }
 
+// Host-side stage timing of a call (V2M_CUDA_PROFILE=1, the counterpart of the
+// reference's V2M_CL_PROFILE, src/v2m_gpu.cpp:250-258): each stage's wall time
+// after synchronizing the stream, printed to stderr when the call ends.
+struct StageClock {
+    bool on = false;
+    cudaStream_t stream = nullptr;
+    std::chrono::steady_clock::time_point t0;
+    std::string out;
+    explicit StageClock(const char* what) : on(std::getenv("V2M_CUDA_PROFILE") != nullptr) {
+        if (on) {
+            out = std::string("[v2m_cuda] ") + what;
+            t0 = std::chrono::steady_clock::now();
+        }
+    }
+    void lap(const char* stage) {
+        if (!on) {
+            return;
+        }
+        if (stream) {
+            cudaStreamSynchronize(stream);
+        }
+        const auto t = std::chrono::steady_clock::now();
+        char buf[96];
+        std::snprintf(buf, sizeof(buf), " %s %.2f ms", stage, std::chrono::duration<double, std::milli>(t - t0).count());
+        out += buf;
+        t0 = t;
+    }
+    ~StageClock() {
+        if (on) {
+            std::fprintf(stderr, "%s\n", out.c_str());
+        }
+    }
+};
+thread_local StageClock* g_clock = nullptr;
+
+void lap(const char* stage) {
+    if (g_clock) {
+        g_clock->lap(stage);
+    }
+}
+
 void ck(cudaError_t e, const char* where) {
     if (e != cudaSuccess) {
         throw CudaError(std::string(where) + ": CUDA error " + std::to_string((int)e) + " (" + cudaGetErrorString(e) + ")");
@@ -170,6 +211,18 @@ void check_kernel_error(v2m_session* s) {
     }
 }
 
+// True when p is device memory (not readable by the host): views may carry
+// arrays already on the device (the device grid build and seeding hand theirs
+// on without a host round trip).
+bool on_device(const void* p) {
+    cudaPointerAttributes a;
+    if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice;
+}
+
 void validate(const v2m_grid_view* g, const v2m_relax_params* p, const v2m_nodes_view* nd) {
     if (!g || !p || !nd) {
         throw ArgError("null argument");
@@ -229,8 +282,9 @@ void validate(const v2m_grid_view* g, const v2m_relax_params* p, const v2m_nodes
     if (p->max_iters < 0) {
         throw ArgError("max_iters must be >= 0");
     }
-    // brick tables: every slot a lookup can reach must exist
-    const int64_t nb = (int64_t)g->nbx * g->nby * g->nbz;
+    // brick tables: every slot a lookup can reach must exist (host arrays;
+    // device-resident ones come from this library's own grid build)
+    const int64_t nb = on_device(g->bl_cnt) ? 0 : (int64_t)g->nbx * g->nby * g->nbz;
     for (int64_t b = 0; b < nb; ++b) {
         const int c = g->bl_cnt[b];
         if (c < 0 || c > V2M_BL + 1) {
@@ -241,7 +295,7 @@ void validate(const v2m_grid_view* g, const v2m_relax_params* p, const v2m_nodes
             throw ArgError("brick slot beyond the phi array");
         }
     }
-    for (int64_t i = 0; i < nd->n; ++i) {
+    for (int64_t i = 0, nn = on_device(nd->typ) ? 0 : nd->n; i < nn; ++i) {
         if (nd->typ[i] > V2M_CORNER) {
             throw ArgError("node type out of range");
         }
@@ -287,7 +341,7 @@ template <typename T>
 T* upload(v2m_session* s, const T* host, size_t count) {
     T* d = s->alloc<T>(count);
     if (count) {
-        ck(cudaMemcpyAsync(d, host, count * sizeof(T), cudaMemcpyHostToDevice, s->stream), "upload");
+        ck(cudaMemcpyAsync(d, host, count * sizeof(T), cudaMemcpyDefault, s->stream), "upload");
     }
     return d;
 }
@@ -411,6 +465,7 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
     for (int v = 0; v < nvol; ++v) {
         validate(gv + v, pv + v, nv + v);
     }
+    lap("checks");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
         cudaGetLastError();
@@ -427,6 +482,9 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
         s->device = dev;
         s->nvol = nvol;
         ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        if (g_clock) {
+            g_clock->stream = s->stream;
+        }
         s->serial_power = env_int("V2M_CUDA_SERIAL_POWER", 0);
         s->force_threads = env_int("V2M_CUDA_FORCE_THREADS", 256);
         if (s->force_threads != 64 && s->force_threads != 128 && s->force_threads != 256) {
@@ -514,6 +572,7 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
         ck(cudaMemsetAsync(d.key, 0, 4 * N, s->stream), "memset");
         ck(cudaMemsetAsync(d.sorted, 0, 4 * N, s->stream), "memset");
         ck(cudaMemsetAsync(d.cstart, 0, 4 * KT, s->stream), "memset");
+        lap("allocate");
         std::vector<uint16_t> nodevol(N, 0xFFFF);
         std::vector<int16_t> tilevol(d.ntile_key, -1);
         for (int v = 0; v < nvol; ++v) {
@@ -552,11 +611,12 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
                 tilevol[V.tofs_key + t] = (int16_t)v;
             }
             if (I.n > 0) {
-                ck(cudaMemcpyAsync(d.lab + I.nofs, nv[v].lab, 2 * (size_t)I.n, cudaMemcpyHostToDevice, s->stream), "lab");
-                ck(cudaMemcpyAsync(d.typ + I.nofs, nv[v].typ, (size_t)I.n, cudaMemcpyHostToDevice, s->stream), "typ");
-                ck(cudaMemcpyAsync(d.part + I.nofs, nv[v].part, 4 * (size_t)I.n, cudaMemcpyHostToDevice, s->stream), "part");
+                ck(cudaMemcpyAsync(d.lab + I.nofs, nv[v].lab, 2 * (size_t)I.n, cudaMemcpyDefault, s->stream), "lab");
+                ck(cudaMemcpyAsync(d.typ + I.nofs, nv[v].typ, (size_t)I.n, cudaMemcpyDefault, s->stream), "typ");
+                ck(cudaMemcpyAsync(d.part + I.nofs, nv[v].part, 4 * (size_t)I.n, cudaMemcpyDefault, s->stream), "part");
             }
         }
+        lap("grid upload + corner tables");
         ck(cudaMemcpyAsync(d.vols, s->hvols.data(), sizeof(DVol) * nvol, cudaMemcpyHostToDevice, s->stream), "vols");
         ck(cudaMemcpyAsync(d.nodevol, nodevol.data(), 2 * N, cudaMemcpyHostToDevice, s->stream), "nodevol");
         ck(cudaMemcpyAsync(d.tilevol, tilevol.data(), 2 * (size_t)d.ntile_key, cudaMemcpyHostToDevice, s->stream), "tilevol");
@@ -568,7 +628,7 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
             }
             float* tmp = nullptr;
             ck(cudaMallocAsync((void**)&tmp, 12 * (size_t)I.n, s->stream), "cudaMallocAsync");
-            ck(cudaMemcpyAsync(tmp, nv[v].P, 12 * (size_t)I.n, cudaMemcpyHostToDevice, s->stream), "P");
+            ck(cudaMemcpyAsync(tmp, nv[v].P, 12 * (size_t)I.n, cudaMemcpyDefault, s->stream), "P");
             launch_pack_nodes(s->stream, d, v, I.n, tmp, d.typ);
             ck(cudaFreeAsync(tmp, s->stream), "cudaFreeAsync");
         }
@@ -577,6 +637,7 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
         ck(cudaMemcpyAsync(s->typ0, d.typ, N, cudaMemcpyDeviceToDevice, s->stream), "seed typ");
         ck(cudaMemcpyAsync(s->part0, d.part, 4 * N, cudaMemcpyDeviceToDevice, s->stream), "seed part");
         do_reset(s);
+        lap("node upload");
         s->nbr_threads = env_int("V2M_CUDA_NBR_THREADS", 128);
         if (s->nbr_threads != 64 && s->nbr_threads != 128 && s->nbr_threads != 256) {
             s->nbr_threads = 128;
@@ -690,6 +751,7 @@ void do_iterate(v2m_session* s, int iters, int graph) {
     const auto t0 = std::chrono::steady_clock::now();
     if (graph) {
         build_graph(s);
+        lap("graph capture");
         const int G = s->graph_iters;
         int done_it = 0;
         // per-iteration launches inside the graph: force + tail
@@ -862,6 +924,175 @@ struct v2m_seed_result {
     std::vector<uint8_t> typ;
     std::vector<uint16_t> part, part3;
 };
+
+namespace {
+
+int pick_device(int device) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        cudaGetLastError();
+        throw CudaError("no CUDA device available");
+    }
+    const int dev = device < 0 ? 0 : device;
+    if (dev >= ndev) {
+        throw ArgError("device index out of range");
+    }
+    ck(cudaSetDevice(dev), "cudaSetDevice");
+    return dev;
+}
+
+void release_seeds(SeedBuffers& B, cudaStream_t st) {
+    cudaStreamSynchronize(st);
+    for (void* p : B.tmp) {
+        cudaFree(p);
+    }
+    B.tmp.clear();
+}
+
+// The seeding's own argument checks (before any device is touched).
+void check_seed_args(const v2m_grid_view* g, const v2m_relax_params* prm) {
+    if (!g->grade) {
+        throw ArgError("seeding needs the grid's size grades (grade)");
+    }
+    if (prm->nseed < 1 || prm->nseed > 256) {
+        throw ArgError("nseed must be in [1, 256]");
+    }
+    {
+        // the counts and offsets are int32, as the reference's: bound the
+        // lattice points of the finest level (spacing hmin) over all voxels,
+        // and the grid vertices
+        const double s0 = seed_spacing(0, prm->nseed, g->hmin, g->hmax);
+        const double per = (g->vs[0] / s0 + 2.0) * (g->vs[1] / (0.8660254 * s0) + 2.0) *
+                           (g->vs[2] / (0.8164966 * s0) + 2.0);
+        const double nvox = (double)g->nx * g->ny * g->nz;
+        const double nvert = (double)(g->nx + 1) * (g->ny + 1) * (g->nz + 1);
+        if (!(s0 > 0.0) || per * nvox >= 2147483647.0 || nvert >= 2147483647.0) {
+            throw ArgError("seeding: the grid could hold more seeds than int32 counts allow");
+        }
+    }
+}
+
+// Seeding of grid g (a view of host or device arrays, g->grade required) on
+// device dev, into B (device arrays; release_seeds frees them). `tmp` holds the
+// grid's device copy and its corner tables.
+void seed_on(v2m_session& tmp, const v2m_grid_view* g, const v2m_relax_params* prm, int dev, SeedBuffers& B) {
+    check_seed_args(g, prm);
+    SeedArgs A;
+    A.g = upload_grid(&tmp, g);
+    const size_t nvox = (size_t)g->nx * g->ny * g->nz;
+    A.grade = upload(&tmp, g->grade, nvox);
+    std::vector<float> sp(prm->nseed);
+    for (int L = 0; L < prm->nseed; ++L) {
+        sp[L] = seed_spacing(L, prm->nseed, g->hmin, g->hmax);
+    }
+    A.spacing = upload(&tmp, sp.data(), sp.size());
+    A.nseed = prm->nseed;
+    A.voxmode = prm->voxel_trap ? 1 : 0;
+    A.jseed = prm->jseed;
+    A.corners = prm->corners ? 1 : 0;
+    A.hmax = g->hmax;
+    cudaDeviceGetAttribute(&A.sms, cudaDevAttrMultiProcessorCount, dev);
+    A.stream = tmp.stream;
+    std::string err;
+    const cudaError_t e = seed_run(A, B, err);
+    if (e != cudaSuccess) {
+        release_seeds(B, tmp.stream);
+        cudaGetLastError();
+        if (!err.empty()) {
+            throw ArgError("seeding: " + err);
+        }
+        throw CudaError(std::string("seeding: ") + cudaGetErrorString(e));
+    }
+}
+
+void seeds_to_host(const SeedBuffers& B, cudaStream_t st, v2m_seed_result& r) {
+    const size_t m = (size_t)B.n;
+    r.P.resize(3 * m);
+    r.lab.resize(m);
+    r.typ.resize(m);
+    r.part.resize(2 * m);
+    r.part3.resize(m);
+    if (m) {
+        ck(cudaMemcpyAsync(r.P.data(), B.P, 12 * m, cudaMemcpyDeviceToHost, st), "seeds");
+        ck(cudaMemcpyAsync(r.lab.data(), B.lab, 2 * m, cudaMemcpyDeviceToHost, st), "seeds");
+        ck(cudaMemcpyAsync(r.typ.data(), B.typ, m, cudaMemcpyDeviceToHost, st), "seeds");
+        ck(cudaMemcpyAsync(r.part.data(), B.part, 4 * m, cudaMemcpyDeviceToHost, st), "seeds");
+        ck(cudaMemcpyAsync(r.part3.data(), B.part3, 2 * m, cudaMemcpyDeviceToHost, st), "seeds");
+    }
+    ck(cudaStreamSynchronize(st), "synchronize");
+}
+
+// The device grid build's arguments from the C ABI's, checked.
+GridBuildArgs grid_args(const uint16_t* L, int32_t nx, int32_t ny, int32_t nz, const float* vs,
+                        const v2m_grid_params* p) {
+    if (!L || !vs || !p) {
+        throw ArgError("null argument");
+    }
+    if (nx < 1 || ny < 1 || nz < 1 || (int64_t)nx * ny * nz > (int64_t)0x7FFFFFFF) {
+        throw ArgError("grid dimensions must be positive, at most 2^31 voxels");
+    }
+    if (!(vs[0] > 0.0f && vs[1] > 0.0f && vs[2] > 0.0f)) {
+        throw ArgError("voxel sizes must be positive");
+    }
+    if (!(p->sigma > 0.0f) || !(p->sigma_curv > 0.0f) || p->sigma_thin < 0.0f || !(p->g >= 0.0f) ||
+        !(p->K > 0.0f) || (p->nhlab > 0 && !p->hlab) || p->nhlab < 0) {
+        throw ArgError("grid parameters out of range (sigma, sigma_curv > 0; sigma_thin, g >= 0; K > 0)");
+    }
+    GridBuildArgs A;
+    A.L = L;
+    A.nx = nx;
+    A.ny = ny;
+    A.nz = nz;
+    A.vs[0] = vs[0];
+    A.vs[1] = vs[1];
+    A.vs[2] = vs[2];
+    GridParamsH& q = A.prm;
+    q.sigma = p->sigma;
+    q.sigma_thin = p->sigma_thin;
+    q.thin_lo = p->thin_lo;
+    q.thin_hi = p->thin_hi;
+    q.thick = p->thick;
+    q.thin_floor = p->thin_floor;
+    q.preserve = p->preserve;
+    q.sigma_curv = p->sigma_curv;
+    q.hbase = p->hbase;
+    q.hmin = p->hmin;
+    q.hmax = p->hmax;
+    q.K = p->K;
+    q.g = p->g;
+    if (p->nhlab > 0) {
+        q.hlab.assign(p->hlab, p->hlab + p->nhlab);
+    }
+    return A;
+}
+
+// A view of the device grid build's output (device arrays).
+v2m_grid_view device_view(const GridBuildArgs& A, const GridBuildOut& O) {
+    v2m_grid_view g{};
+    g.nx = A.nx;
+    g.ny = A.ny;
+    g.nz = A.nz;
+    g.nbx = (A.nx + 7) / 8;
+    g.nby = (A.ny + 7) / 8;
+    g.nbz = (A.nz + 7) / 8;
+    g.vs[0] = A.vs[0];
+    g.vs[1] = A.vs[1];
+    g.vs[2] = A.vs[2];
+    g.L = O.L;
+    g.bl_cnt = O.bl_cnt;
+    g.bl_lab = O.bl_lab;
+    g.bl_slot = O.bl_slot;
+    g.phi = O.phi;
+    g.nslots = O.nslots;
+    g.h = O.h;
+    g.hmin = O.hmin;
+    g.hmax = O.hmax;
+    g.gm = 0;
+    g.grade = O.grade;
+    return g;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -1489,89 +1720,22 @@ int v2m_seed_cuda(const v2m_grid_view* g, const v2m_relax_params* prm, int devic
         *n = 0;
         v2m_nodes_view none{};
         validate(g, prm, &none);
-        if (!g->grade) {
-            throw ArgError("seeding needs the grid's size grades (grade)");
-        }
-        if (prm->nseed < 1 || prm->nseed > 256) {
-            throw ArgError("nseed must be in [1, 256]");
-        }
-        {
-            // the counts and offsets are int32, as the reference's: bound the
-            // lattice points of the finest level (spacing hmin) over all voxels,
-            // and the grid vertices
-            const double s0 = seed_spacing(0, prm->nseed, g->hmin, g->hmax);
-            const double per = (g->vs[0] / s0 + 2.0) * (g->vs[1] / (0.8660254 * s0) + 2.0) *
-                               (g->vs[2] / (0.8164966 * s0) + 2.0);
-            const double nvox = (double)g->nx * g->ny * g->nz;
-            const double nvert = (double)(g->nx + 1) * (g->ny + 1) * (g->nz + 1);
-            if (!(s0 > 0.0) || per * nvox >= 2147483647.0 || nvert >= 2147483647.0) {
-                throw ArgError("seeding: the grid could hold more seeds than int32 counts allow");
-            }
-        }
-        int ndev = 0;
-        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
-            cudaGetLastError();
-            throw CudaError("no CUDA device available");
-        }
-        const int dev = device < 0 ? 0 : device;
-        if (dev >= ndev) {
-            throw ArgError("device index out of range");
-        }
-        ck(cudaSetDevice(dev), "cudaSetDevice");
+        check_seed_args(g, prm);
+        const int dev = pick_device(device);
         v2m_session tmp;   // (an allocation context: the grid's device copy)
         tmp.device = dev;
         ck(cudaStreamCreateWithFlags(&tmp.stream, cudaStreamNonBlocking), "cudaStreamCreate");
-        SeedArgs A;
-        A.g = upload_grid(&tmp, g);
-        const size_t nvox = (size_t)g->nx * g->ny * g->nz;
-        A.grade = upload(&tmp, g->grade, nvox);
-        std::vector<float> sp(prm->nseed);
-        for (int L = 0; L < prm->nseed; ++L) {
-            sp[L] = seed_spacing(L, prm->nseed, g->hmin, g->hmax);
-        }
-        A.spacing = upload(&tmp, sp.data(), sp.size());
-        A.nseed = prm->nseed;
-        A.voxmode = prm->voxel_trap ? 1 : 0;
-        A.jseed = prm->jseed;
-        A.corners = prm->corners ? 1 : 0;
-        A.hmax = g->hmax;
-        cudaDeviceGetAttribute(&A.sms, cudaDevAttrMultiProcessorCount, dev);
-        A.stream = tmp.stream;
         SeedBuffers B;
-        std::string err;
-        const cudaError_t e = seed_run(A, B, err);
-        auto release = [&] {
-            cudaStreamSynchronize(tmp.stream);
-            for (void* p : B.tmp) {
-                cudaFree(p);
-            }
-            B.tmp.clear();
-        };
-        if (e != cudaSuccess) {
-            release();
-            cudaGetLastError();
-            if (!err.empty()) {
-                throw ArgError("seeding: " + err);
-            }
-            throw CudaError(std::string("seeding: ") + cudaGetErrorString(e));
-        }
+        seed_on(tmp, g, prm, dev, B);
         std::unique_ptr<v2m_seed_result> r(new v2m_seed_result());
-        const size_t m = (size_t)B.n;
-        r->P.resize(3 * m);
-        r->lab.resize(m);
-        r->typ.resize(m);
-        r->part.resize(2 * m);
-        r->part3.resize(m);
-        if (m) {
-            ck(cudaMemcpyAsync(r->P.data(), B.P, 12 * m, cudaMemcpyDeviceToHost, tmp.stream), "seeds");
-            ck(cudaMemcpyAsync(r->lab.data(), B.lab, 2 * m, cudaMemcpyDeviceToHost, tmp.stream), "seeds");
-            ck(cudaMemcpyAsync(r->typ.data(), B.typ, m, cudaMemcpyDeviceToHost, tmp.stream), "seeds");
-            ck(cudaMemcpyAsync(r->part.data(), B.part, 4 * m, cudaMemcpyDeviceToHost, tmp.stream), "seeds");
-            ck(cudaMemcpyAsync(r->part3.data(), B.part3, 2 * m, cudaMemcpyDeviceToHost, tmp.stream), "seeds");
+        try {
+            seeds_to_host(B, tmp.stream, *r);
+        } catch (...) {
+            release_seeds(B, tmp.stream);
+            throw;
         }
-        release();
-        ck(cudaGetLastError(), "seeding");
-        *n = (int64_t)m;
+        release_seeds(B, tmp.stream);
+        *n = (int64_t)r->lab.size();
         *out = r.release();
     });
 }
@@ -1622,55 +1786,12 @@ void v2m_grid_params_default(v2m_grid_params* p) {
 int v2m_grid_build_cuda(const uint16_t* L, int32_t nx, int32_t ny, int32_t nz, const float* vs,
                         const v2m_grid_params* p, int device, v2m_grid_result** out) {
     return guard([&] {
-        if (!out || !L || !vs || !p) {
+        if (!out) {
             throw ArgError("null argument");
         }
         *out = nullptr;
-        if (nx < 1 || ny < 1 || nz < 1 || (int64_t)nx * ny * nz > (int64_t)0x7FFFFFFF) {
-            throw ArgError("grid dimensions must be positive, at most 2^31 voxels");
-        }
-        if (!(vs[0] > 0.0f && vs[1] > 0.0f && vs[2] > 0.0f)) {
-            throw ArgError("voxel sizes must be positive");
-        }
-        if (!(p->sigma > 0.0f) || !(p->sigma_curv > 0.0f) || p->sigma_thin < 0.0f || !(p->g >= 0.0f) ||
-            !(p->K > 0.0f) || (p->nhlab > 0 && !p->hlab) || p->nhlab < 0) {
-            throw ArgError("grid parameters out of range (sigma, sigma_curv > 0; sigma_thin, g >= 0; K > 0)");
-        }
-        int ndev = 0;
-        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
-            cudaGetLastError();
-            throw CudaError("no CUDA device available");
-        }
-        const int dev = device < 0 ? 0 : device;
-        if (dev >= ndev) {
-            throw ArgError("device index out of range");
-        }
-        ck(cudaSetDevice(dev), "cudaSetDevice");
-        GridBuildArgs A;
-        A.L = L;
-        A.nx = nx;
-        A.ny = ny;
-        A.nz = nz;
-        A.vs[0] = vs[0];
-        A.vs[1] = vs[1];
-        A.vs[2] = vs[2];
-        GridParamsH& q = A.prm;
-        q.sigma = p->sigma;
-        q.sigma_thin = p->sigma_thin;
-        q.thin_lo = p->thin_lo;
-        q.thin_hi = p->thin_hi;
-        q.thick = p->thick;
-        q.thin_floor = p->thin_floor;
-        q.preserve = p->preserve;
-        q.sigma_curv = p->sigma_curv;
-        q.hbase = p->hbase;
-        q.hmin = p->hmin;
-        q.hmax = p->hmax;
-        q.K = p->K;
-        q.g = p->g;
-        if (p->nhlab > 0) {
-            q.hlab.assign(p->hlab, p->hlab + p->nhlab);
-        }
+        GridBuildArgs A = grid_args(L, nx, ny, nz, vs, p);
+        const int dev = pick_device(device);
         A.device = dev;
         cudaStream_t st = nullptr;
         ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -1733,6 +1854,75 @@ int v2m_grid_build_cuda(const uint16_t* L, int32_t nx, int32_t ny, int32_t nz, c
         r->limit_sweeps = O.limit_sweeps;
         *out = r.release();
     });
+}
+
+int v2m_points_cuda(const uint16_t* L, int32_t nx, int32_t ny, int32_t nz, const float* vs, const v2m_grid_params* gp,
+                    const v2m_relax_params* prm, int device, v2m_seed_result** out, int64_t* n, v2m_relax_stats* st) {
+    v2m_session* s = nullptr;
+    v2m_session tmp;   // (the allocation context of the grid build and the seeding)
+    GridBuildOut O;
+    SeedBuffers B;
+    const int rc = guard([&] {
+        if (!out || !n || !prm) {
+            throw ArgError("null argument");
+        }
+        *out = nullptr;
+        *n = 0;
+        GridBuildArgs A = grid_args(L, nx, ny, nz, vs, gp);
+        const int dev = pick_device(device);
+        tmp.device = dev;
+        ck(cudaStreamCreateWithFlags(&tmp.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        A.device = dev;
+        A.stream = tmp.stream;
+        std::string err;
+        const cudaError_t e = grid_build(A, O, err);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw CudaError(std::string("grid build: ") + cudaGetErrorString(e));
+        }
+        // the stages hand their device arrays on: grid -> seeds -> session
+        const v2m_grid_view gv = device_view(A, O);
+        v2m_nodes_view none{};
+        validate(&gv, prm, &none);
+        seed_on(tmp, &gv, prm, dev, B);
+        v2m_nodes_view nv{};
+        nv.n = B.n;
+        nv.P = B.P;
+        nv.lab = B.lab;
+        nv.typ = B.typ;
+        nv.part = B.part;
+        s = create(1, &gv, prm, &nv, dev);
+        do_rebuild(s);
+        do_iterate(s, s->max_iters, env_int("V2M_CUDA_GRAPH", 1));
+        std::unique_ptr<v2m_seed_result> r(new v2m_seed_result());
+        seeds_to_host(B, tmp.stream, *r);   // (lab and part3 stay the seeds')
+        v2m_nodes_view hv{};
+        hv.n = B.n;
+        hv.P = r->P.data();
+        hv.lab = r->lab.data();
+        hv.typ = r->typ.data();
+        hv.part = r->part.data();
+        read_nodes(s, 0, &hv);
+        if (st) {
+            fill_stats(s, 0, st);
+        }
+        *n = B.n;
+        *out = r.release();
+    });
+    const std::string keep = g_err;
+    if (s) {
+        cudaStreamSynchronize(s->stream);
+        delete s;
+    }
+    if (tmp.stream) {
+        release_seeds(B, tmp.stream);
+        for (void* x : O.tmp) {
+            cudaFree(x);
+        }
+        O.tmp.clear();
+    }
+    g_err = keep;
+    return rc;
 }
 
 int v2m_grid_result_view(const v2m_grid_result* r, v2m_grid_view* g) {
@@ -1846,23 +2036,31 @@ int v2m_relax_cuda(const v2m_grid_view* g, const v2m_relax_params* prm, v2m_node
 int v2m_relax_cuda_batch(int nvol, const v2m_grid_view* g, const v2m_relax_params* prm, v2m_nodes_view* nd,
                          v2m_relax_stats* st, int device) {
     v2m_session* s = nullptr;
+    StageClock clock("relax_cl:");
+    g_clock = &clock;
     const int rc = guard([&] {
         s = create(nvol, g, prm, nd, device);
         do_rebuild(s);
+        lap("first list build");
         do_iterate(s, s->max_iters, env_int("V2M_CUDA_GRAPH", 1));
+        lap("loop");
         for (int v = 0; v < nvol; ++v) {
             read_nodes(s, v, nd + v);
             if (st) {
                 fill_stats(s, v, st + v);
             }
         }
+        lap("read-back");
     });
     if (s) {
         const std::string keep = g_err;
         cudaStreamSynchronize(s->stream);
         delete s;
         g_err = keep;
+        clock.stream = nullptr;
+        lap("release");
     }
+    g_clock = nullptr;
     return rc;
 }
 

@@ -717,16 +717,19 @@ __global__ void __launch_bounds__(256, 4) k_force(const DVol* __restrict__ vols,
     // the positions in batches of kForceBatch, so that a node's dependent chain
     // is 1 + ceil(nnb / 4) memory round trips rather than 2 ceil(nnb / 4); the
     // bars are still added one by one in list order. A list id outside the
-    // node's volume (a corrupted list) is reported and the list cut there.
+    // node's volume (a corrupted list) is clamped into it, so that no gather
+    // leaves the volume's nodes, and reported after the fold: the check feeds
+    // neither the loop nor the addresses' dependences on the other ids.
     int jj[V2M_K];
-    int m = n;
+    const int m = n;
+    const unsigned lo = (unsigned)V.nofs, span = (unsigned)V.n;
+    unsigned bad = 0u;
 #pragma unroll
     for (int k = 0; k < V2M_K; ++k) {
-        jj[k] = k < n ? __ldg(row + (int64_t)k * N) : (int)i;
-        if (k < m && (jj[k] < V.nofs || jj[k] >= V.nofs + V.n)) {
-            raise_error(G, 3, (int)i);
-            m = k;
-        }
+        const int j = k < n ? __ldg(row + (int64_t)k * N) : (int)i;
+        const unsigned r = (unsigned)j - lo;
+        bad |= k < n && r >= span;
+        jj[k] = r < span ? j : (int)lo;
     }
 #pragma unroll
     for (int k0 = 0; k0 < V2M_K; k0 += kForceBatch) {
@@ -759,6 +762,9 @@ __global__ void __launch_bounds__(256, 4) k_force(const DVol* __restrict__ vols,
         }
     }
     F[i] = make_float4(fx, fy, fz, fa);
+    if (bad) {
+        raise_error(G, 3, (int)i);
+    }
 }
 
 // ---- move + per-iteration reductions ------------------------------------------------

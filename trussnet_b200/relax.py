@@ -81,14 +81,18 @@ def seed_cl(g: Grid, prm: RelaxParams, device: int = -1) -> tuple[Nodes, np.ndar
     n = C.c_int64()
     _lib.check(L.v2m_seed_cuda(C.byref(gv), C.byref(pv), device, C.byref(h), C.byref(n)))
     try:
-        m = n.value
-        nd = Nodes(P=np.zeros((m, 3), np.float32), lab=np.zeros(m, np.uint16), typ=np.zeros(m, np.uint8),
-                   part=np.zeros((m, 2), np.uint16))
-        part3 = np.zeros(m, np.uint16)
-        _lib.check(L.v2m_seed_copy(h, nd.P.ctypes.data, nd.lab.ctypes.data, nd.typ.ctypes.data, nd.part.ctypes.data,
-                                   part3.ctypes.data))
+        nd, part3 = _copy_seed_result(L, h, n.value)
     finally:
         L.v2m_seed_free(h)
+    return nd, part3
+
+
+def _copy_seed_result(L, h, m: int) -> tuple[Nodes, np.ndarray]:
+    nd = Nodes(P=np.zeros((m, 3), np.float32), lab=np.zeros(m, np.uint16), typ=np.zeros(m, np.uint8),
+               part=np.zeros((m, 2), np.uint16))
+    part3 = np.zeros(m, np.uint16)
+    _lib.check(L.v2m_seed_copy(h, nd.P.ctypes.data, nd.lab.ctypes.data, nd.typ.ctypes.data, nd.part.ctypes.data,
+                               part3.ctypes.data))
     return nd, part3
 
 
@@ -120,6 +124,38 @@ def grid_cl(L: np.ndarray, vs=(1.0, 1.0, 1.0), prm: GridParams | None = None, de
     finally:
         lib.v2m_grid_free(h)
     return g
+
+
+def points_cl(L: np.ndarray, vs=(1.0, 1.0, 1.0), gprm: GridParams | None = None, prm: RelaxParams | None = None,
+              device: int = -1) -> tuple[Nodes, np.ndarray, RelaxStats]:
+    """The pipeline's points mode on a CUDA device (v2m_points_cuda): the label
+    volume uploaded once, grid built, seeded and relaxed from device arrays,
+    the relaxed nodes copied back once -- build_grid_cpu -> seed_cpu ->
+    relax_cpu bit for bit. Returns (nodes, part3, stats)."""
+    lib = _lib.load()
+    L = np.ascontiguousarray(L, np.uint16)
+    nz, ny, nx = L.shape
+    gprm = gprm or GridParams()
+    prm = prm or RelaxParams()
+    pc = GridParamsC()
+    for f in ("sigma", "sigma_thin", "thin_lo", "thin_hi", "thick", "thin_floor", "preserve", "sigma_curv", "hbase",
+              "hmin", "hmax", "K", "g"):
+        setattr(pc, f, float(getattr(gprm, f)))
+    hl = np.ascontiguousarray(gprm.hlab, np.float32)
+    pc.hlab = hl.ctypes.data if hl.size else None
+    pc.nhlab = int(hl.size)
+    vsa = np.asarray(vs, np.float32)
+    pv = prm.to_c()
+    sv = RelaxStatsC()
+    h = C.c_void_p()
+    n = C.c_int64()
+    _lib.check(lib.v2m_points_cuda(L.ctypes.data, nx, ny, nz, vsa.ctypes.data, C.byref(pc), C.byref(pv), device,
+                                   C.byref(h), C.byref(n), C.byref(sv)))
+    try:
+        nd, part3 = _copy_seed_result(lib, h, n.value)
+    finally:
+        lib.v2m_seed_free(h)
+    return nd, part3, RelaxStats.from_c(sv)
 
 
 def validate_lists(nbr: np.ndarray, nnb: np.ndarray, pi: np.ndarray, pj: np.ndarray) -> str:
