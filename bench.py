@@ -360,15 +360,24 @@ def run_batch(args):
     sess.close()
     step_ms = max_over_ranks(ms / args.steps)
     seq_ms = None
+    seq_sync_ms = None
     e2e = {}
     from trussnet_b200 import relax_cl, relax_cl_batch
     if world == 1:
-        # the same relaxations, one volume at a time, plain launches (each session warmed once)
+        # the same relaxations, one volume at a time, plain launches (each session warmed once):
+        # the loop's control on the device, the host reading it every 25 iterations; and the
+        # same with the reference relax_cl's blocking read-back every iteration
         seq_ms = 0.0
+        seq_sync_ms = 0.0
         for g, nd in vols:
             with Session(g, prm, nd, device=local) as s1:
                 s1.timed_runs(1, graph=False)
                 seq_ms += s1.timed_runs(1, graph=False)
+                os.environ["V2M_CUDA_HOST_CHECK"] = "1"
+                try:
+                    seq_sync_ms += s1.timed_runs(1, graph=False)
+                finally:
+                    del os.environ["V2M_CUDA_HOST_CHECK"]
         torch.cuda.synchronize(local)
         # end to end through the C ABI: one batch call against one relax_cl call per
         # volume (host buffers, every upload, set-up and read-back inside), same results
@@ -407,6 +416,8 @@ def run_batch(args):
                            "parallelism": (f"volumes sharded over {world} ranks by node count (LPT), no collective "
                                            f"in the loop" if world > 1 else "one session")},
                 "sequential_plain_ms": seq_ms, "batched_speedup": (seq_ms / step_ms) if seq_ms else None,
+                "sequential_plain_readback_every_iteration_ms": seq_sync_ms if world == 1 else None,
+                "batched_speedup_vs_readback_every_iteration": (seq_sync_ms / step_ms) if world == 1 else None,
                 "e2e": {"value": n * iters / e2e["batch_call_s"], "unit": UNIT,
                         "h2d_bytes_per_step": int(sum(g.nbytes() for g in grids) + sum(nd.nbytes() for nd in nodes)),
                         "d2h_bytes_per_step": int(sum(nd.P.nbytes + nd.typ.nbytes + nd.part.nbytes for nd in nodes)),
@@ -636,8 +647,22 @@ def run_cuda(args):
     # iterations profiled stage by stage (plain launches, outside the timed region)
     sess.reset()
     sess.rebuild()
-    stages = sess.profile_stages(min(100, iters))
+    nprof = min(100, iters)
+    stages = sess.profile_stages(nprof)
+    trapped, interior = sess.queue_sizes()
     sess.close()
+    # the move's roofline: algorithmic bytes per iteration -- every node's 91 B
+    # (read P 12, F 16, V 12, typ 1, lab 2, part 4, h 4; write P 12, V 12, h 4,
+    # |dp|/h 4, power 4) and, per trapped node, one brick record (48 B) and two
+    # labels' eight corner values (64 B) -- over the move stage's time per iteration
+    move_ms = stages["move"] / nprof if nprof else 0.0
+    move_bytes = 91 * n + 112 * trapped
+    move_achieved = move_bytes / (move_ms / 1e3) / 1e9 if move_ms > 0 else None
+    move_roofline = {"kernel": "k_move_pre + k_move_main", "bound": "hbm", "achieved": move_achieved, "peak": peak,
+                     "unit": "GB/s", "frac": move_achieved / peak if move_achieved else None,
+                     "peak_source": peak_kind, "bytes_per_iteration": move_bytes, "ms_per_iteration": move_ms,
+                     "queued_trapped": trapped, "queued_interior": interior,
+                     "traffic": profiled_traffic("k_move_main", args.workload)}
     # end to end through the public call (tn::relax_cl's C ABI) with pinned host buffers
     e2e = None
     if args.e2e_steps > 0:
@@ -656,6 +681,7 @@ def run_cuda(args):
                            "rebuilds_per_step": st.rebuilds, "final_types": [st.n_interior, st.n_interface,
                                                                              st.n_junction, st.n_corner]},
                 "clocks": clocks, "e2e": e2e, "gpu_launches": int(cnt["launches"]), "roofline": roofline,
+                "move_roofline": move_roofline,
                 "stage_ms_first100": stages, "cpu_baseline": cb, "adjoint": adj}
         print(json.dumps(line), flush=True)
     if world > 1:

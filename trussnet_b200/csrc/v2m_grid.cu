@@ -40,6 +40,7 @@
 #include "../../include/v2m_cuda.h"
 #include "v2m_field.cuh"
 #include "v2m_grid.h"
+#include "v2m_kernels.h"
 
 namespace v2m {
 namespace {
@@ -587,9 +588,14 @@ cudaError_t grid_build(const GridBuildArgs& A, GridBuildOut& O, std::string& err
     const int nb = d.nbx * d.nby * d.nbz;
     const GridParamsH& p = A.prm;
     std::vector<void*>& tmp = O.tmp;
+    auto lap = [&](const char* what) {
+        if (A.lap) {
+            A.lap(what);
+        }
+    };
     auto dalloc = [&](size_t bytes) -> void* {
         void* q = nullptr;
-        if (cudaMalloc(&q, std::max<size_t>(bytes, 16)) != cudaSuccess) {
+        if (pool_malloc(&q, std::max<size_t>(bytes, 16), st) != cudaSuccess) {
             return nullptr;
         }
         tmp.push_back(q);
@@ -645,8 +651,10 @@ cudaError_t grid_build(const GridBuildArgs& A, GridBuildOut& O, std::string& err
     V2M_ALLOC(bl_cnt, int, nb);
     V2M_ALLOC(bl_lab, uint16_t, (size_t)nb * V2M_BL);
     V2M_ALLOC(bl_slot, int, nb);
+    lap("upload");
     k_brick_labels<<<(nb + 7) / 8, 256, 0, st>>>(L, d, R, bl_cnt, bl_lab, nb);
     V2M_TRY(cudaGetLastError());
+    lap("brick labels");
     // 2. slots, in brick order
     int *cnt, *ofs;
     V2M_ALLOC(cnt, int, nb + 1);
@@ -684,7 +692,9 @@ cudaError_t grid_build(const GridBuildArgs& A, GridBuildOut& O, std::string& err
         return cudaGetLastError();
     };
     // 3. the wide (curvature) smoothing, for the sizing
+    lap("slots");
     V2M_TRY(smooth(p.sigma_curv, Rc, phi));
+    lap("curvature smoothing");
     DGrid g;
     std::memset(&g, 0, sizeof(g));
     g.nx = A.nx;
@@ -715,32 +725,35 @@ cudaError_t grid_build(const GridBuildArgs& A, GridBuildOut& O, std::string& err
     SizeArgs sa{ dhlab, (int)hlab.size(), hbase, hmin, hmax, p.K, hcurv };
     k_size<<<gs_blocks(nv, sms), 256, 0, st>>>(g, sa, h);
     V2M_TRY(cudaGetLastError());
+    lap("sizing");
     // thickness (for the thin-layer sizing and blend): the peak on the device,
     // its erfinv on the host (the host's logf, as the reference)
-    std::vector<float> tvox;
     float* tv = nullptr;
     if (p.thick > 0.0f || p.sigma_thin > 0.0f) {
         V2M_ALLOC(tv, float, nv);
         k_thick_peak<<<gs_blocks(nv, sms), 256, 0, st>>>(g, 2, tv);
-        tvox.resize(nv);
-        V2M_TRY(cudaMemcpyAsync(tvox.data(), tv, 4 * (size_t)nv, cudaMemcpyDeviceToHost, st));
-        V2M_TRY(cudaStreamSynchronize(st));
+        lap("thickness peak");
         const float sg = p.sigma_curv;
         const unsigned nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-        std::vector<std::thread> pool;
-        for (unsigned q = 0; q < nth; ++q) {
-            pool.emplace_back([&, q] {
-                const int64_t a = nv * q / nth, b = nv * (q + 1) / nth;
-                for (int64_t v = a; v < b; ++v) {
-                    const float m = tvox[v];
-                    tvox[v] = (m < 0.0f || m >= 0.9999f) ? 1e30f : 2.8284271f * sg * erfinv_giles(m);
-                }
-            });
-        }
-        for (auto& t : pool) {
-            t.join();
-        }
-        V2M_TRY(cudaMemcpyAsync(tv, tvox.data(), 4 * (size_t)nv, cudaMemcpyHostToDevice, st));
+        // through the pinned staging buffers, chunk by chunk, in place on the host threads
+        V2M_TRY(staged_map(tv, tv, 4 * (size_t)nv, st, [&](void* buf, size_t bytes, size_t) {
+            float* t = static_cast<float*>(buf);
+            const int64_t cnt = (int64_t)(bytes / 4);
+            std::vector<std::thread> pool;
+            for (unsigned q = 0; q < nth; ++q) {
+                pool.emplace_back([=] {
+                    const int64_t a = cnt * q / nth, b = cnt * (q + 1) / nth;
+                    for (int64_t v = a; v < b; ++v) {
+                        const float m = t[v];
+                        t[v] = (m < 0.0f || m >= 0.9999f) ? 1e30f : 2.8284271f * sg * erfinv_giles(m);
+                    }
+                });
+            }
+            for (auto& th : pool) {
+                th.join();
+            }
+        }));
+        lap("thickness erfinv (host)");
     }
     if (p.thick > 0.0f) {
         const float floor_mm = p.thin_floor * vmin;
@@ -749,6 +762,7 @@ cudaError_t grid_build(const GridBuildArgs& A, GridBuildOut& O, std::string& err
     }
     // 5. the interface fields: sigma, then the thin-layer blend with sigma_thin
     V2M_TRY(smooth(p.sigma, Ri, phi));
+    lap("interface smoothing");
     if (p.sigma_thin > 0.0f) {
         float* w = tv;   // (the thickness, consumed into the blend weight)
         float* wt;
@@ -779,6 +793,7 @@ cudaError_t grid_build(const GridBuildArgs& A, GridBuildOut& O, std::string& err
         }
         std::swap(phi, phi2);   // phi: the blend
         g.phi = phi;
+        lap("thin-layer blend");
     }
     if (p.preserve > 0.0f) {
         k_preserve<<<gs_blocks(nv, sms), 256, 0, st>>>(g, phi, p.preserve);
@@ -806,6 +821,7 @@ cudaError_t grid_build(const GridBuildArgs& A, GridBuildOut& O, std::string& err
             break;
         }
     }
+    lap("gradient limit");
     // 7. grades
     const std::vector<float> th = grade_thresholds(hmin, hmax);
     float* dth;
@@ -815,6 +831,7 @@ cudaError_t grid_build(const GridBuildArgs& A, GridBuildOut& O, std::string& err
     V2M_ALLOC(grade, uint8_t, nv);
     k_grade<<<gs_blocks(nv, sms), 256, 0, st>>>(h, nv, dth, grade);
     V2M_TRY(cudaGetLastError());
+    lap("grades");
     O.hmin = hmin;
     O.hmax = hmax;
     O.L = L;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -24,6 +25,7 @@ struct GridBuildArgs {
     GridParamsH prm;
     int device = 0;
     cudaStream_t stream = nullptr;
+    std::function<void(const char*)> lap;   // stage timing hook (may be empty)
 };
 
 // Device arrays (in `tmp`, freed by the caller) and the derived sizes.

@@ -23,6 +23,7 @@
 #include <sys/stat.h>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/v2m_cuda.h"
@@ -145,6 +146,159 @@ struct VolInfo {
 
 }  // namespace
 
+namespace v2m {
+
+cudaMemPool_t library_pool(int device) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    if (device < 0 || device >= 64) {
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[device]) {
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        if (cudaMemPoolCreate(&pools[device], &props) != cudaSuccess) {
+            cudaGetLastError();
+            pools[device] = nullptr;
+            return nullptr;
+        }
+        const char* e = std::getenv("V2M_CUDA_POOL_KEEP_MB");
+        uint64_t keep = (uint64_t)(e ? std::max(0, std::atoi(e)) : 16384) << 20;
+        cudaMemPoolSetAttribute(pools[device], cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    return pools[device];
+}
+
+namespace {
+
+constexpr size_t kStageBytes = (size_t)32 << 20;
+
+// memcpy split over up to 8 host threads in 1 MB-aligned slices
+void parallel_copy(void* dst, const void* src, size_t len) {
+    const size_t slice = (size_t)1 << 20;
+    const unsigned nth = (unsigned)std::min<size_t>(std::max(1u, std::min(8u, std::thread::hardware_concurrency())),
+                                                    (len + slice - 1) / slice);
+    if (nth <= 1) {
+        std::memcpy(dst, src, len);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const size_t per = (len / nth + slice - 1) / slice * slice;
+    for (unsigned q = 0; q < nth; ++q) {
+        const size_t a = std::min(len, q * per), b = std::min(len, a + per);
+        if (a < b) {
+            pool.emplace_back([=] { std::memcpy((char*)dst + a, (const char*)src + a, b - a); });
+        }
+    }
+    for (auto& t : pool) {
+        t.join();
+    }
+}
+
+struct Staging {
+    std::mutex mu;
+    void* buf[2] = { nullptr, nullptr };
+    cudaEvent_t ev[2] = { nullptr, nullptr };
+};
+
+Staging& staging() {
+    static Staging st;
+    return st;
+}
+
+cudaError_t staging_ready(Staging& S) {
+    for (int q = 0; q < 2; ++q) {
+        if (!S.buf[q]) {
+            cudaError_t e = cudaMallocHost(&S.buf[q], kStageBytes);
+            if (e != cudaSuccess) {
+                S.buf[q] = nullptr;
+                return e;
+            }
+        }
+        if (!S.ev[q]) {
+            cudaError_t e = cudaEventCreateWithFlags(&S.ev[q], cudaEventDisableTiming);
+            if (e != cudaSuccess) {
+                S.ev[q] = nullptr;
+                return e;
+            }
+        }
+    }
+    return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t staged_map(void* dst, const void* src, size_t bytes, cudaStream_t s,
+                       const std::function<void(void*, size_t, size_t)>& fn) {
+    Staging& S = staging();
+    std::lock_guard<std::mutex> lk(S.mu);
+    cudaError_t e = staging_ready(S);
+    if (e != cudaSuccess) {
+        return e;
+    }
+    const size_t nchunk = (bytes + kStageBytes - 1) / kStageBytes;
+    // chunk c goes device -> buf[c % 2] (event), host fn, then buf -> dst (event);
+    // the buffer is reused two chunks later, after its copy back has completed
+    for (size_t c = 0; c < nchunk; ++c) {
+        const int q = (int)(c & 1);
+        const size_t off = c * kStageBytes, len = std::min(kStageBytes, bytes - off);
+        if ((e = cudaEventSynchronize(S.ev[q])) != cudaSuccess) {
+            return e;
+        }
+        if ((e = cudaMemcpyAsync(S.buf[q], (const char*)src + off, len, cudaMemcpyDeviceToHost, s)) != cudaSuccess) {
+            return e;
+        }
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) {
+            return e;
+        }
+        fn(S.buf[q], len, off);
+        if (dst) {
+            if ((e = cudaMemcpyAsync((char*)dst + off, S.buf[q], len, cudaMemcpyHostToDevice, s)) != cudaSuccess) {
+                return e;
+            }
+            if ((e = cudaEventRecord(S.ev[q], s)) != cudaSuccess) {
+                return e;
+            }
+        }
+    }
+    return cudaStreamSynchronize(s);
+}
+
+cudaError_t staged_d2h(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    Staging& S = staging();
+    std::lock_guard<std::mutex> lk(S.mu);
+    cudaError_t e = staging_ready(S);
+    if (e != cudaSuccess) {
+        return e;
+    }
+    const size_t nchunk = (bytes + kStageBytes - 1) / kStageBytes;
+    for (size_t c = 0; c < nchunk + 1; ++c) {
+        if (c < nchunk) {   // the DMA of chunk c ...
+            const size_t off = c * kStageBytes, len = std::min(kStageBytes, bytes - off);
+            if ((e = cudaMemcpyAsync(S.buf[c & 1], (const char*)src + off, len, cudaMemcpyDeviceToHost, s)) !=
+                    cudaSuccess ||
+                (e = cudaEventRecord(S.ev[c & 1], s)) != cudaSuccess) {
+                return e;
+            }
+        }
+        if (c > 0) {   // ... while the host copies chunk c - 1 out (over several threads: a fresh
+                       // destination's first-touch page faults are the cost, and they run in parallel)
+            const size_t p = c - 1, off = p * kStageBytes, len = std::min(kStageBytes, bytes - off);
+            if ((e = cudaEventSynchronize(S.ev[p & 1])) != cudaSuccess) {
+                return e;
+            }
+            parallel_copy((char*)dst + off, S.buf[p & 1], len);
+        }
+    }
+    return cudaSuccess;
+}
+
+}  // namespace v2m
+
 struct v2m_session {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -175,7 +329,7 @@ struct v2m_session {
     T* alloc(size_t count) {
         void* p = nullptr;
         const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
-        ck(cudaMalloc(&p, bytes), "cudaMalloc");
+        ck(pool_malloc(&p, bytes, stream), "device allocation");
         allocs.push_back(p);
         return static_cast<T*>(p);
     }
@@ -188,9 +342,10 @@ struct v2m_session {
             cudaEventDestroy(e);
         }
         for (void* p : allocs) {
-            cudaFree(p);
+            cudaFreeAsync(p, stream);   // (back to the library's pool)
         }
         if (stream) {
+            cudaStreamSynchronize(stream);
             cudaStreamDestroy(stream);
         }
     }
@@ -351,7 +506,7 @@ T* upload(v2m_session* s, const T* host, size_t count) {
 void build_corner_tables(v2m_session* s, DGrid& g, size_t nb) {
     uint4* xbrick = s->alloc<uint4>(3 * nb);
     int* xn = nullptr;
-    ck(cudaMallocAsync((void**)&xn, 4 * std::max<size_t>(nb, 1), s->stream), "cudaMallocAsync");
+    ck(pool_malloc((void**)&xn, 4 * std::max<size_t>(nb, 1), s->stream), "cudaMallocAsync");
     launch_xcount(s->stream, g, xbrick, xn, (int)nb);
     ck(cudaGetLastError(), "corner tables");
     std::vector<int> hn(nb);
@@ -627,7 +782,7 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
                 continue;
             }
             float* tmp = nullptr;
-            ck(cudaMallocAsync((void**)&tmp, 12 * (size_t)I.n, s->stream), "cudaMallocAsync");
+            ck(pool_malloc((void**)&tmp, 12 * (size_t)I.n, s->stream), "cudaMallocAsync");
             ck(cudaMemcpyAsync(tmp, nv[v].P, 12 * (size_t)I.n, cudaMemcpyDefault, s->stream), "P");
             launch_pack_nodes(s->stream, d, v, I.n, tmp, d.typ);
             ck(cudaFreeAsync(tmp, s->stream), "cudaFreeAsync");
@@ -780,6 +935,10 @@ void do_iterate(v2m_session* s, int iters, int graph) {
             ck(cudaEventCreate(&e0), "event");
             ck(cudaEventCreate(&e1), "event");
         }
+        // the host reads the control blocks every `every` iterations (25; 1 is the
+        // reference's relax_cl, which blocks on a read-back every iteration,
+        // src/v2m_gpu.cpp:348)
+        const int every = std::max(1, env_int("V2M_CUDA_HOST_CHECK", 25));
         for (int k = 0; k < iters; ++k) {
             enqueue_force(s, e0, e1);
             enqueue_tail(s);
@@ -790,7 +949,7 @@ void do_iterate(v2m_session* s, int iters, int graph) {
                 ck(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
                 s->force_ms += ms;
             }
-            if ((k + 1) % 25 == 0 || k + 1 == iters) {
+            if ((k + 1) % every == 0 || k + 1 == iters) {
                 read_ctl(s, c);
                 inject("iterate", c[0].it);
                 if (all_done(s, c)) {
@@ -857,7 +1016,7 @@ void read_nodes(v2m_session* s, int v, v2m_nodes_view* nd) {
         return;
     }
     float* tmp = nullptr;
-    ck(cudaMallocAsync((void**)&tmp, 12 * (size_t)I.n, s->stream), "cudaMallocAsync");
+    ck(pool_malloc((void**)&tmp, 12 * (size_t)I.n, s->stream), "cudaMallocAsync");
     launch_unpack_P(s->stream, s->d, I.nofs, I.n, tmp);
     ck(cudaMemcpyAsync(nd->P, tmp, 12 * (size_t)I.n, cudaMemcpyDeviceToHost, s->stream), "P");
     if (std::getenv("V2M_CUDA_FAIL_AT")) {
@@ -904,14 +1063,31 @@ float seed_spacing(int L, int nseed, float hmin, float hmax) {
 
 }  // namespace
 
+// A host array left uninitialized (the device copy writes every element).
+template <typename T>
+struct HostArray {
+    std::unique_ptr<T[]> p;
+    size_t n = 0;
+    void resize(size_t count) {
+        p.reset(count ? new T[count] : nullptr);
+        n = count;
+    }
+    T* data() const {
+        return p.get();
+    }
+    size_t size() const {
+        return n;
+    }
+};
+
 // A grid built on the device, held on the host (tn::Grid's arrays).
 struct v2m_grid_result {
     int32_t nx = 0, ny = 0, nz = 0;
     float vs[3] = { 1, 1, 1 };
-    std::vector<uint16_t> L, bl_lab;
-    std::vector<int32_t> bl_cnt, bl_slot;
-    std::vector<float> phi, h;
-    std::vector<uint8_t> grade;
+    HostArray<uint16_t> L, bl_lab;
+    HostArray<int32_t> bl_cnt, bl_slot;
+    HostArray<float> phi, h;
+    HostArray<uint8_t> grade;
     int64_t nslots = 0;
     float hbase = 0, hmin = 0, hmax = 0;
     int32_t R = 0, limit_sweeps = 0;
@@ -942,11 +1118,11 @@ int pick_device(int device) {
 }
 
 void release_seeds(SeedBuffers& B, cudaStream_t st) {
-    cudaStreamSynchronize(st);
     for (void* p : B.tmp) {
-        cudaFree(p);
+        cudaFreeAsync(p, st);
     }
     B.tmp.clear();
+    cudaStreamSynchronize(st);
 }
 
 // The seeding's own argument checks (before any device is touched).
@@ -1277,7 +1453,7 @@ int v2m_session_read_array(v2m_session* s, int vol, int what, void* host, int64_
         };
         void* tmp = nullptr;
         auto scratch = [&](size_t b) {
-            ck(cudaMallocAsync(&tmp, std::max<size_t>(b, 16), s->stream), "cudaMallocAsync");
+            ck(pool_malloc(&tmp, std::max<size_t>(b, 16), s->stream), "cudaMallocAsync");
             return tmp;
         };
         switch (what) {
@@ -1383,7 +1559,7 @@ int v2m_session_write_array(v2m_session* s, int vol, int what, const void* host,
         };
         void* tmp = nullptr;
         auto staged = [&](int64_t b) {
-            ck(cudaMallocAsync(&tmp, std::max<size_t>((size_t)b, 16), s->stream), "cudaMallocAsync");
+            ck(pool_malloc(&tmp, std::max<size_t>((size_t)b, 16), s->stream), "cudaMallocAsync");
             ck(cudaMemcpyAsync(tmp, host, (size_t)b, cudaMemcpyHostToDevice, s->stream), "write");
             return tmp;
         };
@@ -1398,7 +1574,7 @@ int v2m_session_write_array(v2m_session* s, int vol, int what, const void* host,
             float* t = (float*)staged(12LL * n);
             std::vector<float> hn(n);
             float* hd = nullptr;
-            ck(cudaMallocAsync((void**)&hd, 4 * (size_t)n + 16, s->stream), "cudaMallocAsync");
+            ck(pool_malloc((void**)&hd, 4 * (size_t)n + 16, s->stream), "cudaMallocAsync");
             launch_hn(s->stream, d, I.nofs, n, hd);
             launch_float3_to4(s->stream, t, I.nofs, n, d.Pq);
             launch_set_hn(s->stream, d, I.nofs, n, hd);
@@ -1456,7 +1632,7 @@ int v2m_session_write_lists(v2m_session* s, int vol, const int32_t* nbr, const i
             }
         }
         int* t = nullptr;
-        ck(cudaMallocAsync((void**)&t, 4 * ((size_t)n * V2M_K + n) + 16, s->stream), "cudaMallocAsync");
+        ck(pool_malloc((void**)&t, 4 * ((size_t)n * V2M_K + n) + 16, s->stream), "cudaMallocAsync");
         ck(cudaMemcpyAsync(t, nbr, 4 * (size_t)n * V2M_K, cudaMemcpyHostToDevice, s->stream), "write");
         ck(cudaMemcpyAsync(t + (size_t)n * V2M_K, nnb, 4 * (size_t)n, cudaMemcpyHostToDevice, s->stream), "write");
         launch_lists_from_rowmajor(s->stream, s->d, I.nofs, n, t, t + (size_t)n * V2M_K);
@@ -1796,14 +1972,17 @@ int v2m_grid_build_cuda(const uint16_t* L, int32_t nx, int32_t ny, int32_t nz, c
         cudaStream_t st = nullptr;
         ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
         A.stream = st;
+        StageClock clock("grid build:");
+        clock.stream = st;
+        A.lap = [&](const char* w) { clock.lap(w); };
         GridBuildOut O;
         std::string err;
         auto release = [&] {
-            cudaStreamSynchronize(st);
             for (void* x : O.tmp) {
-                cudaFree(x);
+                cudaFreeAsync(x, st);
             }
             O.tmp.clear();
+            cudaStreamSynchronize(st);
             cudaStreamDestroy(st);
         };
         const cudaError_t e = grid_build(A, O, err);
@@ -1821,7 +2000,8 @@ int v2m_grid_build_cuda(const uint16_t* L, int32_t nx, int32_t ny, int32_t nz, c
         r->vs[0] = vs[0];
         r->vs[1] = vs[1];
         r->vs[2] = vs[2];
-        r->L.assign(L, L + nv);
+        r->L.resize(nv);
+        parallel_copy(r->L.data(), L, 2 * nv);
         r->bl_cnt.resize(nb);
         r->bl_lab.resize(nb * V2M_BL);
         r->bl_slot.resize(nb);
@@ -1830,7 +2010,7 @@ int v2m_grid_build_cuda(const uint16_t* L, int32_t nx, int32_t ny, int32_t nz, c
         r->grade.resize(nv);
         auto d2h = [&](void* dst, const void* src, size_t bytes) {
             if (bytes) {
-                ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st), "grid read-back");
+                ck(staged_d2h(dst, src, bytes, st), "grid read-back");
             }
         };
         try {
@@ -1841,6 +2021,7 @@ int v2m_grid_build_cuda(const uint16_t* L, int32_t nx, int32_t ny, int32_t nz, c
             d2h(r->h.data(), O.h, 4 * nv);
             d2h(r->grade.data(), O.grade, nv);
             ck(cudaStreamSynchronize(st), "synchronize");
+            clock.lap("read-back");
         } catch (...) {
             release();
             throw;
@@ -1885,6 +2066,7 @@ int v2m_points_cuda(const uint16_t* L, int32_t nx, int32_t ny, int32_t nz, const
         v2m_nodes_view none{};
         validate(&gv, prm, &none);
         seed_on(tmp, &gv, prm, dev, B);
+        ck(cudaStreamSynchronize(tmp.stream), "synchronize");   // (the session reads them on its own stream)
         v2m_nodes_view nv{};
         nv.n = B.n;
         nv.P = B.P;
@@ -1917,9 +2099,10 @@ int v2m_points_cuda(const uint16_t* L, int32_t nx, int32_t ny, int32_t nz, const
     if (tmp.stream) {
         release_seeds(B, tmp.stream);
         for (void* x : O.tmp) {
-            cudaFree(x);
+            cudaFreeAsync(x, tmp.stream);
         }
         O.tmp.clear();
+        cudaStreamSynchronize(tmp.stream);
     }
     g_err = keep;
     return rc;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -18,6 +19,33 @@ constexpr int kMoveThreads = 256;   // k_move_pre's block; volume node ranges ar
 constexpr int kMainThreads = 128;   // k_move_main's block
 constexpr int kCtlThreads = 256;
 constexpr int kNodeAlign = kMoveThreads;
+
+// The library's stream-ordered memory pool on `device` (created on first use;
+// v2m_host.cu). Freed blocks stay reserved for the next session, up to
+// V2M_CUDA_POOL_KEEP_MB (default 16384; 0: returned at once), so repeated calls
+// do not map fresh device memory each time. The pool is the library's own: the
+// device's default pool is left as the process has it.
+cudaMemPool_t library_pool(int device);
+
+// cudaMallocFromPoolAsync from the library's pool of the current device.
+inline cudaError_t pool_malloc(void** p, size_t bytes, cudaStream_t s) {
+    int dev = 0;
+    const cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        return e;
+    }
+    cudaMemPool_t pool = library_pool(dev);
+    return pool ? cudaMallocFromPoolAsync(p, bytes, pool, s) : cudaErrorMemoryAllocation;
+}
+
+// Copies between device memory and pageable host memory through two pinned
+// staging buffers of the library (allocated once per process, double-buffered:
+// the DMA of one chunk overlaps the host copy of the previous one).
+// staged_map runs fn(chunk, bytes, offset) on the host over each chunk of
+// src (device) in pinned memory and copies the chunk back to dst (device).
+cudaError_t staged_d2h(void* dst, const void* src, size_t bytes, cudaStream_t s);
+cudaError_t staged_map(void* dst, const void* src, size_t bytes, cudaStream_t s,
+                       const std::function<void(void*, size_t, size_t)>& fn);
 
 // Every device array of a session (flat over its volumes).
 struct Dev {

@@ -590,7 +590,7 @@ struct Scratch {
             cudaFreeAsync(p, s);
         }
         bytes = b;
-        return cudaMallocAsync(&p, b, s);
+        return pool_malloc(&p, b, s);
     }
     ~Scratch() {
         if (p) {
@@ -622,7 +622,7 @@ cudaError_t seed_stages(const SeedArgs& A, SeedBuffers& B, std::string& err) {
     Scratch sc{ s };
     auto alloc = [&](size_t bytes) -> void* {
         void* p = nullptr;
-        if (cudaMallocAsync(&p, std::max<size_t>(bytes, 16), s) != cudaSuccess) {
+        if (pool_malloc(&p, std::max<size_t>(bytes, 16), s) != cudaSuccess) {
             return nullptr;
         }
         B.tmp.push_back(p);
