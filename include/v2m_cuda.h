@@ -251,6 +251,9 @@ int v2m_session_stats(v2m_session* s, int vol, v2m_relax_stats* st);
 #define V2M_ARR_HIST 13      /* int32 [34]  log2 histogram, max |dp|/h bits, half-skin count */
 #define V2M_ARR_SERIAL_SUMS 14 /* int32 [1] iterations whose FIRE power was within rounding of zero, so that
                                   its sign was taken from relax_cpu's serial order */
+#define V2M_ARR_DIRS 15      /* float [3n]  each node's constraint direction at its position (read only): an
+                                  INTERFACE node's unit normal of psi_(own, partner), a JUNCTION node's unit
+                                  junction-line direction, zero otherwise -- v2m_unroll_set_constraints' input */
 int v2m_session_read_array(v2m_session* s, int vol, int what, void* host, int64_t bytes);
 /* Overwrite an internal array of volume `vol` from host memory (P, typ, part, nbr, nnb, V, hn). */
 int v2m_session_write_array(v2m_session* s, int vol, int what, const void* host, int64_t bytes);
@@ -324,6 +327,14 @@ int v2m_unroll_loss_backward(v2m_unroll* u, const float* x, const float* G, floa
                              int accumulate);
 /* reverse of the last forward pass: gx0 = dL/dx0 and gG = dL/dG (+ gG_in if not NULL) from gxK = dL/dxK */
 int v2m_unroll_backward(v2m_unroll* u, const float* G, const float* gxK, float* gx0, float* gG, const float* gG_in);
+/* Taped constraints, the trapped move frozen like the active bars: with dirs (HOST float [3n], x/y/z per
+ * node) each INTERFACE node's step is projected onto the plane normal to its direction (it glides in its
+ * interface's tangent plane) and each JUNCTION node's onto its direction (it moves along the junction
+ * line); other types and zero directions are unconstrained (CORNER nodes stay, as always). The
+ * directions are normalised and stay fixed over the unroll; V2M_ARR_DIRS of a session gives them at the
+ * session's positions. dirs = NULL removes the constraints. Either way the next forward pass records a
+ * new tape (replay before it is an error). */
+int v2m_unroll_set_constraints(v2m_unroll* u, const float* dirs);
 /* the tape (K x n active-bar masks) to host memory */
 int v2m_unroll_tape(v2m_unroll* u, uint32_t* host, int64_t count);
 /* device milliseconds of the last forward (K steps) and backward passes */

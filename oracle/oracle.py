@@ -46,7 +46,7 @@ def load():
 _INT = {"key": np.int32, "sorted": np.int32, "cstart": np.int32, "nbr": np.int32, "nnb": np.int32,
         "typ": np.uint8, "part": np.uint16, "hist": np.int32}
 _PER = {"key": 1, "sorted": 1, "Ps": 4, "nbr": V2M_K, "nnb": 1, "F": 4, "hn": 1, "mv": 1, "V": 3, "pw": 1,
-        "P0": 3, "P": 3, "typ": 1, "part": 2}
+        "P0": 3, "P": 3, "typ": 1, "part": 2, "dirs": 3}
 
 
 class Oracle:
@@ -152,7 +152,7 @@ def _unroll_args(nbr, nnb, typ, G, cs):
         for f in ("orc_unroll_forward_f64", "orc_unroll_grad_f64"):
             getattr(L, f).restype = C.c_double
             getattr(L, f).argtypes = [C.c_int, vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_double, C.c_int,
-                                      vp, vp] + ([vp] if f.endswith("grad_f64") else []) + [vp, C.c_int]
+                                      vp, vp] + ([vp] if f.endswith("grad_f64") else []) + [vp, C.c_int, vp]
         L._unroll_set = True
     nbr = np.ascontiguousarray(nbr, np.int32).reshape(-1)
     nnb = np.ascontiguousarray(nnb, np.int32)
@@ -163,10 +163,35 @@ def _unroll_args(nbr, nnb, typ, G, cs):
     return L, nbr, nnb, typ, G, m, cs
 
 
-def unroll_forward_f64(nbr, nnb, typ, G, cs, fscale, fsurf, dt, K, x0, tape=None):
+def unroll_dirs(typ, dirs):
+    """The taped constraints as the oracle takes them, [n, 4] float64: each
+    INTERFACE (kind 1) and JUNCTION (kind 2) node's direction normalised in
+    double and rounded to float32 (as v2m_unroll_set_constraints stores it),
+    zero rows for other types and zero directions; None stays None."""
+    if dirs is None:
+        return None
+    typ = np.asarray(typ, np.uint8).reshape(-1)
+    d = np.asarray(dirs, np.float32).reshape(-1, 3).astype(np.float64)
+    r = np.sqrt((d * d).sum(1))
+    kind = np.where(typ == 1, 1.0, np.where(typ == 2, 2.0, 0.0))
+    kind[r == 0.0] = 0.0
+    out = np.zeros((len(typ), 4))
+    ok = kind > 0
+    out[ok, :3] = (d[ok] / r[ok, None]).astype(np.float32)
+    out[:, 3] = kind
+    return np.ascontiguousarray(out)
+
+
+def _dptr(d):
+    return None if d is None else d.ctypes.data
+
+
+def unroll_forward_f64(nbr, nnb, typ, G, cs, fscale, fsurf, dt, K, x0, tape=None, dirs=None):
     """FP64: K unroll steps from x0 [n,3]; returns (xK, loss at xK, tape). With
     tape=None the active bars are decided and recorded; with a tape (uint32
-    [K, n]) they are replayed (the taped function)."""
+    [K, n]) they are replayed (the taped function). dirs [n, 3]: taped
+    constraints (unroll_dirs)."""
+    dd = unroll_dirs(typ, dirs)
     L, nbr, nnb, typ, G, m, cs = _unroll_args(nbr, nnb, typ, G, cs)
     x0 = np.ascontiguousarray(x0, np.float64)
     xK = np.zeros_like(x0)
@@ -174,13 +199,15 @@ def unroll_forward_f64(nbr, nnb, typ, G, cs, fscale, fsurf, dt, K, x0, tape=None
     tape = np.zeros((K, len(nnb)), np.uint32) if tape is None else np.ascontiguousarray(tape, np.uint32)
     loss = L.orc_unroll_forward_f64(len(nnb), nbr.ctypes.data, nnb.ctypes.data, typ.ctypes.data, m.ctypes.data,
                                     cs.ctypes.data, G.ctypes.data, fscale, fsurf, dt, K, x0.ctypes.data,
-                                    xK.ctypes.data, tape.ctypes.data, int(replay))
+                                    xK.ctypes.data, tape.ctypes.data, int(replay), _dptr(dd))
     return xK, loss, tape
 
 
-def unroll_grad_f64(nbr, nnb, typ, G, cs, fscale, fsurf, dt, K, x0, tape=None):
+def unroll_grad_f64(nbr, nnb, typ, G, cs, fscale, fsurf, dt, K, x0, tape=None, dirs=None):
     """FP64: (loss, dloss/dx0 [n,3], dloss/dG [shape of G], tape) by reverse mode
-    of the taped function (recorded here when tape is None)."""
+    of the taped function (recorded here when tape is None); dirs as in
+    unroll_forward_f64."""
+    dd = unroll_dirs(typ, dirs)
     L, nbr, nnb, typ, G, m, cs = _unroll_args(nbr, nnb, typ, G, cs)
     x0 = np.ascontiguousarray(x0, np.float64)
     gx = np.zeros_like(x0)
@@ -189,5 +216,5 @@ def unroll_grad_f64(nbr, nnb, typ, G, cs, fscale, fsurf, dt, K, x0, tape=None):
     tape = np.zeros((K, len(nnb)), np.uint32) if tape is None else np.ascontiguousarray(tape, np.uint32)
     loss = L.orc_unroll_grad_f64(len(nnb), nbr.ctypes.data, nnb.ctypes.data, typ.ctypes.data, m.ctypes.data,
                                  cs.ctypes.data, G.ctypes.data, fscale, fsurf, dt, K, x0.ctypes.data, gx.ctypes.data,
-                                 gG.ctypes.data, tape.ctypes.data, int(replay))
+                                 gG.ctypes.data, tape.ctypes.data, int(replay), _dptr(dd))
     return loss, gx, gG, tape

@@ -125,6 +125,11 @@
         case V2M_ARR_TYP: src = st->typ; nb = n; break;                                                          \
         case V2M_ARR_PART: src = st->part; nb = 4 * n; break;                                                    \
         case V2M_ARR_HIST: src = st->hist; nb = 4 * 32; break;                                                   \
+        case V2M_ARR_DIRS:                                                                                       \
+            nb = (int64_t)sizeof(REALT) * 3 * n;                                                                 \
+            if (bytes < nb) return -1;                                                                           \
+            PFX##constraint_dirs(st, (REALT*)out);                                                               \
+            return nb;                                                                                           \
         default: return -1;                                                                                      \
         }                                                                                                        \
         if (bytes < nb) return -1;                                                                               \

@@ -637,6 +637,42 @@ static void FN(crossing)(const FN(state)* s, int a, int b, const REAL* p, const 
     for (int k = 0; k < 3; ++k) c[k] = p[k] + t * (q[k] - p[k]);
 }
 
+/* The constraint direction of every node at its position (the CUDA session's
+   V2M_ARR_DIRS read): an INTERFACE node's unit normal of psi_(own, partner), a
+   JUNCTION node's unit junction-line direction (the cross product of the two
+   interface gradients the junction move of :926-945 below uses), zero for the
+   other types and where the vector vanishes. */
+static void FN(constraint_dirs)(const FN(state)* s, REAL* out) {
+    for (int64_t i = 0; i < s->n; ++i) {
+        const int ty = s->typ[i], a = s->lab[i], b = s->part[2 * i], c = s->part[2 * i + 1];
+        REAL d[3] = { K(0.0), K(0.0), K(0.0) };
+        if (ty == V2M_INTERFACE || ty == V2M_JUNCTION) {
+            const REAL* p = s->P + 3 * i;
+            REAL g1[3], u[3];
+            FN(psi_grad)(s, a, b, p, g1);
+            u[0] = g1[0];
+            u[1] = g1[1];
+            u[2] = g1[2];
+            if (ty == V2M_JUNCTION) {
+                REAL g2[3];
+                FN(psi_grad)(s, a, c, p, g2);
+                u[0] = g1[1] * g2[2] - g1[2] * g2[1];
+                u[1] = g1[2] * g2[0] - g1[0] * g2[2];
+                u[2] = g1[0] * g2[1] - g1[1] * g2[0];
+            }
+            const REAL un = SQRT(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+            if (un > K(0.0)) {
+                d[0] = u[0] / un;
+                d[1] = u[1] / un;
+                d[2] = u[2] / un;
+            }
+        }
+        out[3 * i] = d[0];
+        out[3 * i + 1] = d[1];
+        out[3 * i + 2] = d[2];
+    }
+}
+
 static void FN(tangential)(const FN(state)* s, int a, int b, const REAL* p, REAL* v) {
     REAL g[3];
     FN(psi_grad)(s, a, b, p, g);

@@ -20,6 +20,11 @@
  *              stiffness c_i, whose jumps make the untaped step discontinuous,
  *              is frozen
  *   x_i'     = x_i + dt F_i / max(c_i, 1)      (CORNER nodes stay)
+ *              or, with taped constraints (dirs: per node a unit direction d
+ *              and a kind), x_i' = x_i + P_i dt F_i / max(c_i, 1) with
+ *              P_i = I - d d^T (kind 1, an INTERFACE node in its tangent plane)
+ *              or d d^T (kind 2, a JUNCTION node along its line); the reverse
+ *              step's increment adjoint is then P_i dt lam_i / max(c_i, 1)
  *   loss     = sum over every list entry (i, j) of (l_ij / hm_ij - 1)^2,
  *              hm_ij = (h_i + h_j) / 2, at the final positions.
  */
@@ -39,7 +44,17 @@ typedef struct {
     double cs[3];
     const double* G;
     double fscale, fsurf, dt;
+    const double* dirs;   /* n x 4 (d, kind) or NULL */
 } unroll_t;
+
+/* v <- P_i v */
+static void project(const unroll_t* U, int i, double* v) {
+    if (!U->dirs) return;
+    const double* d = U->dirs + 4 * (long)i;
+    if (d[3] == 0.0) return;
+    double t = v[0] * d[0] + v[1] * d[1] + v[2] * d[2];
+    for (int k = 0; k < 3; ++k) v[k] = d[3] == 1.0 ? v[k] - t * d[k] : t * d[k];
+}
 
 /* h at x, its gradient (may be NULL), the 8 corner indices and weights */
 static double size_at(const unroll_t* U, const double* x, double* grad, long* idx, double* w) {
@@ -119,7 +134,9 @@ static void step(const unroll_t* U, const double* x, double* y, double* h, uint3
         }
         if (!replay) mask[i] = bits;
         double s = U->dt / (c > 1 ? c : 1);
-        for (int d = 0; d < 3; ++d) y[3 * i + d] = x[3 * i + d] + s * F[d];
+        double inc[3] = { s * F[0], s * F[1], s * F[2] };
+        project(U, i, inc);
+        for (int d = 0; d < 3; ++d) y[3 * i + d] = x[3 * i + d] + inc[d];
     }
 }
 
@@ -181,6 +198,7 @@ static void step_backward(const unroll_t* U, const double* x, double* h, double*
         int c = __builtin_popcount(mask[i]);
         double mu[3];
         for (int d = 0; d < 3; ++d) mu[d] = U->dt * lam_in[3 * i + d] / (c > 1 ? c : 1);
+        project(U, i, mu);
         for (int k = 0; k < U->nnb[i]; ++k) {
             int j = U->nbr[(long)i * UK + k];
             double e[3] = { x[3 * i] - x[3 * j], x[3 * i + 1] - x[3 * j + 1], x[3 * i + 2] - x[3 * j + 2] };
@@ -217,15 +235,17 @@ static unroll_t make(int n, const int32_t* nbr, const int32_t* nnb, const uint8_
     U.fscale = fscale;
     U.fsurf = fsurf;
     U.dt = dt;
+    U.dirs = NULL;
     return U;
 }
 
 /* K steps from x0 (n x 3) into xK; returns the loss at xK. tape: K x n masks,
-   recorded (replay = 0) or replayed (replay = 1) */
+   recorded (replay = 0) or replayed (replay = 1); dirs: taped constraints or NULL */
 double orc_unroll_forward_f64(int n, const int32_t* nbr, const int32_t* nnb, const uint8_t* typ, const int32_t* m,
                               const double* cs, const double* G, double fscale, double fsurf, double dt, int K,
-                              const double* x0, double* xK, uint32_t* tape, int replay) {
+                              const double* x0, double* xK, uint32_t* tape, int replay, const double* dirs) {
     unroll_t U = make(n, nbr, nnb, typ, m, cs, G, fscale, fsurf, dt);
+    U.dirs = dirs;
     double* a = (double*)malloc(sizeof(double) * 3 * (size_t)n);
     double* b = (double*)malloc(sizeof(double) * 3 * (size_t)n);
     double* h = (double*)malloc(sizeof(double) * (size_t)n);
@@ -248,8 +268,10 @@ double orc_unroll_forward_f64(int n, const int32_t* nbr, const int32_t* nnb, con
    the function taped by this call's forward pass (replay = 0) or by `tape` */
 double orc_unroll_grad_f64(int n, const int32_t* nbr, const int32_t* nnb, const uint8_t* typ, const int32_t* m,
                            const double* cs, const double* G, double fscale, double fsurf, double dt, int K,
-                           const double* x0, double* gx0, double* gG, uint32_t* tape, int replay) {
+                           const double* x0, double* gx0, double* gG, uint32_t* tape, int replay,
+                           const double* dirs) {
     unroll_t U = make(n, nbr, nnb, typ, m, cs, G, fscale, fsurf, dt);
+    U.dirs = dirs;
     size_t s3 = 3 * (size_t)n;
     double* X = (double*)malloc(sizeof(double) * s3 * (size_t)(K + 1));
     double* h = (double*)malloc(sizeof(double) * (size_t)n);

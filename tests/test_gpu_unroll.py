@@ -17,6 +17,7 @@ import numpy as np
 import pytest
 
 from oracle.oracle import unroll_forward_f64, unroll_grad_f64
+from cases import first_diff, same_bits
 from trussnet_b200 import Session, synth
 from trussnet_b200.types import RelaxParams
 
@@ -146,4 +147,78 @@ def test_sizing_by_gradient_lowers_the_loss(cuda_lib):
     assert float(G1.min()) >= float(Gt.min()) and float(G1.max()) <= float(Gt.max())
     x1, lx = optimize_positions(u, x0, Gt, steps=12, step=0.02)
     assert lx[-1] < lx[0], lx
+    u.close()
+
+
+def test_constrained_adjoint(cuda_lib, record_property):
+    """Taped constraints (Unroll.set_constraints): the session's constraint
+    directions (V2M_ARR_DIRS) after 3 relaxation iterations of tpm_small equal
+    the oracle's bit for bit; the constrained unroll keeps INTERFACE nodes in
+    their tangent planes and JUNCTION nodes on their lines; its loss and
+    gradients match the FP64 constrained unroll (relative 2-norm <= 1e-4) and
+    FP64 finite differences along the gradient (<= 1e-4); removing the
+    constraints gives back the unconstrained unroll bit for bit."""
+    import cases
+    import torch
+    from oracle.oracle import Oracle
+    from trussnet_b200.adjoint import Unroll
+    g, nd = cases.tpm_small()
+    prm = RelaxParams(max_iters=3)
+    o = Oracle("f32").state(g, prm, nd.copy())
+    o.run()
+    with Session(g, prm, nd.copy()) as s:
+        s.run()
+        P, typ = s.read("P").reshape(-1, 3), s.read("typ")
+        nbr, nnb, dirs = s.read("nbr"), s.read("nnb"), s.read("dirs").reshape(-1, 3)
+    assert same_bits(P, o.read("P").reshape(-1, 3)) and same_bits(typ, o.read("typ"))
+    d = first_diff(dirs, o.read("dirs").reshape(-1, 3))
+    assert d is None, f"constraint directions vs the oracle: {d}"
+    m, K = 10, 12
+    G = synth.sizing_grid((m, m, m), 1.4, 2.0, seed=5)
+    cs = tuple((v - 1) / (m - 1) for v in (g.nx, g.ny, g.nz))
+    u = Unroll(nbr, nnb, typ, G.shape[::-1], cs, FSCALE, FSURF, DT, K, 5)
+    x0, Gt = torch.tensor(P, device="cuda"), torch.tensor(G, device="cuda")
+    free = u.forward(x0, Gt).cpu().numpy()
+    u.set_constraints(dirs)
+    from trussnet_b200._lib import V2mError
+    with pytest.raises(V2mError):
+        u.forward(x0, Gt, replay=True)   # the constraints invalidate the tape
+    xK = u.forward(x0, Gt)
+    loss = u.loss(xK, Gt)
+    gxK, gG1 = u.loss_backward(xK, Gt)
+    gx0, gG2 = u.backward(Gt, gxK)
+    disp = xK.cpu().numpy().astype(np.float64) - P
+    itf, jun = typ == 1, typ == 2
+    un = dirs.astype(np.float64) / np.maximum(np.linalg.norm(dirs.astype(np.float64), axis=1), 1e-30)[:, None]
+    along = np.abs((disp[itf] * un[itf]).sum(1)).max()
+    across = np.linalg.norm(np.cross(disp[jun], un[jun]), axis=1).max()
+    record_property("interface_normal_motion_max", float(along))
+    record_property("junction_off_line_motion_max", float(across))
+    # float32 positions: each of the K steps rounds x + increment (|x| < 44: half
+    # an ulp is 1.9e-6), against free motions of order 1e-2
+    assert along <= 1e-4 and across <= 1e-4, (along, across)
+    assert np.abs(((free - P)[itf] * un[itf]).sum(1)).max() > 1e-2
+    assert np.all(disp[typ == 3] == 0.0)
+    tape = u.tape()
+    args = (nbr, nnb, typ, G.astype(np.float64), cs, FSCALE, FSURF, DT, K)
+    x64 = P.astype(np.float64)
+    L64, gx64, gG64, _ = unroll_grad_f64(*args, x64, tape, dirs=dirs)
+    gx = gx0.cpu().numpy().astype(np.float64)
+    gG = (gG1 + gG2).cpu().numpy().astype(np.float64)
+    e_loss, e_x, e_G = abs(loss - L64) / abs(L64), rel(gx, gx64), rel(gG, gG64)
+    record_property("constrained_loss_rel_err", e_loss)
+    record_property("constrained_grad_x_rel_err_vs_fp64", e_x)
+    record_property("constrained_grad_G_rel_err_vs_fp64", e_G)
+    assert e_loss <= 1e-4 and e_x <= 1e-4 and e_G <= 1e-4, (e_loss, e_x, e_G)
+    eps = 1e-3
+    dx = gx / np.linalg.norm(gx)
+    lp = unroll_forward_f64(*args, x64 + eps * dx, tape, dirs=dirs)[1]
+    lm = unroll_forward_f64(*args, x64 - eps * dx, tape, dirs=dirs)[1]
+    an = float(np.sum(gx * dx))
+    e_fd = abs((lp - lm) / (2 * eps) - an) / abs(an)
+    record_property("constrained_fd_rel_err_along_gradient", e_fd)
+    assert e_fd <= 1e-4, e_fd
+    u.set_constraints(None)
+    again = u.forward(x0, Gt).cpu().numpy()
+    assert same_bits(again, free)
     u.close()

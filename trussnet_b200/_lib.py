@@ -25,6 +25,7 @@ EXPORTS = [
     "v2m_session_write_lists", "v2m_session_info", "v2m_session_counters", "v2m_session_timed_runs",
     "v2m_session_clear_counters", "v2m_unroll_create", "v2m_unroll_destroy", "v2m_unroll_forward",
     "v2m_unroll_loss", "v2m_unroll_loss_backward", "v2m_unroll_backward", "v2m_unroll_tape", "v2m_unroll_timing",
+    "v2m_unroll_set_constraints",
     "v2m_unroll_last_error", "v2m_session_autotune", "v2m_session_shapes",
     "v2m_session_profile_stages", "v2m_session_queue_sizes", "v2m_bin_sort_noalloc", "v2m_bin_sort_noalloc_error",
     "v2m_validate_lists", "v2m_grid_params_default", "v2m_grid_build_cuda", "v2m_grid_result_view",
@@ -103,6 +104,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.v2m_unroll_loss_backward.argtypes = [vp, vp, vp, C.c_float, vp, vp, C.c_int]
         L.v2m_unroll_backward.argtypes = [vp, vp, vp, vp, vp, vp]
         L.v2m_unroll_tape.argtypes = [vp, vp, C.c_int64]
+        L.v2m_unroll_set_constraints.argtypes = [vp, vp]
         L.v2m_unroll_timing.argtypes = [vp, P(C.c_float), P(C.c_float)]
         _lib = L
         return L

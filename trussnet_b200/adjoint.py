@@ -93,6 +93,18 @@ class Unroll:
                                                      self._ptr(gG), None))
         return gx0, gG
 
+    def set_constraints(self, dirs=None):
+        """Taped constraints (see v2m_unroll_set_constraints): dirs float [n, 3],
+        each INTERFACE node's interface normal and each JUNCTION node's
+        junction-line direction (Session.read('dirs')); None removes them."""
+        if dirs is None:
+            _lib.check_unroll(self.L.v2m_unroll_set_constraints(self.h, None))
+            return
+        d = np.ascontiguousarray(dirs, np.float32).reshape(-1)
+        if d.size != 3 * self.n:
+            raise ValueError("dirs needs 3 values per node")
+        _lib.check_unroll(self.L.v2m_unroll_set_constraints(self.h, d.ctypes.data))
+
     def tape(self) -> np.ndarray:
         out = np.zeros((self.K, self.n), np.uint32)
         _lib.check_unroll(self.L.v2m_unroll_tape(self.h, out.ctypes.data, out.size))

@@ -14,6 +14,14 @@
 //   x_i' = x_i + dt sum_k f_k (x_i - x_j) / max(c_i, 1), f = (l0 - l) / l,
 //          l0 = a_ij (h_i + h_j), a_ij = fsurf/2 (both non-INTERIOR) or fscale/2;
 //          CORNER nodes stay.
+// Optional taped constraints (v2m_unroll_set_constraints) freeze the trapped
+// move's geometry the way the tape freezes the active bars: node i's increment
+// is projected, x_i' = x_i + P_i (s_i F_i), with P_i = I - n n^T for an
+// INTERFACE node (it glides in the tangent plane of its interface, unit normal
+// n) or P_i = t t^T for a JUNCTION node (it moves along the junction line, unit
+// direction t); the directions are constants of the unroll, taken once from the
+// field at the starting positions. P_i is symmetric, so the reverse step's
+// increment adjoint is mu_i = s_i P_i lam_i.
 // Loss: sum over every list entry (i, j) of (l_ij / hm_ij - 1)^2, hm = (h_i+h_j)/2.
 //
 // Reverse mode with checkpoints every `ckpt` steps: the backward pass recomputes
@@ -26,6 +34,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
@@ -153,6 +162,28 @@ __global__ void k_unpack(const float4* __restrict__ x4, float* __restrict__ x3, 
     }
 }
 
+// P_i v in place: kind (d.w) 1 removes the component along d (a plane), kind 2
+// keeps only it (a line), kind 0 leaves v.
+__device__ __forceinline__ void project(const float4* __restrict__ dirs, int i, float& x, float& y, float& z) {
+    if (!dirs) {
+        return;
+    }
+    const float4 d = __ldg(dirs + i);
+    if (d.w == 0.0f) {
+        return;
+    }
+    const float t = x * d.x + y * d.y + z * d.z;
+    if (d.w == 1.0f) {
+        x = x - t * d.x;
+        y = y - t * d.y;
+        z = z - t * d.z;
+    } else {
+        x = t * d.x;
+        y = t * d.y;
+        z = t * d.z;
+    }
+}
+
 // one step xh -> yh (the new state's sizes included); records (replay = 0) or
 // replays the active-bar masks. A replay visits only the taped bars, in the same
 // ascending slot order as the recording. Ids and positions are loaded kB at a
@@ -161,8 +192,8 @@ constexpr int kB = 4;
 
 __global__ void k_step(Dims D, const float* __restrict__ G, const float4* __restrict__ xh,
                        const int* __restrict__ nbrf, const uint8_t* __restrict__ nnb, const uint8_t* __restrict__ typ,
-                       float fscale, float fsurf, float dt, uint32_t* __restrict__ mask, int replay,
-                       float4* __restrict__ yh, int n) {
+                       float fscale, float fsurf, float dt, const float4* __restrict__ dirs,
+                       uint32_t* __restrict__ mask, int replay, float4* __restrict__ yh, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) {
         return;
@@ -229,7 +260,9 @@ __global__ void k_step(Dims D, const float* __restrict__ G, const float4* __rest
         mask[i] = bits;
     }
     const float s = dt / (float)(act > 1 ? act : 1);
-    yh[i] = with_size(D, G, p.x + s * fx, p.y + s * fy, p.z + s * fz);
+    float ix = s * fx, iy = s * fy, iz = s * fz;
+    project(dirs, i, ix, iy, iz);
+    yh[i] = with_size(D, G, p.x + ix, p.y + iy, p.z + iz);
 }
 
 __global__ void k_loss(const float4* __restrict__ xh, const int* __restrict__ nbrf, const uint8_t* __restrict__ nnb,
@@ -272,7 +305,8 @@ __global__ void k_loss(const float4* __restrict__ xh, const int* __restrict__ nb
 // sizing grid's 8-corner scatter stays on fixed-point atomics.
 //
 // The reverse of step t reads, for every node, one 32-byte record: the state
-// (x_t, h_t), mu = s_t lam_{t+1} (s_t = dt / max(c_t, 1), the node's step scale)
+// (x_t, h_t), mu = s_t P lam_{t+1} (s_t = dt / max(c_t, 1), the node's step scale,
+// P its taped projection or I)
 // and the step's taped mask. A bar pointing at j then costs one load of its
 // source's record.
 struct __align__(32) Rec {
@@ -280,20 +314,23 @@ struct __align__(32) Rec {
     float4 mub;   // mu (3 floats), the taped mask (bits)
 };
 
-__device__ __forceinline__ Rec make_rec(const float4& xh, const float4& lam, uint32_t bits, float dt) {
+__device__ __forceinline__ Rec make_rec(const float4& xh, const float4& lam, uint32_t bits, float dt,
+                                        const float4* __restrict__ dirs, int i) {
     const int act = __popc(bits);
     const float s = dt / (float)(act > 1 ? act : 1);
+    float mx = s * lam.x, my = s * lam.y, mz = s * lam.z;
+    project(dirs, i, mx, my, mz);
     Rec r;
     r.xh = xh;
-    r.mub = make_float4(s * lam.x, s * lam.y, s * lam.z, __uint_as_float(bits));
+    r.mub = make_float4(mx, my, mz, __uint_as_float(bits));
     return r;
 }
 
 __global__ void k_rec(const float4* __restrict__ xh, const float4* __restrict__ lam, const uint32_t* __restrict__ mask,
-                      float dt, Rec* __restrict__ rec, int n) {
+                      float dt, const float4* __restrict__ dirs, Rec* __restrict__ rec, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
-        rec[i] = make_rec(xh[i], lam[i], mask[i], dt);
+        rec[i] = make_rec(xh[i], lam[i], mask[i], dt, dirs, i);
     }
 }
 
@@ -391,7 +428,7 @@ constexpr int kBwdNodes = kT / kRoles;
 __global__ void __launch_bounds__(kT, 4) k_step_bwd_g(Dims D, const float* __restrict__ G, const Rec* __restrict__ rec,
                              const float4* __restrict__ lam_in, const int* __restrict__ nbrf,
                              const uint8_t* __restrict__ typ, float fscale, float fsurf, float dt,
-                             const uint8_t* __restrict__ indeg, const int* __restrict__ tsrcf,
+                             const float4* __restrict__ dirs, const uint8_t* __restrict__ indeg, const int* __restrict__ tsrcf,
                              const uint8_t* __restrict__ tslot, float4* __restrict__ lam_out,
                              const float4* __restrict__ xh_prev, const uint32_t* __restrict__ mask_prev,
                              Rec* __restrict__ rec_prev, unsigned long long* __restrict__ gG, int n) {
@@ -515,7 +552,7 @@ __global__ void __launch_bounds__(kT, 4) k_step_bwd_g(Dims D, const float* __res
     const float4 lo = make_float4((float)l3[0], (float)l3[1], (float)l3[2], 0.0f);
     lam_out[j] = lo;
     if (rec_prev) {
-        rec_prev[j] = make_rec(xh_prev[j], lo, mask_prev[j], dt);
+        rec_prev[j] = make_rec(xh_prev[j], lo, mask_prev[j], dt, dirs, j);
     }
 }
 
@@ -566,6 +603,8 @@ struct v2m_unroll {
     int* nbr = nullptr;              // slot-major lists, bit 31 = the neighbour is not INTERIOR
     uint8_t* nnb = nullptr;
     uint8_t* typ = nullptr;
+    float4* dirs = nullptr;          // taped constraints (direction, kind), or null
+    float4* dirs_buf = nullptr;      // their buffer (kept when they are cleared)
     uint32_t* tape = nullptr;        // K x n
     float4* ck = nullptr;            // nck checkpoints x n
     float4* seg = nullptr;           // (ckpt + 1) x n segment states (x, h)
@@ -653,8 +692,8 @@ void run_steps(v2m_unroll* u, const float* G, const float4* xh, int t0, int t1, 
     const float4* cur = xh;
     for (int t = t0; t < t1; ++t) {
         float4* nxt = seg + (size_t)(t - t0 + 1) * n;
-        k_step<<<blocks(n), kT, 0, st>>>(u->D, G, cur, u->nbr, u->nnb, u->typ, u->fscale, u->fsurf, u->dt,
-                                                u->tape + (size_t)t * n, replay, nxt, n);
+        k_step<<<blocks(n), kT, 0, st>>>(u->D, G, cur, u->nbr, u->nnb, u->typ, u->fscale, u->fsurf, u->dt, u->dirs,
+                                         u->tape + (size_t)t * n, replay, nxt, n);
         cur = nxt;
     }
 }
@@ -900,11 +939,12 @@ int v2m_unroll_backward(v2m_unroll* u, const float* G, const float* gxK, float* 
             Rec* rc = u->rec;
             Rec* rp = u->rec + n;
             k_rec<<<blocks(n), kT, 0, u->stream>>>(b + (size_t)(t1 - 1 - t0) * n, u->lamf,
-                                                   u->tape + (size_t)(t1 - 1) * n, u->dt, rc, n);
+                                                   u->tape + (size_t)(t1 - 1) * n, u->dt, u->dirs, rc, n);
             for (int t = t1 - 1; t >= t0; --t) {
                 const bool more = t > t0;
                 k_step_bwd_g<<<(unsigned)((n + kBwdNodes - 1) / kBwdNodes), kT, 0, u->stream>>>(
-                    u->D, G, rc, u->lamf, u->nbr, u->typ, u->fscale, u->fsurf, u->dt, u->indeg, u->tsrc, u->tslot,
+                    u->D, G, rc, u->lamf, u->nbr, u->typ, u->fscale, u->fsurf, u->dt, u->dirs, u->indeg, u->tsrc,
+                    u->tslot,
                     u->lamb, more ? b + (size_t)(t - 1 - t0) * n : nullptr,
                     more ? u->tape + (size_t)(t - 1) * n : nullptr, more ? rp : nullptr, u->gG, n);
                 std::swap(u->lamf, u->lamb);
@@ -923,6 +963,46 @@ int v2m_unroll_backward(v2m_unroll* u, const float* G, const float* gxK, float* 
             uck(cudaGetLastError(), "launch");
             uck(cudaStreamSynchronize(u->stream), "synchronize");
         }
+    });
+}
+
+// Taped constraints from dirs (host, float [3n]; null clears them): an INTERFACE
+// node's unit interface normal, a JUNCTION node's unit junction-line direction
+// (V2M_ARR_DIRS of a session gives both); entries of other types are ignored,
+// and a zero direction leaves its node free. Directions are normalised here.
+// Invalidates the tape: the next forward pass records a new one.
+int v2m_unroll_set_constraints(v2m_unroll* u, const float* dirs) {
+    return uguard([&] {
+        if (!u) {
+            throw std::invalid_argument("bad argument");
+        }
+        uck(cudaSetDevice(u->device), "cudaSetDevice");
+        uck(cudaStreamSynchronize(u->stream), "synchronize");
+        if (!dirs) {
+            u->dirs = nullptr;
+            u->have_tape = 0;
+            return;
+        }
+        const size_t nn = (size_t)u->n;
+        std::vector<uint8_t> typ(nn);
+        uck(cudaMemcpy(typ.data(), u->typ, nn, cudaMemcpyDeviceToHost), "read types");
+        std::vector<float4> h(nn);
+        for (size_t i = 0; i < nn; ++i) {
+            const float x = dirs[3 * i], y = dirs[3 * i + 1], z = dirs[3 * i + 2];
+            const float kind = typ[i] == V2M_INTERFACE ? 1.0f : (typ[i] == V2M_JUNCTION ? 2.0f : 0.0f);
+            const double r = std::sqrt((double)x * x + (double)y * y + (double)z * z);
+            if (!std::isfinite(r)) {
+                throw std::invalid_argument("constraint direction not finite");
+            }
+            h[i] = (kind == 0.0f || r == 0.0) ? make_float4(0.0f, 0.0f, 0.0f, 0.0f)
+                                              : make_float4((float)(x / r), (float)(y / r), (float)(z / r), kind);
+        }
+        if (!u->dirs_buf) {
+            u->dirs_buf = u->alloc<float4>(nn);
+        }
+        uck(cudaMemcpy(u->dirs_buf, h.data(), 16 * nn, cudaMemcpyHostToDevice), "upload");
+        u->dirs = u->dirs_buf;
+        u->have_tape = 0;
     });
 }
 

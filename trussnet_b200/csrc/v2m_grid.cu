@@ -10,8 +10,12 @@
 //                   pass order and summation order
 //   k_size          per-voxel size: own label, strongest competitor,         [v2m_size_voxel / v2m_kappa_max, src/opencl/v2m_grid_body.cl:321-475]
 //                   curvature bound 1/(K |kappa|)
-//   k_thick_peak    per voxel, the largest own-label phi within +-2 voxels   [v2m_thick_voxel, src/opencl/v2m_grid_body.cl:241-276]
-//                   (its erfinv is taken on the host: it needs the host's logf)
+//   k_thick_peak_bricks  per voxel, the largest own-label phi within +-2    [v2m_thick_voxel, src/opencl/v2m_grid_body.cl:241-276]
+//                   voxels; one block per brick, the halo's labels and phi
+//                   in shared memory
+//   k_thick_pick    the voxels whose thickness needs erfinv, listed; the
+//                   host maps their peaks (erfinv needs the host's logf) and
+//   k_thick_put     scatters the thicknesses back
 //   k_axis_min /    the thin-layer blend weight: min filter, smoothstep,     [src/v2m_grid.cpp:465-527]
 //   k_smoothstep /  Gaussian blur, separable passes on the dense grid
 //   k_axis_blur
@@ -316,35 +320,147 @@ __global__ void k_size(DGrid g, SizeArgs A, float* __restrict__ h) {
     }
 }
 
-// The thickness's device half (v2m_thick_voxel): the largest phi of the
-// voxel's own label over the own-label voxels within +-r; -1 in a uniform brick.
-__global__ void k_thick_peak(DGrid g, int r, float* __restrict__ out) {
-    const int64_t nv = (int64_t)g.nx * g.ny * g.nz;
-    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv; v += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(v % g.nx), j = (int)((v / g.nx) % g.ny), k = (int)(v / ((int64_t)g.nx * g.ny));
-        if (g.bl_slot[brick_index(g, i, j, k)] < 0) {
-            out[v] = -1.0f;
-            continue;
+// The voxels whose thickness needs erfinv (peak m in [0, 0.9999)) listed for the
+// host, the others set to "no thickness" (1e30) here. The list's order varies
+// from run to run; each entry carries its voxel, so the results do not.
+__global__ void k_thick_pick(float* __restrict__ tv, int64_t nv, int* __restrict__ cnt, int* __restrict__ idx,
+                             float* __restrict__ val) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < nv; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t v = base + threadIdx.x;
+        const float m = v < nv ? tv[v] : -1.0f;
+        const bool need = v < nv && m >= 0.0f && m < 0.9999f;
+        if (v < nv && !need) {
+            tv[v] = 1e30f;
         }
-        const int a = g.L[v];
-        float m = 0.0f;
-        for (int dz = -r; dz <= r; ++dz) {
-            for (int dy = -r; dy <= r; ++dy) {
-                for (int dx = -r; dx <= r; ++dx) {
-                    const int u = i + dx, w = j + dy, z = k + dz;
-                    if (u < 0 || w < 0 || z < 0 || u >= g.nx || w >= g.ny || z >= g.nz) {
-                        if (a != 0) {
-                            continue;   // (label_at is 0 outside the grid)
-                        }
-                    } else if (g.L[u + (size_t)g.nx * (w + (size_t)g.ny * z)] != a) {
-                        continue;
-                    }
-                    const float f = phi_voxel(g, a, u, w, z);
-                    m = f > m ? f : m;
-                }
+        const unsigned b = __ballot_sync(0xffffffffu, need);
+        int at = 0;
+        if (lane == 0 && b) {
+            at = atomicAdd(cnt, __popc(b));
+        }
+        at = __shfl_sync(0xffffffffu, at, 0);
+        if (need) {
+            const int k = at + __popc(b & ((1u << lane) - 1u));
+            idx[k] = (int)v;
+            val[k] = m;
+        }
+    }
+}
+
+__global__ void k_thick_put(float* __restrict__ tv, const int* __restrict__ idx, const float* __restrict__ val,
+                            int n) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        tv[idx[k]] = val[k];
+    }
+}
+
+// The thickness's device half (v2m_thick_voxel): the largest phi of the
+// voxel's own label over the own-label voxels within +-2; -1 in a uniform
+// brick. One block per brick, 2 voxels a thread. A mixed
+// brick stages the labels of its (8+4)^3 halo (0 outside the grid, as
+// label_at) and, for each listed label that some voxel of the brick owns, that
+// label's phi over the halo (phi_voxel, outside the grid included); the voxels
+// of that label then take the maximum over their own-label neighbours from
+// shared memory. The maximum starts at +0 and takes f > m, so its value does
+// not depend on the visiting order. A voxel whose label is not among the
+// brick's first V2M_BL (an overflowing brick) takes the per-voxel loop.
+constexpr int kPeakR = 2;
+constexpr int kPeakT = V2M_BS + 2 * kPeakR;   // 12
+
+__global__ void __launch_bounds__(256) k_thick_peak_bricks(DGrid g, float* __restrict__ out) {
+    __shared__ uint16_t lt[kPeakT * kPeakT * kPeakT];
+    __shared__ float pt[kPeakT * kPeakT * kPeakT];
+    const int b = blockIdx.x;
+    const int bx = b % g.nbx, by = (b / g.nbx) % g.nby, bz = b / (g.nbx * g.nby);
+    const int i0 = bx * V2M_BS, j0 = by * V2M_BS, k0 = bz * V2M_BS;
+    int vi[2], vj[2], vk[2], own[2];
+    bool in[2];
+    float m[2] = { 0.0f, 0.0f };
+    bool done[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int t = threadIdx.x + 256 * q;
+        vi[q] = i0 + (t & 7);
+        vj[q] = j0 + ((t >> 3) & 7);
+        vk[q] = k0 + (t >> 6);
+        in[q] = vi[q] < g.nx && vj[q] < g.ny && vk[q] < g.nz;
+        done[q] = !in[q];
+    }
+    const size_t sx = (size_t)g.nx, sxy = (size_t)g.nx * g.ny;
+    if (g.bl_slot[b] < 0) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            if (in[q]) {
+                out[vi[q] + sx * vj[q] + sxy * vk[q]] = -1.0f;
             }
         }
-        out[v] = m;
+        return;
+    }
+    for (int e = threadIdx.x; e < kPeakT * kPeakT * kPeakT; e += 256) {
+        const int u = i0 - kPeakR + e % kPeakT, w = j0 - kPeakR + (e / kPeakT) % kPeakT,
+                  z = k0 - kPeakR + e / (kPeakT * kPeakT);
+        lt[e] = (uint16_t)label_at(g, u, w, z);
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        own[q] = in[q] ? g.L[vi[q] + sx * vj[q] + sxy * vk[q]] : -1;
+    }
+    const int cnt = min(g.bl_cnt[b], V2M_BL);
+    for (int s = 0; s < cnt; ++s) {
+        const int l = g.bl_lab[(size_t)b * V2M_BL + s];
+        if (!__syncthreads_or(own[0] == l || own[1] == l)) {
+            continue;
+        }
+        for (int e = threadIdx.x; e < kPeakT * kPeakT * kPeakT; e += 256) {
+            pt[e] = phi_voxel(g, l, i0 - kPeakR + e % kPeakT, j0 - kPeakR + (e / kPeakT) % kPeakT,
+                              k0 - kPeakR + e / (kPeakT * kPeakT));
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            if (!done[q] && own[q] == l) {
+                const int c = (vi[q] - i0) + kPeakT * ((vj[q] - j0) + kPeakT * (vk[q] - k0));
+                float mm = 0.0f;
+                for (int dz = 0; dz <= 2 * kPeakR; ++dz) {
+                    for (int dy = 0; dy <= 2 * kPeakR; ++dy) {
+                        for (int dx = 0; dx <= 2 * kPeakR; ++dx) {
+                            const int e = c + dx + kPeakT * (dy + kPeakT * dz);
+                            if (lt[e] == l) {
+                                const float f = pt[e];
+                                mm = f > mm ? f : mm;
+                            }
+                        }
+                    }
+                }
+                m[q] = mm;
+                done[q] = true;
+            }
+        }
+        __syncthreads();   // pt is refilled for the next label
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        if (!in[q]) {
+            continue;
+        }
+        if (!done[q]) {   // own label beyond the brick's list: the per-voxel loop
+            const int a = own[q];
+            float mm = 0.0f;
+            for (int dz = -kPeakR; dz <= kPeakR; ++dz) {
+                for (int dy = -kPeakR; dy <= kPeakR; ++dy) {
+                    for (int dx = -kPeakR; dx <= kPeakR; ++dx) {
+                        const int u = vi[q] + dx, w = vj[q] + dy, z = vk[q] + dz;
+                        if (label_at(g, u, w, z) != a) {
+                            continue;
+                        }
+                        const float f = phi_voxel(g, a, u, w, z);
+                        mm = f > mm ? f : mm;
+                    }
+                }
+            }
+            m[q] = mm;
+        }
+        out[vi[q] + sx * vj[q] + sxy * vk[q]] = m[q];
     }
 }
 
@@ -731,29 +847,49 @@ cudaError_t grid_build(const GridBuildArgs& A, GridBuildOut& O, std::string& err
     float* tv = nullptr;
     if (p.thick > 0.0f || p.sigma_thin > 0.0f) {
         V2M_ALLOC(tv, float, nv);
-        k_thick_peak<<<gs_blocks(nv, sms), 256, 0, st>>>(g, 2, tv);
+        k_thick_peak_bricks<<<(unsigned)((int64_t)g.nbx * g.nby * g.nbz), 256, 0, st>>>(g, tv);
         lap("thickness peak");
+        // only the voxels with a peak in [0, 0.9999) need erfinv: listed on the
+        // device, their peaks mapped on the host through the pinned staging
+        // buffers, chunk by chunk, in place, and scattered back
+        int* npick;
+        int* pidx;
+        float* pval;
+        V2M_ALLOC(npick, int, 1);
+        V2M_ALLOC(pidx, int, nv);
+        V2M_ALLOC(pval, float, nv);
+        V2M_TRY(cudaMemsetAsync(npick, 0, 4, st));
+        k_thick_pick<<<gs_blocks(nv, sms), 256, 0, st>>>(tv, (int64_t)nv, npick, pidx, pval);
+        V2M_TRY(cudaGetLastError());
+        int hpick = 0;
+        V2M_TRY(cudaMemcpyAsync(&hpick, npick, 4, cudaMemcpyDeviceToHost, st));
+        V2M_TRY(cudaStreamSynchronize(st));
         const float sg = p.sigma_curv;
         const unsigned nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-        // through the pinned staging buffers, chunk by chunk, in place on the host threads
-        V2M_TRY(staged_map(tv, tv, 4 * (size_t)nv, st, [&](void* buf, size_t bytes, size_t) {
+        V2M_TRY(staged_map(pval, pval, 4 * (size_t)hpick, st, [&](void* buf, size_t bytes, size_t) {
             float* t = static_cast<float*>(buf);
             const int64_t cnt = (int64_t)(bytes / 4);
+            const unsigned nt = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nth, cnt / 65536));
+            auto run = [=](unsigned q) {
+                const int64_t a = cnt * q / nt, b = cnt * (q + 1) / nt;
+                for (int64_t v = a; v < b; ++v) {
+                    t[v] = 2.8284271f * sg * erfinv_giles(t[v]);
+                }
+            };
             std::vector<std::thread> pool;
-            for (unsigned q = 0; q < nth; ++q) {
-                pool.emplace_back([=] {
-                    const int64_t a = cnt * q / nth, b = cnt * (q + 1) / nth;
-                    for (int64_t v = a; v < b; ++v) {
-                        const float m = t[v];
-                        t[v] = (m < 0.0f || m >= 0.9999f) ? 1e30f : 2.8284271f * sg * erfinv_giles(m);
-                    }
-                });
+            for (unsigned q = 1; q < nt; ++q) {
+                pool.emplace_back(run, q);
             }
+            run(0);
             for (auto& th : pool) {
                 th.join();
             }
         }));
-        lap("thickness erfinv (host)");
+        if (hpick > 0) {
+            k_thick_put<<<gs_blocks(hpick, sms), 256, 0, st>>>(tv, pidx, pval, hpick);
+            V2M_TRY(cudaGetLastError());
+        }
+        lap(("thickness erfinv (host, " + std::to_string(hpick) + " voxels)").c_str());
     }
     if (p.thick > 0.0f) {
         const float floor_mm = p.thin_floor * vmin;

@@ -8,6 +8,7 @@
 // round trip and a run of iterations replays as one graph. The host reads the
 // per-volume control blocks only between graph replays, to stop early.
 #include <cuda_runtime.h>
+#include <sys/mman.h>
 
 #include <algorithm>
 #include <climits>
@@ -24,6 +25,7 @@
 #include <stdexcept>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/v2m_cuda.h"
@@ -1066,10 +1068,33 @@ float seed_spacing(int L, int nseed, float hmin, float hmax) {
 // A host array left uninitialized (the device copy writes every element).
 template <typename T>
 struct HostArray {
-    std::unique_ptr<T[]> p;
+    // plain memory (T is an arithmetic type); large arrays 2 MB aligned and
+    // marked for transparent huge pages, which halves their first-touch cost
+    // when the device copies land in them
+    struct Free {
+        void operator()(T* q) const {
+            std::free(q);
+        }
+    };
+    std::unique_ptr<T, Free> p;
     size_t n = 0;
     void resize(size_t count) {
-        p.reset(count ? new T[count] : nullptr);
+        static_assert(std::is_arithmetic<T>::value, "HostArray holds plain numbers");
+        constexpr size_t kHuge = (size_t)2 << 20;
+        const size_t bytes = count * sizeof(T);
+        void* q = nullptr;
+        if (bytes >= 2 * kHuge) {
+            q = std::aligned_alloc(kHuge, (bytes + kHuge - 1) / kHuge * kHuge);
+            if (q) {
+                madvise(q, bytes, MADV_HUGEPAGE);   // advice only: ignored where unsupported
+            }
+        } else if (bytes) {
+            q = std::malloc(bytes);
+        }
+        if (bytes && !q) {
+            throw std::bad_alloc();
+        }
+        p.reset(static_cast<T*>(q));
         n = count;
     }
     T* data() const {
@@ -1525,6 +1550,13 @@ int v2m_session_read_array(v2m_session* s, int vol, int what, void* host, int64_
             std::memcpy(h, c[vol].hist, 32 * 4);
             std::memcpy(h + 32, &c[vol].maxbits, 4);
             h[33] = c[vol].nhalf;
+            break;
+        }
+        case V2M_ARR_DIRS: {
+            need(12LL * n);
+            float* t = (float*)scratch(12 * (size_t)n);
+            launch_constraint_dirs(s->stream, d, vol, n, s->hvols[vol].g.gm < 0, t);
+            d2h(t, 12LL * n);
             break;
         }
         case V2M_ARR_SERIAL_SUMS: {

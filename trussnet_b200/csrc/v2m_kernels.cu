@@ -1432,6 +1432,46 @@ __global__ void k_set_rebuild(VolCtl* ctl, int nvol, int val, Global* G) {
     }
 }
 
+// The constraint direction of each node of one volume at its current position,
+// for the differentiable unroll's trapped steps: an INTERFACE node's unit normal
+// of psi_(own, partner) (it glides in the tangent plane), a JUNCTION node's unit
+// junction-line direction, normal_(own, partner 1) x normal_(own, partner 2)
+// (it moves along the line); zero for the others or where a gradient vanishes.
+template <bool kShape>
+__global__ void k_constraint_dirs(const DVol* __restrict__ vols, int v, const float4* __restrict__ Pq,
+                                  const uint8_t* __restrict__ typ, const uint16_t* __restrict__ lab,
+                                  const uint32_t* __restrict__ part, float* __restrict__ out) {
+    const DVol& V = vols[v];
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= V.n) {
+        return;
+    }
+    const int64_t i = V.nofs + t;
+    const int ty = typ[i];
+    float d[3] = { 0.0f, 0.0f, 0.0f };
+    if (ty == V2M_INTERFACE || ty == V2M_JUNCTION) {
+        const float4 p = Pq[i];
+        const int a = lab[i], b = (int)(part[i] & 0xFFFFu), c = (int)(part[i] >> 16);
+        const float4 g1 = psi_grad4<kShape>(V.g, a, b, p.x, p.y, p.z);
+        float u[3] = { g1.x, g1.y, g1.z };
+        if (ty == V2M_JUNCTION) {
+            const float4 g2 = psi_grad4<kShape>(V.g, a, c, p.x, p.y, p.z);
+            u[0] = g1.y * g2.z - g1.z * g2.y;
+            u[1] = g1.z * g2.x - g1.x * g2.z;
+            u[2] = g1.x * g2.y - g1.y * g2.x;
+        }
+        const float un = sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+        if (un > 0.0f) {
+            d[0] = u[0] / un;
+            d[1] = u[1] / un;
+            d[2] = u[2] / un;
+        }
+    }
+    out[3 * t] = d[0];
+    out[3 * t + 1] = d[1];
+    out[3 * t + 2] = d[2];
+}
+
 // Row-major copy of the slot-major lists of one volume (for checks and read-back).
 __global__ void k_lists_rowmajor(const int* __restrict__ nbr, const uint8_t* __restrict__ nnb, int64_t nofs, int n,
                                  int64_t N, int* __restrict__ out, int* __restrict__ nout) {
@@ -1624,6 +1664,14 @@ void launch_refresh(cudaStream_t s, const Dev& d, int blocks) {
 
 void launch_set_rebuild(cudaStream_t s, const Dev& d, int val) {
     k_set_rebuild<<<nblk(d.nvol, 128), 128, 0, s>>>(d.ctl, d.nvol, val, d.G);
+}
+
+void launch_constraint_dirs(cudaStream_t s, const Dev& d, int v, int n, bool shape, float* out) {
+    if (shape) {
+        k_constraint_dirs<true><<<nblk(n, 256), 256, 0, s>>>(d.vols, v, d.Pq, d.typ, d.lab, d.part, out);
+    } else {
+        k_constraint_dirs<false><<<nblk(n, 256), 256, 0, s>>>(d.vols, v, d.Pq, d.typ, d.lab, d.part, out);
+    }
 }
 
 void launch_lists_rowmajor(cudaStream_t s, const Dev& d, int64_t nofs, int n, int* out, int* nout) {

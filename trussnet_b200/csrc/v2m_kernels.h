@@ -99,6 +99,7 @@ void launch_xfill(cudaStream_t s, const DGrid& g, const int2* tabs, float* xphi,
 void launch_refresh(cudaStream_t s, const Dev& d, int blocks);
 void launch_set_rebuild(cudaStream_t s, const Dev& d, int val);
 void launch_lists_rowmajor(cudaStream_t s, const Dev& d, int64_t nofs, int n, int* out, int* nout);
+void launch_constraint_dirs(cudaStream_t s, const Dev& d, int v, int n, bool shape, float* out);
 void launch_lists_from_rowmajor(cudaStream_t s, const Dev& d, int64_t nofs, int n, const int* in, const int* nin);
 void launch_pack_nodes(cudaStream_t s, const Dev& d, int v, int n, const float* P, const uint8_t* typ_all);
 void launch_unpack_P(cudaStream_t s, const Dev& d, int64_t nofs, int n, float* P);

@@ -29,9 +29,9 @@ from .types import (ARR, V2M_K, Grid, GridParams, GridParamsC, GridView, Nodes, 
 
 _ARR_DTYPE = {"key": np.int32, "sorted": np.int32, "cstart": np.int32, "Ps": np.float32, "nbr": np.int32,
               "nnb": np.int32, "F": np.float32, "hn": np.float32, "mv": np.float32, "V": np.float32, "pw": np.float32,
-              "P0": np.float32, "hist": np.int32, "serial_sums": np.int32, "P": np.float32, "typ": np.uint8, "part": np.uint16}
+              "P0": np.float32, "hist": np.int32, "serial_sums": np.int32, "dirs": np.float32, "P": np.float32, "typ": np.uint8, "part": np.uint16}
 _PER_NODE = {"key": 1, "sorted": 1, "Ps": 4, "nbr": V2M_K, "nnb": 1, "F": 4, "hn": 1, "mv": 1, "V": 3, "pw": 1,
-             "P0": 3, "P": 3, "typ": 1, "part": 2}
+             "P0": 3, "P": 3, "typ": 1, "part": 2, "dirs": 3}
 
 
 def device_count() -> int:
@@ -114,16 +114,27 @@ def grid_cl(L: np.ndarray, vs=(1.0, 1.0, 1.0), prm: GridParams | None = None, de
     vsa = np.asarray(vs, np.float32)
     h = C.c_void_p()
     _lib.check(lib.v2m_grid_build_cuda(L.ctypes.data, nx, ny, nz, vsa.ctypes.data, C.byref(pc), device, C.byref(h)))
-    try:
-        gv = GridView()
-        _lib.check(lib.v2m_grid_result_view(h, C.byref(gv)))
-        g = Grid.from_view(gv)
-        R = C.c_int32()
-        _lib.check(lib.v2m_grid_result_info(h, None, C.byref(R), None, None))
-        g.R = R.value
-    finally:
-        lib.v2m_grid_free(h)
+    owner = _GridResult(lib, h)
+    gv = GridView()
+    _lib.check(lib.v2m_grid_result_view(h, C.byref(gv)))
+    g = Grid.from_view(gv, owner)   # the grid's arrays are the result's host memory, no copy
+    R = C.c_int32()
+    _lib.check(lib.v2m_grid_result_info(h, None, C.byref(R), None, None))
+    g.R = R.value
     return g
+
+
+class _GridResult:
+    """Owner of a v2m_grid_result's host arrays: freed when the last array
+    viewing them is gone (the result holds host memory only)."""
+
+    def __init__(self, lib, h):
+        self.lib, self.h = lib, h
+
+    def __del__(self):
+        if self.h:
+            self.lib.v2m_grid_free(self.h)
+            self.h = None
 
 
 def points_cl(L: np.ndarray, vs=(1.0, 1.0, 1.0), gprm: GridParams | None = None, prm: RelaxParams | None = None,

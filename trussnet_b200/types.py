@@ -22,7 +22,7 @@ V2M_NOLAB = 0xFFFF
 V2M_INTERIOR, V2M_INTERFACE, V2M_JUNCTION, V2M_CORNER = 0, 1, 2, 3
 
 # internal arrays (V2M_ARR_* of include/v2m_cuda.h)
-ARR = dict(key=1, sorted=2, cstart=3, Ps=4, nbr=5, nnb=6, F=7, hn=8, mv=9, V=10, pw=11, P0=12, hist=13, serial_sums=14,
+ARR = dict(key=1, sorted=2, cstart=3, Ps=4, nbr=5, nnb=6, F=7, hn=8, mv=9, V=10, pw=11, P0=12, hist=13, serial_sums=14, dirs=15,
            P=20, typ=21, part=22)
 
 
@@ -203,14 +203,20 @@ class Grid:
         return v
 
     @classmethod
-    def from_view(cls, v: GridView) -> "Grid":
-        """Copy a C view's arrays into a Grid."""
+    def from_view(cls, v: GridView, owner=None) -> "Grid":
+        """A Grid of a C view's arrays: copies, or (owner given) views of the
+        view's own memory that keep `owner`, the holder of that memory, alive
+        for as long as any of them lives."""
         nv = v.nx * v.ny * v.nz
         nb = v.nbx * v.nby * v.nbz
 
         def arr(ptr, dtype, count):
             if not ptr or count == 0:
                 return np.zeros(0, dtype)
+            if owner is not None:
+                buf = (C.c_char * (count * np.dtype(dtype).itemsize)).from_address(ptr)
+                buf._owner = owner
+                return np.frombuffer(buf, dtype, count)
             return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(np.ctypeslib.as_ctypes_type(dtype))),
                                          shape=(count,)).copy()
         g = cls(nx=v.nx, ny=v.ny, nz=v.nz, vs=tuple(v.vs),
