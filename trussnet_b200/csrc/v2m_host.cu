@@ -719,7 +719,8 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
         s->typ0 = s->alloc<uint8_t>(N);
         s->part0 = s->alloc<uint32_t>(N);
         ck(cudaMemsetAsync(d.nnb, 0, N, s->stream), "memset");
-        ck(cudaMemsetAsync(d.nbr, 0, sizeof(int) * (size_t)N * V2M_K, s->stream), "memset");
+        launch_lists_init(s->stream, d);
+        ck(cudaGetLastError(), "list init");
         ck(cudaMemsetAsync(d.Pq, 0, sizeof(float4) * N, s->stream), "memset");
         ck(cudaMemsetAsync(d.P0, 0, sizeof(float4) * N, s->stream), "memset");
         ck(cudaMemsetAsync(d.Ps, 0, sizeof(float4) * N, s->stream), "memset");

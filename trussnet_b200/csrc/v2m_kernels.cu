@@ -607,8 +607,9 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
     // final ranks
     m = warp_validate(sm, m, lane, i, ti_int, li, sorted, typ, lab);
     m = warp_prune(sm, m, lane);
-    if (lane < m) {
-        nbr[(int64_t)lane * N + i] = sm.id[lane];
+    // slots past m hold the node's own id (k_force loads whole batches of slots)
+    if (lane < V2M_K) {
+        nbr[(int64_t)lane * N + i] = lane < m ? sm.id[lane] : (int)i;
     }
     if (lane == 0) {
         nnb[i] = (uint8_t)m;
@@ -689,7 +690,25 @@ constexpr int kForceBatch = 4;
 // entries are one coalesced 128-byte row; neighbour position + signed size is
 // one 16-byte gather. Bars are added in list order, as v2m_force does: the
 // deterministic ordered fold of the node's CSR row (no float atomics).
-__global__ void __launch_bounds__(256, 4) k_force(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
+//
+// The kernel is bound by those gathers: a warp's request for the k-th
+// neighbours of its 32 nodes touches ~29 distinct 32-byte sectors, and the L1's
+// per-request wavefronts, not DRAM (whose traffic equals the algorithmic bytes),
+// set its time. It therefore keeps its own instructions and registers low:
+//   - the ids arrive in batches of kForceBatch, the next batch's ids loaded
+//     while the current batch's positions are in flight (no id array held in
+//     registers: 48 registers, 5 blocks of 256 per multiprocessor);
+//   - list slots past nnb hold the node's own id (every list writer pads them),
+//     so the loads need no per-slot predicate; a padded bar is excluded from
+//     the fold by its slot index, exactly as the reference's loop bound does;
+//   - the size factor of a bar is (node factor if the neighbour is
+//     non-interior, else fscale / 2), the node factor being fsurf / 2 for a
+//     non-interior node and fscale / 2 otherwise: the same products as
+//     ((both non-interior) ? fsurf : fscale) * 0.5f, since halving is exact.
+// A list id outside the node's volume (a corrupted list) is clamped into it, so
+// that no gather leaves the volume's nodes, and reported after the fold through
+// the largest offset seen: the check feeds neither the loop nor the addresses.
+__global__ void __launch_bounds__(256, 5) k_force(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
                                                const uint16_t* __restrict__ nodevol, const float4* __restrict__ Pq,
                                                const int* __restrict__ nbr, const uint8_t* __restrict__ nnb,
                                                float4* __restrict__ F, int64_t N, Global* G) {
@@ -706,52 +725,46 @@ __global__ void __launch_bounds__(256, 4) k_force(const DVol* __restrict__ vols,
     if (c.done || c.it >= V.max_iters) {
         return;
     }
-    const float fscale = V.fscale, fsurf = V.fsurf;
+    const float fsh = V.fscale * 0.5f, fuh = V.fsurf * 0.5f;
     const float4 p = Pq[i];
     const float hi = fabsf(p.w);
-    const bool ni = signbit(p.w);
+    const float cneg = signbit(p.w) ? fuh : fsh;
     const int n = nnb[i];
-    float fx = 0.0f, fy = 0.0f, fz = 0.0f, fa = 0.0f;
+    const unsigned lo = (unsigned)V.nofs, top = (unsigned)V.n - 1u;
+    const float4* __restrict__ Pv = Pq + lo;
     const int* row = nbr + i;
-    // every id first (one round trip: the slot-major rows are coalesced), then
-    // the positions in batches of kForceBatch, so that a node's dependent chain
-    // is 1 + ceil(nnb / 4) memory round trips rather than 2 ceil(nnb / 4); the
-    // bars are still added one by one in list order. A list id outside the
-    // node's volume (a corrupted list) is clamped into it, so that no gather
-    // leaves the volume's nodes, and reported after the fold: the check feeds
-    // neither the loop nor the addresses' dependences on the other ids.
-    int jj[V2M_K];
-    const int m = n;
-    const unsigned lo = (unsigned)V.nofs, span = (unsigned)V.n;
-    unsigned bad = 0u;
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f, fa = 0.0f;
+    unsigned mx = 0u;
+    int jn[kForceBatch];
 #pragma unroll
-    for (int k = 0; k < V2M_K; ++k) {
-        const int j = k < n ? __ldg(row + (int64_t)k * N) : (int)i;
-        const unsigned r = (unsigned)j - lo;
-        bad |= k < n && r >= span;
-        jj[k] = r < span ? j : (int)lo;
+    for (int u = 0; u < kForceBatch; ++u) {
+        jn[u] = __ldg(row + (int64_t)u * N);
     }
 #pragma unroll
     for (int k0 = 0; k0 < V2M_K; k0 += kForceBatch) {
-        if (k0 >= m) {
+        if (k0 >= n) {
             break;
         }
         float4 qq[kForceBatch];
 #pragma unroll
         for (int u = 0; u < kForceBatch; ++u) {
-            qq[u] = __ldg(Pq + (k0 + u < m ? jj[k0 + u] : (int)i));
+            const unsigned r = (unsigned)jn[u] - lo;
+            mx = max(mx, r);
+            qq[u] = __ldg(Pv + min(r, top));
+        }
+        if (k0 + kForceBatch < V2M_K) {
+#pragma unroll
+            for (int u = 0; u < kForceBatch; ++u) {
+                jn[u] = __ldg(row + (int64_t)(k0 + kForceBatch + u) * N);
+            }
         }
 #pragma unroll
         for (int u = 0; u < kForceBatch; ++u) {
-            if (k0 + u >= m) {
-                break;
-            }
             const float4 q = qq[u];
             const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
             const float l = sqrtf(ex * ex + ey * ey + ez * ez);
-            const float hj = fabsf(q.w);
-            const float l0 = ((ni && signbit(q.w)) ? fsurf : fscale) * 0.5f * (hi + hj);
-            if (l >= l0 || l <= 0.0f) {
+            const float l0 = (__float_as_int(q.w) < 0 ? cneg : fsh) * (hi + fabsf(q.w));
+            if (k0 + u >= n || l >= l0 || l <= 0.0f) {
                 continue;
             }
             const float f = (l0 - l) / l;
@@ -762,7 +775,7 @@ __global__ void __launch_bounds__(256, 4) k_force(const DVol* __restrict__ vols,
         }
     }
     F[i] = make_float4(fx, fy, fz, fa);
-    if (bad) {
+    if (mx > top) {
         raise_error(G, 3, (int)i);
     }
 }
@@ -1472,6 +1485,15 @@ __global__ void k_constraint_dirs(const DVol* __restrict__ vols, int v, const fl
     out[3 * t + 2] = d[2];
 }
 
+// Every list slot holds the node's own id until a list build writes it (the
+// force kernel loads whole batches of slots, padding included).
+__global__ void k_lists_init(int* __restrict__ nbr, int64_t N) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < N * V2M_K) {
+        nbr[t] = (int)(t % N);
+    }
+}
+
 // Row-major copy of the slot-major lists of one volume (for checks and read-back).
 __global__ void k_lists_rowmajor(const int* __restrict__ nbr, const uint8_t* __restrict__ nnb, int64_t nofs, int n,
                                  int64_t N, int* __restrict__ out, int* __restrict__ nout) {
@@ -1498,9 +1520,7 @@ __global__ void k_lists_from_rowmajor(int* __restrict__ nbr, uint8_t* __restrict
     const int64_t i = t / V2M_K;
     const int k = (int)(t % V2M_K);
     const int c = nin[i];
-    if (k < c) {
-        nbr[(int64_t)k * N + nofs + i] = in[t] + (int)nofs;
-    }
+    nbr[(int64_t)k * N + nofs + i] = k < c ? in[t] + (int)nofs : (int)(nofs + i);   // padded with the node's own id
     if (k == 0) {
         nnb[nofs + i] = (uint8_t)c;
     }
@@ -1672,6 +1692,10 @@ void launch_constraint_dirs(cudaStream_t s, const Dev& d, int v, int n, bool sha
     } else {
         k_constraint_dirs<false><<<nblk(n, 256), 256, 0, s>>>(d.vols, v, d.Pq, d.typ, d.lab, d.part, out);
     }
+}
+
+void launch_lists_init(cudaStream_t s, const Dev& d) {
+    k_lists_init<<<nblk(d.N * V2M_K, 256), 256, 0, s>>>(d.nbr, d.N);
 }
 
 void launch_lists_rowmajor(cudaStream_t s, const Dev& d, int64_t nofs, int n, int* out, int* nout) {

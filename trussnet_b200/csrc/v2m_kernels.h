@@ -98,6 +98,7 @@ void launch_xcount(cudaStream_t s, const DGrid& g, uint4* xbrick, int* xn, int n
 void launch_xfill(cudaStream_t s, const DGrid& g, const int2* tabs, float* xphi, int ntab);
 void launch_refresh(cudaStream_t s, const Dev& d, int blocks);
 void launch_set_rebuild(cudaStream_t s, const Dev& d, int val);
+void launch_lists_init(cudaStream_t s, const Dev& d);
 void launch_lists_rowmajor(cudaStream_t s, const Dev& d, int64_t nofs, int n, int* out, int* nout);
 void launch_constraint_dirs(cudaStream_t s, const Dev& d, int v, int n, bool shape, float* out);
 void launch_lists_from_rowmajor(cudaStream_t s, const Dev& d, int64_t nofs, int n, const int* in, const int* nin);
