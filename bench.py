@@ -175,7 +175,33 @@ def cpu_baseline(g, nd, prm, iters):
         cores = min(cores, cap) if cap > 0 else cores
     return {"value": nd.size() * iters / dt, "unit": UNIT, "cores": cores, "kind": "reference",
             "sample": f"relax_cpu on the same grid and seeds, {iters} iterations (first list build included), "
-                      f"{dt:.2f} s"}
+                      f"{dt:.2f} s", "_nodes": a, "_seeds": nd, "_params": p}
+
+
+def parity_check(g, cb, local):
+    """The bench's own output check: relax_cl (the CUDA path, through the C ABI)
+    on the CPU baseline's sample -- the same grid, seeds and iterations -- compared
+    bit for bit (positions, types, partners) with the reference's relax_cpu result,
+    or, where the parameters use an extension of the loop that the reference lacks,
+    with the plain-C restatement's."""
+    from trussnet_b200 import relax_cl
+    ref = cb.pop("_nodes")
+    p = cb.pop("_params")
+    seeds = cb.pop("_seeds")
+    against = "relax_cpu (oracle/_ref, the compiled reference)"
+    if p.rebuild_policy != 0 or p.h_mode != 0 or p.rebuild_div != 0:
+        # an extension of the loop the reference does not have: checked against the
+        # plain-C restatement, which implements it (the reference sample is timing only)
+        from oracle.oracle import Oracle
+        ref = seeds.copy()
+        Oracle("f32").relax(g, p, ref)
+        against = "the plain-C FP32 restatement (oracle/v2m_oracle.c): the parameters use an extension"
+    dev = seeds.copy()
+    st = relax_cl(g, p, dev, device=local)
+    same = {"P": bool(np.array_equal(dev.P.view(np.uint32), ref.P.view(np.uint32))),
+            "typ": bool(np.array_equal(dev.typ, ref.typ)), "part": bool(np.array_equal(dev.part, ref.part))}
+    return {"against": against, "iterations": p.max_iters,
+            "nodes": int(ref.size()), "list_builds": st.rebuilds, "bit_exact": all(same.values()), **same}
 
 
 def dist_setup(args):
@@ -668,8 +694,11 @@ def run_cuda(args):
     if args.e2e_steps > 0:
         e2e = e2e_leg(args, g, nd, prm, n, iters, world, local, barrier)
     cb = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(g, nd, prm, args.ref_iters)
+        if cb is not None:
+            parity = parity_check(g, cb, local)
     adj = adjoint_leg(local) if rank == 0 and world == 1 and args.e2e_steps > 0 else None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -682,7 +711,7 @@ def run_cuda(args):
                                                                              st.n_junction, st.n_corner]},
                 "clocks": clocks, "e2e": e2e, "gpu_launches": int(cnt["launches"]), "roofline": roofline,
                 "move_roofline": move_roofline,
-                "stage_ms_first100": stages, "cpu_baseline": cb, "adjoint": adj}
+                "stage_ms_first100": stages, "cpu_baseline": cb, "parity": parity, "adjoint": adj}
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()

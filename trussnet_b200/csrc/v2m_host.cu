@@ -695,6 +695,7 @@ v2m_session* create(int nvol, const v2m_grid_view* gv, const v2m_relax_params* p
         d.Vel = s->alloc<float4>(N);
         d.P0 = s->alloc<float4>(N);
         d.Ps = s->alloc<float4>(N);
+        d.Js = s->alloc<int2>(N);
         d.typ = s->alloc<uint8_t>(N);
         d.lab = s->alloc<uint16_t>(N);
         d.part = s->alloc<uint32_t>(N);

@@ -269,8 +269,16 @@ __global__ void k_scatter(const VolCtl* __restrict__ ctl, const DVol* __restrict
     }
 }
 
+// The label test of a candidate, taken in bin order with its id: the label in
+// the low 16 bits, bit 16 set for an INTERIOR node.
+__device__ __forceinline__ int snap_info(int ty, int lb) {
+    return lb | (ty == V2M_INTERIOR ? 0x10000 : 0);
+}
+
 // One thread per bin: the bin's ids ascending (the CPU's stable counting sort,
-// src/v2m_particles.cpp:791-795), then their positions and sizes in bin order.
+// src/v2m_particles.cpp:791-795), then their positions and sizes in bin order,
+// and beside them (Js) each slot's id and label test (snap_info) as they are at
+// this build, for the full list build that follows.
 // A bin of more than kSmallBin ids is handed to the whole block
 // (block_bin_sort, over `tmp` at the same offsets), so the work stays linear in
 // the bin's size: clustered or coincident nodes cannot stall one thread.
@@ -278,7 +286,9 @@ __global__ void __launch_bounds__(kBinSortThreads) k_binsort(const DVol* __restr
                                                           const int16_t* __restrict__ tilevol,
                                                           const int* __restrict__ cstart, int* __restrict__ sorted,
                                                           int* __restrict__ tmp, const float4* __restrict__ Pq,
-                                                          float4* __restrict__ Ps, int64_t KT, const Global* G) {
+                                                          const uint8_t* __restrict__ typ, const uint16_t* __restrict__ lab,
+                                                          float4* __restrict__ Ps, int2* __restrict__ Js, int64_t KT,
+                                                          const Global* G) {
     __shared__ BinSortSmem sm;
     __shared__ int64_t big[kBinSortThreads];
     __shared__ int nbig;
@@ -298,8 +308,10 @@ __global__ void __launch_bounds__(kBinSortThreads) k_binsort(const DVol* __restr
                 if (s1 - s0 <= kSmallBin) {
                     small_bin_sort(sorted + s0, s1 - s0);
                     for (int s = s0; s < s1; ++s) {
-                        const float4 p = Pq[sorted[s]];
+                        const int j = sorted[s];
+                        const float4 p = Pq[j];
                         Ps[s] = make_float4(p.x, p.y, p.z, fabsf(p.w));
+                        Js[s] = make_int2(j, snap_info(typ[j], lab[j]));
                     }
                 } else {
                     big[atomicAdd(&nbig, 1)] = e;
@@ -312,8 +324,10 @@ __global__ void __launch_bounds__(kBinSortThreads) k_binsort(const DVol* __restr
             const int s0 = cstart[big[q]], s1 = cstart[big[q] + 1];
             block_bin_sort(sorted + s0, tmp + s0, s1 - s0, sm);
             for (int s = s0 + threadIdx.x; s < s1; s += kBinSortThreads) {
-                const float4 p = Pq[sorted[s]];
+                const int j = sorted[s];
+                const float4 p = Pq[j];
                 Ps[s] = make_float4(p.x, p.y, p.z, fabsf(p.w));
+                Js[s] = make_int2(j, snap_info(typ[j], lab[j]));
             }
             __syncthreads();
         }
@@ -435,10 +449,19 @@ __device__ __forceinline__ float axis_gap(float p, int c, float o, float b, int 
     return 0.0f;
 }
 
+// kSnap: the full list build, right after the hash build: each candidate's id
+// and label test come from the build's bin-order snapshot (Js) in the same
+// coalesced load round as its position, and are applied in the scan, so the
+// buffer holds accepted entries only. Otherwise (the self-refresh between
+// builds, where types may have changed since the snapshot) the scan appends
+// distance-tested candidates and warp_validate checks them against the
+// current typ / lab arrays.
+template <bool kSnap>
 __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& sm, const float4* __restrict__ Pq,
                                const uint8_t* __restrict__ typ, const uint16_t* __restrict__ lab,
                                const int* __restrict__ cstart, const int* __restrict__ sorted,
-                               const float4* __restrict__ Ps, int* __restrict__ nbr, uint8_t* __restrict__ nnb, int64_t N) {
+                               const float4* __restrict__ Ps, const int2* __restrict__ Js, int* __restrict__ nbr,
+                               uint8_t* __restrict__ nnb, int64_t N) {
     const DHash& H = V.H;
     const float4 pi = Pq[i];
     const float px = pi.x, py = pi.y, pz = pi.z;
@@ -574,28 +597,40 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
             const int lo = before + __popc(ends & ((2u << lane) - 1u));
             const int bs0 = __shfl_sync(0xffffffffu, s0, lo & 31);
             const int bexc = __shfl_sync(0xffffffffu, incl - c, lo & 31);
-            // the distance test only; the rest waits for warp_validate
+            // kSnap: every test here; else the distance test only, the rest
+            // waits for warp_validate
             bool ok = false;
             float d2 = 0.0f;
-            int sidx = 0;
+            int sidx = 0, jid = 0;
             if (q < total) {
                 sidx = bs0 + (q - bexc);
                 const float4 ps = Ps[sidx];
+                int2 js = make_int2(0, 0);
+                if (kSnap) {
+                    js = Js[sidx];
+                }
                 const float ex = ps.x - px, ey = ps.y - py, ez = ps.z - pz;
                 d2 = ex * ex + ey * ey + ez * ez;
                 const float rj = ts * 0.5f * (hi + ps.w);
                 ok = !(d2 >= rj * rj) && !(d2 > bd2);   // (a NaN distance is kept, as before)
+                if (kSnap) {
+                    jid = js.x;
+                    ok = ok && jid != (int)i &&
+                         !(ti_int && (js.y & 0x10000) && (js.y & 0xFFFF) != li);
+                }
             }
             const unsigned mask = __ballot_sync(0xffffffffu, ok);
             if (ok) {
                 const int slot = m + __popc(mask & ((1u << lane) - 1u));
-                sm.d[slot] = d2;
-                sm.id[slot] = -sidx - 1;
+                sm.d[slot] = kSnap ? sqrtf(d2) : d2;
+                sm.id[slot] = kSnap ? jid : -sidx - 1;
             }
             m += __popc(mask);
             __syncwarp();
             if (m > kCap - 32) {
-                m = warp_validate(sm, m, lane, i, ti_int, li, sorted, typ, lab);
+                if (!kSnap) {
+                    m = warp_validate(sm, m, lane, i, ti_int, li, sorted, typ, lab);
+                }
                 m = warp_prune(sm, m, lane);
                 if (m == V2M_K) {
                     const float bd = sm.d[V2M_K - 1] * 1.0001f;
@@ -605,7 +640,9 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
         }
     }
     // final ranks
-    m = warp_validate(sm, m, lane, i, ti_int, li, sorted, typ, lab);
+    if (!kSnap) {
+        m = warp_validate(sm, m, lane, i, ti_int, li, sorted, typ, lab);
+    }
     m = warp_prune(sm, m, lane);
     // slots past m hold the node's own id (k_force loads whole batches of slots)
     if (lane < V2M_K) {
@@ -623,8 +660,9 @@ __global__ void __launch_bounds__(kNbrMaxThreads, 4) k_neighbors(const DVol* __r
                                                            const uint16_t* __restrict__ nodevol, const float4* __restrict__ Pq,
                                                            const uint8_t* __restrict__ typ, const uint16_t* __restrict__ lab,
                                                            const int* __restrict__ cstart, const int* __restrict__ sorted,
-                                                           const float4* __restrict__ Ps, int* __restrict__ nbr,
-                                                           uint8_t* __restrict__ nnb, int64_t N, const Global* G) {
+                                                           const float4* __restrict__ Ps, const int2* __restrict__ Js,
+                                                           int* __restrict__ nbr, uint8_t* __restrict__ nnb, int64_t N,
+                                                           const Global* G) {
     __shared__ NbrWarpSmem sm[kNbrMaxThreads / 32];
     if (!*((volatile const int*)&G->rebuild_any)) {
         return;
@@ -636,7 +674,7 @@ __global__ void __launch_bounds__(kNbrMaxThreads, 4) k_neighbors(const DVol* __r
         if (v == 0xFFFF || !ctl[v].rebuild) {
             continue;
         }
-        warp_neighbors(vols[v], i, lane, sm[w], Pq, typ, lab, cstart, sorted, Ps, nbr, nnb, N);
+        warp_neighbors<true>(vols[v], i, lane, sm[w], Pq, typ, lab, cstart, sorted, Ps, Js, nbr, nnb, N);
     }
 }
 
@@ -660,7 +698,7 @@ __global__ void __launch_bounds__(kNbrMaxThreads, 4) k_refresh(const DVol* __res
         if (ctl[v].done) {
             continue;
         }
-        warp_neighbors(vols[v], i, lane, sm[w], Pq, typ, lab, cstart, sorted, Ps, nbr, nnb, N);
+        warp_neighbors<false>(vols[v], i, lane, sm[w], Pq, typ, lab, cstart, sorted, Ps, nullptr, nbr, nnb, N);
         if (lane == 0) {
             const float4 p = Pq[i];
             P0[i] = make_float4(p.x, p.y, p.z, 0.0f);
@@ -1632,14 +1670,14 @@ void launch_scan(cudaStream_t s, const Dev& d) {
 void launch_scatter(cudaStream_t s, const Dev& d) {
     k_scatter<<<gsblocks(d, d.N, 256), 256, 0, s>>>(d.ctl, d.vols, d.nodevol, d.key, d.cursor, d.sorted, d.N, d.G);
     k_binsort<<<gsblocks(d, d.KT, kBinSortThreads), kBinSortThreads, 0, s>>>(d.vols, d.ctl, d.tilevol, d.cstart,
-                                                                             d.sorted, d.sort_tmp, d.Pq, d.Ps, d.KT,
-                                                                             d.G);
+                                                                             d.sorted, d.sort_tmp, d.Pq, d.typ, d.lab,
+                                                                             d.Ps, d.Js, d.KT, d.G);
 }
 
 void launch_neighbors(cudaStream_t s, const Dev& d, int threads) {
     k_neighbors<<<gsblocks(d, d.N, threads / 32) * 2, threads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.typ, d.lab,
-                                                                        d.cstart, d.sorted, d.Ps, d.nbr, d.nnb, d.N,
-                                                                        d.G);
+                                                                        d.cstart, d.sorted, d.Ps, d.Js, d.nbr, d.nnb,
+                                                                        d.N, d.G);
 }
 
 void launch_force(cudaStream_t s, const Dev& d, int threads) {

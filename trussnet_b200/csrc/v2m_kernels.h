@@ -65,6 +65,7 @@ struct Dev {
     float4* Vel = nullptr;         // FIRE velocity
     float4* P0 = nullptr;          // positions at the last list build
     float4* Ps = nullptr;          // bin-order positions + h at the last build
+    int2* Js = nullptr;            // bin-order node id and label test (snap_info) at the last build
     uint8_t* typ = nullptr;
     uint16_t* lab = nullptr;
     uint32_t* part = nullptr;      // two uint16 partner labels
