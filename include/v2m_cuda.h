@@ -69,6 +69,9 @@ typedef struct {
     int32_t gm;                  /* number of gray thresholds; 0 = label volume; < 0 = analytic shape fields */
     int64_t ngTW;                /* floats in gTW (tn::Grid::gTW.size()); 0 = 2 gm (gray-scale) */
     const uint8_t* grade;        /* nx*ny*nz size grades (tn::Grid::grade): seeding only, may be NULL */
+    const float* feat;           /* shape input's sharp features (tn::Grid::feat, grid mm, the layout of
+                                    src/v2m_sdfshape.h ShapeScene::feat): seeding pins nodes on them; may be NULL */
+    int64_t nfeat;               /* floats in feat */
 } v2m_grid_view;
 
 /*
@@ -133,11 +136,13 @@ int v2m_relax_cuda(const v2m_grid_view* g, const v2m_relax_params* prm, v2m_node
 
 /*
  * Seeding on CUDA device `device` (-1 = device 0): tn::seed_cpu
- * (src/v2m_particles.cpp:625-726) without its shape-feature pass -- the graded
- * HCP lattice of the grid's size grades (g->grade is required), each node
- * classified onto its interface or junction curve, the junction-line seeds
- * (params->jseed > 0) with the lattice nodes near them dropped, and the CORNER
- * nodes (params->corners), in the reference's order and bit for bit. Uses
+ * (src/v2m_particles.cpp:625-726) -- the graded HCP lattice of the grid's size
+ * grades (g->grade is required), each node classified onto its interface or
+ * junction curve, the junction-line seeds (params->jseed > 0) with the lattice
+ * nodes near them dropped, the CORNER nodes (params->corners), and, for shape
+ * input with features (g->feat, read on the host), the feature pass
+ * (add_feature_nodes, :304-623: CORNER nodes pinned on the sharp features, the
+ * seeds within 0.4 h of them dropped), in the reference's order and bit for bit. Uses
  * nseed, jseed, corners and voxel_trap of the parameters. *n receives the node
  * count and *out a result to copy out (v2m_seed_copy: P 3n floats, lab n,
  * typ n, part 2n, part3 n or NULL) and free (v2m_seed_free).

@@ -52,7 +52,7 @@ class RefLib:
         L.ref_grid_build_p.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp]
         L.ref_shape_grid.restype = vp
         L.ref_shape_grid.argtypes = [C.c_char_p, C.c_char_p, C.c_double, C.c_double, C.c_double, C.c_int, C.c_float,
-                                     C.c_float, C.c_float, C.c_float]
+                                     C.c_float, C.c_float, C.c_float, C.c_int]
         L.ref_grid_free.argtypes = [vp]
         L.ref_seed.restype = vp
         L.ref_seed.argtypes = [vp, vp, C.POINTER(C.c_int64)]
@@ -158,12 +158,14 @@ class RefLib:
         return self._grid_and_seeds(h, prm)
 
     def shape_and_seed(self, scene: str, voxel=1.0, gap=0.0, margin=3.0, bricks=True, sigma=1.0, hbase=0.0,
-                       hmin=0.0, hmax=0.0, prm: RelaxParams | None = None, overlap="overwrite"):
+                       hmin=0.0, hmax=0.0, prm: RelaxParams | None = None, overlap="overwrite", feat=False):
         """Shape input: the reference's shape compiler on a JSON scene, a grid
         over its raster with the compiled program as the fields (gm = -1), and
-        seed_cpu on it (ref_shape_grid)."""
+        seed_cpu on it (ref_shape_grid). feat: the grid build also takes the
+        scene's sharp features, as the shape front end hands them over (sizing
+        refined near them, tn::Grid::feat set), so seed_cpu pins nodes on them."""
         h = self.L.ref_shape_grid(scene.encode(), overlap.encode(), voxel, gap, margin, int(bricks), sigma, hbase,
-                                  hmin, hmax)
+                                  hmin, hmax, int(feat))
         if not h:
             raise RuntimeError(self.err())
         return self._grid_and_seeds(h, prm)

@@ -279,7 +279,7 @@ void* ref_grid_build(const uint16_t* labels, int nx, int ny, int nz, const float
 // the grid is built from it (sigma, hbase, hmin, hmax as in ref_grid_build) and
 // then takes the program as its fields: gm = -1, gTW = the program.
 void* ref_shape_grid(const char* json, const char* overlap, double voxel, double gap, double margin, int bricks,
-                     float sigma, float hbase, float hmin, float hmax) {
+                     float sigma, float hbase, float hmin, float hmax, int feat) {
     try {
         tn::ShapeScene sc = tn::load_shapes(std::string(json), true, std::string(overlap));
         const size_t N = static_cast<size_t>(sc.nlab);
@@ -313,6 +313,14 @@ void* ref_shape_grid(const char* json, const char* overlap, double voxel, double
         gp.hbase = hbase;
         gp.hmin = hmin;
         gp.hmax = hmax;
+        if (feat) {
+            // the shape front end's hand-off (src/v2m_modes.cpp:543-544): the grid
+            // build takes the program and the features from the volume, shifts
+            // the features into grid mm and refines the sizing near them
+            // (src/v2m_grid.cpp:350-371, 560-600); seed_cpu then pins nodes on them
+            r->lv.sdf = sc.prog;
+            r->lv.sdf_feat = sc.feat;
+        }
         tn::build_grid_cpu(r->lv, gp, r->g);
         r->g.gm = -1;
         r->g.gTW = sc.prog;
@@ -390,6 +398,8 @@ int ref_grid_view(void* h, v2m_grid_view* v) {
     v->gm = g.gm;
     v->ngTW = static_cast<int64_t>(g.gTW.size());
     v->grade = g.grade.empty() ? nullptr : g.grade.data();
+    v->feat = g.feat.empty() ? nullptr : g.feat.data();
+    v->nfeat = static_cast<int64_t>(g.feat.size());
     return 0;
 }
 

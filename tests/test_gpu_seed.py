@@ -55,3 +55,36 @@ def test_seeded_relax_matches_reference(ref, cuda_lib):
     for a in ("P", "typ", "part"):
         d = first_diff(getattr(nd, a), getattr(rnd, a))
         assert d is None, f"{a}: {d}"
+
+
+@pytest.mark.parametrize("name", ["mcx", "csg", "jmesh", "split"])
+def test_seed_shape_features_bit_exact(name, ref, cuda_lib):
+    """Shape input with its sharp features handed to the grid (as the shape
+    front end does): seed_cpu's feature pass -- CORNER nodes pinned on the
+    primitives' corners, edges and rims, the seeds near them dropped -- against
+    the device's."""
+    scene, kw = cases.SHAPE_SCENES[name]
+    prm = RelaxParams()
+    g, rnd = ref.shape_and_seed(scene, voxel=1.0, hbase=2.5, hmin=1.5, hmax=3.5, prm=prm, feat=True, **kw)
+    assert g.feat is not None and g.feat.size > 0
+    nd, part3 = seed_cl(g, prm)
+    check_seeds(rnd, nd, part3)
+    assert (nd.typ == V2M_CORNER).sum() > 0
+
+
+def test_shape_features_seeded_relax_matches_reference(ref, cuda_lib):
+    """Feature-pinned seeds made on the device, relaxed on the device: the
+    reference's seed_cpu + relax_cpu result (the CORNER nodes stay put)."""
+    from trussnet_b200 import relax_cl
+    scene, kw = cases.SHAPE_SCENES["csg"]
+    prm = RelaxParams(max_iters=15)
+    g, rnd = ref.shape_and_seed(scene, voxel=1.0, hbase=2.5, hmin=1.5, hmax=3.5, prm=prm, feat=True, **kw)
+    nd, _ = seed_cl(g, prm)
+    corner = nd.typ == V2M_CORNER
+    P0 = nd.P.copy()
+    ref.relax_cpu(g, prm, rnd)
+    relax_cl(g, prm, nd)
+    for a in ("P", "typ", "part"):
+        d = first_diff(getattr(nd, a), getattr(rnd, a))
+        assert d is None, f"{a}: {d}"
+    assert np.array_equal(nd.P[corner], P0[corner])

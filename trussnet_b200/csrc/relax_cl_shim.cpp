@@ -49,6 +49,8 @@ void relax_cl(const Grid& g, const RelaxParams& prm, Nodes& nd, RelaxStats& st, 
     gv.gTW = g.gTW.empty() ? nullptr : g.gTW.data();
     gv.gm = g.gm;
     gv.ngTW = static_cast<int64_t>(g.gTW.size());
+    gv.feat = g.feat.empty() ? nullptr : g.feat.data();
+    gv.nfeat = static_cast<int64_t>(g.feat.size());
 
     v2m_relax_params pv;
     v2m_relax_params_default(&pv);

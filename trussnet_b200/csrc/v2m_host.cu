@@ -1160,6 +1160,9 @@ void check_seed_args(const v2m_grid_view* g, const v2m_relax_params* prm) {
     if (prm->nseed < 1 || prm->nseed > 256) {
         throw ArgError("nseed must be in [1, 256]");
     }
+    if (g->nfeat < 0 || (g->nfeat > 0 && !g->feat)) {
+        throw ArgError("feat: nfeat floats needed");
+    }
     {
         // the counts and offsets are int32, as the reference's: bound the
         // lattice points of the finest level (spacing hmin) over all voxels,
@@ -1194,6 +1197,8 @@ void seed_on(v2m_session& tmp, const v2m_grid_view* g, const v2m_relax_params* p
     A.jseed = prm->jseed;
     A.corners = prm->corners ? 1 : 0;
     A.hmax = g->hmax;
+    A.feat = g->feat;
+    A.nfeat = g->feat ? g->nfeat : 0;
     cudaDeviceGetAttribute(&A.sms, cudaDevAttrMultiProcessorCount, dev);
     A.stream = tmp.stream;
     std::string err;

@@ -124,6 +124,8 @@ struct SeedArgs {
     float jseed = 0.0f;
     int corners = 1;
     float hmax = 0.0f;
+    const float* feat = nullptr;      // shape input's sharp features (host memory, tn::Grid::feat), or none
+    int64_t nfeat = 0;
     int sms = 148;
     cudaStream_t stream = nullptr;
 };

@@ -14,6 +14,12 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <utility>
+#include <vector>
+
 #include "v2m_field.cuh"
 #include "v2m_kernels.h"
 
@@ -559,6 +565,230 @@ __global__ void k_seed_jcompact(int n, const int* __restrict__ keep, const float
     }
 }
 
+// ---- 5. shape features (tn::seed_cpu's add_feature_nodes, src/v2m_particles.cpp:298-623) ----
+// The curves' geometry (sample points, bisection midpoints, arc length and the
+// resampled points) is computed on the host, in the reference's float and double
+// arithmetic and with the host's cos / sin for circles; every point query (the
+// labels round a point, h at a point) runs here on the device, through the
+// relaxation's own field code.
+
+// the labels round each point x: x and six axis samples at 0.2 h (mask_at)
+template <bool kShape>
+__global__ void __launch_bounds__(kSeedThreads) k_feat_mask(DGrid g, int n, const float* __restrict__ X,
+                                                           unsigned long long* __restrict__ mask) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const float x[3] = { X[3 * (size_t)t], X[3 * (size_t)t + 1], X[3 * (size_t)t + 2] };
+        const float e = 0.2f * size_at(g, 0, x[0], x[1], x[2]);
+        const float dir[7][3] = { { 0, 0, 0 }, { 1, 0, 0 }, { -1, 0, 0 }, { 0, 1, 0 }, { 0, -1, 0 }, { 0, 0, 1 }, { 0, 0, -1 } };
+        unsigned long long m = 0ull;
+#pragma unroll 1
+        for (int d = 0; d < 7; ++d) {
+            int sec;
+            float mg;
+            const int l = owner_label<kShape>(g, 0, x[0] + e * dir[d][0], x[1] + e * dir[d][1], x[2] + e * dir[d][2],
+                                              &sec, &mg);
+            m |= l < 64 ? 1ull << l : 0ull;
+        }
+        mask[t] = m;
+    }
+}
+
+// h at each point (v2m_h_at: the nearest voxel's)
+__global__ void k_feat_hat(DGrid g, int n, const float* __restrict__ X, float* __restrict__ out) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        out[t] = size_at(g, 0, X[3 * (size_t)t], X[3 * (size_t)t + 1], X[3 * (size_t)t + 2]);
+    }
+}
+
+constexpr int kFeatWarps = 4;
+constexpr int kFeatMaxDirs = 160;
+
+// Each candidate's labels round it: the labels at 0.25 h along the ndir
+// directions, counted; up to four of them in the order (tissue labels first,
+// then by count, descending, then by label), with their number (0 when the
+// point lies outside the grid or inside one region). One warp per candidate:
+// the lanes sample the directions, lane 0 ranks the labels.
+template <bool kShape>
+__global__ void __launch_bounds__(32 * kFeatWarps) k_feat_classify(DGrid g, int n, const float* __restrict__ X,
+                                                                  const float* __restrict__ dirs, int ndir,
+                                                                  int4* __restrict__ ls, int* __restrict__ nls,
+                                                                  float* __restrict__ hx) {
+    __shared__ int lb[kFeatWarps][kFeatMaxDirs];
+    __shared__ int dl[kFeatWarps][kFeatMaxDirs], dc[kFeatWarps][kFeatMaxDirs];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int nw = gridDim.x * kFeatWarps;
+    for (int c = blockIdx.x * kFeatWarps + w; c < n; c += nw) {
+        const float x[3] = { X[3 * (size_t)c], X[3 * (size_t)c + 1], X[3 * (size_t)c + 2] };
+        const float h = size_at(g, 0, x[0], x[1], x[2]);
+        const bool out = x[0] < 0 || x[1] < 0 || x[2] < 0 || x[0] > (g.nx - 1) * g.vx || x[1] > (g.ny - 1) * g.vy ||
+                         x[2] > (g.nz - 1) * g.vz;
+        if (lane == 0) {
+            hx[c] = h;
+        }
+        if (out) {
+            if (lane == 0) {
+                nls[c] = 0;
+                ls[c] = make_int4(V2M_NOLAB, V2M_NOLAB, V2M_NOLAB, V2M_NOLAB);
+            }
+            continue;
+        }
+        const float e = 0.25f * h;
+        for (int d = lane; d < ndir; d += 32) {
+            int sec;
+            float mg;
+            lb[w][d] = owner_label<kShape>(g, 0, x[0] + e * dirs[3 * d], x[1] + e * dirs[3 * d + 1],
+                                           x[2] + e * dirs[3 * d + 2], &sec, &mg);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            int nd = 0;   // distinct labels and their counts
+            for (int d = 0; d < ndir; ++d) {
+                const int l = lb[w][d];
+                int q = 0;
+                while (q < nd && dl[w][q] != l) {
+                    ++q;
+                }
+                if (q == nd) {
+                    dl[w][nd] = l;
+                    dc[w][nd] = 0;
+                    ++nd;
+                }
+                ++dc[w][q];
+            }
+            int L[4] = { V2M_NOLAB, V2M_NOLAB, V2M_NOLAB, V2M_NOLAB };
+            int m = 0;
+            if (nd >= 2) {
+                // the first four in (label 0 last, count descending, label ascending) order
+                for (; m < 4 && m < nd; ++m) {
+                    int best = -1;
+                    for (int q = 0; q < nd; ++q) {
+                        if (dc[w][q] < 0) {
+                            continue;
+                        }
+                        if (best < 0) {
+                            best = q;
+                            continue;
+                        }
+                        const int lq = dl[w][q], lb_ = dl[w][best];
+                        const bool zq = lq == 0, zb = lb_ == 0;
+                        const bool before = zq != zb ? !zq
+                                                     : (dc[w][q] != dc[w][best] ? dc[w][q] > dc[w][best] : lq < lb_);
+                        if (before) {
+                            best = q;
+                        }
+                    }
+                    L[m] = dl[w][best];
+                    dc[w][best] = -1;
+                }
+                if (m > 0 && L[0] == 0) {
+                    m = 0;   // (no tissue round it)
+                }
+            }
+            ls[c] = make_int4(L[0], L[1], L[2], L[3]);
+            nls[c] = m;
+        }
+        __syncwarp();
+    }
+}
+
+// the seeds within 0.4 h of a kept feature node are dropped, found through the
+// reference's uniform cells of side `cell` (keys: the sorted packed cells of
+// the feature nodes); keep[i + 1] = kept
+constexpr long long kFeatCellOff = 1ll << 20;
+
+__device__ __host__ __forceinline__ bool feat_cell_key(long long i, long long j, long long k, unsigned long long* key) {
+    i += kFeatCellOff;
+    j += kFeatCellOff;
+    k += kFeatCellOff;
+    if (i < 0 || j < 0 || k < 0 || i >= 2 * kFeatCellOff || j >= 2 * kFeatCellOff || k >= 2 * kFeatCellOff) {
+        return false;
+    }
+    *key = ((unsigned long long)i << 42) | ((unsigned long long)j << 21) | (unsigned long long)k;
+    return true;
+}
+
+__global__ void __launch_bounds__(kSeedThreads) k_feat_drop(DGrid g, int n, const float* __restrict__ P, float cell,
+                                                          int nk, const unsigned long long* __restrict__ keys,
+                                                          const int* __restrict__ kidx, const float* __restrict__ kp,
+                                                          int* __restrict__ keep) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float x[3] = { P[3 * (size_t)i], P[3 * (size_t)i + 1], P[3 * (size_t)i + 2] };
+        const float r = 0.4f * size_at(g, 0, x[0], x[1], x[2]);
+        const long long ci = (long long)floorf(x[0] / cell), cj = (long long)floorf(x[1] / cell),
+                        ck = (long long)floorf(x[2] / cell);
+        const long long reach = (long long)ceilf(r / cell);
+        int drop = 0;
+        for (long long a = -reach; a <= reach && !drop; ++a) {
+            for (long long b = -reach; b <= reach && !drop; ++b) {
+                for (long long c = -reach; c <= reach && !drop; ++c) {
+                    unsigned long long kk;
+                    if (!feat_cell_key(ci + a, cj + b, ck + c, &kk)) {
+                        continue;
+                    }
+                    int lo = 0, hi = nk;   // first entry with key >= kk
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (keys[mid] < kk) {
+                            lo = mid + 1;
+                        } else {
+                            hi = mid;
+                        }
+                    }
+                    for (int e = lo; e < nk && keys[e] == kk; ++e) {
+                        const int k = kidx[e];
+                        const float dx = kp[3 * (size_t)k] - x[0], dy = kp[3 * (size_t)k + 1] - x[1],
+                                    dz = kp[3 * (size_t)k + 2] - x[2];
+                        if (dx * dx + dy * dy + dz * dz < r * r) {
+                            drop = 1;
+                            break;
+                        }
+                    }
+                }
+            }
+        }
+        keep[i + 1] = !drop;
+    }
+}
+
+// the kept seeds compacted in order, then the feature nodes appended (CORNER
+// nodes: own label the first of their labels, partners the next three)
+__global__ void k_feat_compact(int n, const int* __restrict__ keep, const float* __restrict__ P,
+                               const uint16_t* __restrict__ lab, const uint8_t* __restrict__ typ,
+                               const uint16_t* __restrict__ part, const uint16_t* __restrict__ part3, int nk,
+                               const float* __restrict__ kp, const int4* __restrict__ kl, const int* __restrict__ kn,
+                               float* __restrict__ P2, uint16_t* __restrict__ lab2, uint8_t* __restrict__ typ2,
+                               uint16_t* __restrict__ part2, uint16_t* __restrict__ part32) {
+    const int nkeep = keep[n];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + nk; i += gridDim.x * blockDim.x) {
+        if (i < n) {
+            if (keep[i + 1] == keep[i]) {
+                continue;
+            }
+            const int o = keep[i];
+            P2[3 * (size_t)o] = P[3 * (size_t)i];
+            P2[3 * (size_t)o + 1] = P[3 * (size_t)i + 1];
+            P2[3 * (size_t)o + 2] = P[3 * (size_t)i + 2];
+            lab2[o] = lab[i];
+            typ2[o] = typ[i];
+            part2[2 * (size_t)o] = part[2 * (size_t)i];
+            part2[2 * (size_t)o + 1] = part[2 * (size_t)i + 1];
+            part32[o] = part3[i];
+        } else {
+            const int k = i - n, o = nkeep + k;
+            const int4 L = kl[k];
+            const int m = kn[k];
+            P2[3 * (size_t)o] = kp[3 * (size_t)k];
+            P2[3 * (size_t)o + 1] = kp[3 * (size_t)k + 1];
+            P2[3 * (size_t)o + 2] = kp[3 * (size_t)k + 2];
+            lab2[o] = (uint16_t)L.x;
+            typ2[o] = V2M_CORNER;
+            part2[2 * (size_t)o] = (uint16_t)(m > 1 ? L.y : V2M_NOLAB);
+            part2[2 * (size_t)o + 1] = (uint16_t)(m > 2 ? L.z : V2M_NOLAB);
+            part32[o] = (uint16_t)(m > 3 ? L.w : V2M_NOLAB);
+        }
+    }
+}
+
 __global__ void k_iota(int n, int* __restrict__ out) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         out[i] = i;
@@ -613,6 +843,368 @@ cudaError_t scan_counts(Scratch& sc, int* cnt, int64_t n) {
 }
 
 }  // namespace
+
+// ---- 5. shape features: the host's part -------------------------------------------------
+// One feature curve of tn::Grid::feat: 2 a segment (a, b), 3 a circle (centre,
+// normal, radius), 4 a polyline (n, then n points). at() is the reference's
+// curve point at parameter t in [0, 1] (src/v2m_particles.cpp:347-369), the
+// circle's frame its orthonormal pair about the normal (:330-345): the same
+// float expressions, in the same order (this file is compiled without
+// contraction), with the host's cos / sin.
+struct FeatCurve {
+    int type = 0;
+    const float* q = nullptr;
+    float u[3] = { 0, 0, 0 }, w[3] = { 0, 0, 0 };
+
+    FeatCurve(int ty, const float* qq) : type(ty), q(qq) {
+        if (type == 3) {
+            const float* n = q + 3;
+            const float a0 = std::fabs(n[0]) < 0.9f ? 1.0f : 0.0f, a1 = a0 > 0 ? 0.0f : 1.0f;
+            u[0] = n[1] * 0 - n[2] * a1;
+            u[1] = n[2] * a0 - n[0] * 0;
+            u[2] = n[0] * a1 - n[1] * a0;
+            const float lu = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+            for (float& x : u) {
+                x /= lu;
+            }
+            w[0] = n[1] * u[2] - n[2] * u[1];
+            w[1] = n[2] * u[0] - n[0] * u[2];
+            w[2] = n[0] * u[1] - n[1] * u[0];
+        }
+    }
+
+    void at(float t, float* o) const {
+        if (type == 4) {
+            const int n = static_cast<int>(q[0]);
+            const float uu = t * static_cast<float>(n - 1);
+            const int i = std::min(n - 2, std::max(0, static_cast<int>(uu)));
+            const float f = uu - static_cast<float>(i);
+            for (int a = 0; a < 3; ++a) {
+                o[a] = q[1 + 3 * i + a] + f * (q[1 + 3 * (i + 1) + a] - q[1 + 3 * i + a]);
+            }
+        } else if (type == 2) {
+            for (int a = 0; a < 3; ++a) {
+                o[a] = q[a] + t * (q[3 + a] - q[a]);
+            }
+        } else {
+            const float th = 6.28318531f * t, c = std::cos(th), sn = std::sin(th);
+            for (int a = 0; a < 3; ++a) {
+                o[a] = q[a] + q[6] * (c * u[a] + sn * w[a]);
+            }
+        }
+    }
+};
+
+// The feature pass over the seeds in B (src/v2m_particles.cpp:304-623): the
+// candidates (corners; then where the labels round a curve change, bisected;
+// then points spaced by h along each curve), each given the labels round it;
+// one kept per 0.3 h in that order (two or more labels); the seeds within 0.4 h
+// of a kept one dropped; the kept ones appended as CORNER nodes.
+template <bool kShape, class Alloc>
+cudaError_t feature_pass(const SeedArgs& A, SeedBuffers& B, Scratch& sc, Alloc& alloc, std::string& err) {
+    const DGrid& g = A.g;
+    cudaStream_t s = A.stream;
+    constexpr int nsamp = 256;
+    cudaError_t e;
+    // the point queries: masks or sizes of host points, through device buffers
+    float* dX = nullptr;
+    size_t capX = 0;
+    auto points = [&](const std::vector<float>& X) -> cudaError_t {
+        const size_t n = X.size() / 3;
+        if (n > capX) {
+            capX = std::max<size_t>(n, 1024);
+            dX = (float*)alloc(sizeof(float) * 3 * capX);
+            if (!dX) {
+                return cudaErrorMemoryAllocation;
+            }
+        }
+        return cudaMemcpyAsync(dX, X.data(), sizeof(float) * X.size(), cudaMemcpyHostToDevice, s);
+    };
+    unsigned long long* dM = nullptr;
+    size_t capM = 0;
+    auto masks = [&](const std::vector<float>& X, std::vector<unsigned long long>& out) -> cudaError_t {
+        const int n = (int)(X.size() / 3);
+        out.assign((size_t)n, 0ull);
+        if (n == 0) {
+            return cudaSuccess;
+        }
+        cudaError_t r = points(X);
+        if (r != cudaSuccess) {
+            return r;
+        }
+        if ((size_t)n > capM) {
+            capM = std::max<size_t>(n, 1024);
+            dM = (unsigned long long*)alloc(8 * capM);
+            if (!dM) {
+                return cudaErrorMemoryAllocation;
+            }
+        }
+        k_feat_mask<kShape><<<gs_blocks(n, A.sms), kSeedThreads, 0, s>>>(g, n, dX, dM);
+        if ((r = cudaMemcpyAsync(out.data(), dM, 8 * (size_t)n, cudaMemcpyDeviceToHost, s)) != cudaSuccess) {
+            return r;
+        }
+        return cudaStreamSynchronize(s);
+    };
+    auto sizes = [&](const std::vector<float>& X, std::vector<float>& out) -> cudaError_t {
+        const int n = (int)(X.size() / 3);
+        out.assign((size_t)n, 0.0f);
+        if (n == 0) {
+            return cudaSuccess;
+        }
+        cudaError_t r = points(X);
+        if (r != cudaSuccess) {
+            return r;
+        }
+        float* dH = (float*)alloc(sizeof(float) * (size_t)n);
+        if (!dH) {
+            return cudaErrorMemoryAllocation;
+        }
+        k_feat_hat<<<gs_blocks(n, A.sms), kSeedThreads, 0, s>>>(g, n, dX, dH);
+        if ((r = cudaMemcpyAsync(out.data(), dH, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, s)) != cudaSuccess) {
+            return r;
+        }
+        return cudaStreamSynchronize(s);
+    };
+    // the features: corners, then the curves (a polyline needs two points)
+    std::vector<float> fp;
+    std::vector<FeatCurve> curves;
+    for (int64_t k = 0; k < A.nfeat;) {
+        const int type = static_cast<int>(A.feat[k]);
+        const int64_t len = type == 1 ? 4 : type == 2 ? 7 : type == 3 ? 8
+                          : type == 4 && k + 1 < A.nfeat ? 2 + 3 * static_cast<int64_t>(A.feat[k + 1]) : -1;
+        if (len < 0 || k + len > A.nfeat || (type == 4 && A.feat[k + 1] < 0)) {
+            err = "the feature list is malformed at float " + std::to_string(k);
+            return cudaErrorInvalidValue;
+        }
+        const float* q = A.feat + k + 1;
+        if (type == 1) {
+            fp.insert(fp.end(), { q[0], q[1], q[2] });
+        } else if (type != 4 || q[0] >= 2) {
+            curves.emplace_back(type, q);
+        }
+        k += len;
+    }
+    const size_t ncv = curves.size();
+    // the curves' samples and the labels round them
+    std::vector<float> pts(ncv * 3 * (nsamp + 1));
+    for (size_t c = 0; c < ncv; ++c) {
+        for (int k = 0; k <= nsamp; ++k) {
+            curves[c].at(static_cast<float>(k) / nsamp, &pts[3 * (c * (nsamp + 1) + k)]);
+        }
+    }
+    std::vector<unsigned long long> mk;
+    if ((e = masks(pts, mk)) != cudaSuccess) {
+        return e;
+    }
+    // where the labels change: 14 bisection steps, every change at once
+    struct Job {
+        size_t c;
+        float lo, hi;
+        unsigned long long m0;
+    };
+    std::vector<Job> jobs;
+    for (size_t c = 0; c < ncv; ++c) {
+        const unsigned long long* m = &mk[c * (nsamp + 1)];
+        for (int k = 1; k <= nsamp; ++k) {
+            if (m[k] != m[k - 1]) {
+                jobs.push_back({ c, static_cast<float>(k - 1) / nsamp, static_cast<float>(k) / nsamp, m[k - 1] });
+            }
+        }
+    }
+    if (!jobs.empty()) {
+        std::vector<float> X(3 * jobs.size());
+        std::vector<unsigned long long> mm;
+        for (int it = 0; it < 14; ++it) {
+            for (size_t j = 0; j < jobs.size(); ++j) {
+                curves[jobs[j].c].at(0.5f * (jobs[j].lo + jobs[j].hi), &X[3 * j]);
+            }
+            if ((e = masks(X, mm)) != cudaSuccess) {
+                return e;
+            }
+            for (size_t j = 0; j < jobs.size(); ++j) {
+                const float mid = 0.5f * (jobs[j].lo + jobs[j].hi);
+                if (mm[j] == jobs[j].m0) {
+                    jobs[j].lo = mid;
+                } else {
+                    jobs[j].hi = mid;
+                }
+            }
+        }
+        for (size_t j = 0; j < jobs.size(); ++j) {
+            float x[3];
+            curves[jobs[j].c].at(0.5f * (jobs[j].lo + jobs[j].hi), x);
+            fp.insert(fp.end(), x, x + 3);
+        }
+    }
+    // arc length in units of h, then the regular points
+    std::vector<float> mids(ncv * 3 * nsamp);
+    for (size_t c = 0; c < ncv; ++c) {
+        for (int k = 1; k <= nsamp; ++k) {
+            const float* a = &pts[3 * (c * (nsamp + 1) + k - 1)];
+            const float* b = &pts[3 * (c * (nsamp + 1) + k)];
+            float* m = &mids[3 * (c * nsamp + k - 1)];
+            m[0] = 0.5f * (a[0] + b[0]);
+            m[1] = 0.5f * (a[1] + b[1]);
+            m[2] = 0.5f * (a[2] + b[2]);
+        }
+    }
+    std::vector<float> hm;
+    if ((e = sizes(mids, hm)) != cudaSuccess) {
+        return e;
+    }
+    for (size_t c = 0; c < ncv; ++c) {
+        const int type = curves[c].type;
+        const float* P = &pts[3 * c * (nsamp + 1)];
+        std::vector<double> acc(nsamp + 1, 0.0);
+        for (int k = 1; k <= nsamp; ++k) {
+            const float* a = &P[3 * (k - 1)];
+            const float* b = &P[3 * k];
+            const float ds = std::sqrt((b[0] - a[0]) * (b[0] - a[0]) + (b[1] - a[1]) * (b[1] - a[1]) +
+                                       (b[2] - a[2]) * (b[2] - a[2]));
+            acc[k] = acc[k - 1] + ds / std::max(hm[c * nsamp + k - 1], 1e-6f);
+        }
+        const double per = type == 4 ? 2.0 : 1.0;
+        const int ns = std::max(type == 3 ? 6 : 1, static_cast<int>(std::lround(per * acc[nsamp])));
+        for (int q = type == 3 || type == 4 ? 0 : 1; q < ns; ++q) {
+            const double target = acc[nsamp] * q / ns;
+            int k = 1;
+            while (k < nsamp && acc[k] < target) {
+                ++k;
+            }
+            const double f = acc[k] > acc[k - 1] ? (target - acc[k - 1]) / (acc[k] - acc[k - 1]) : 0.0;
+            for (int a = 0; a < 3; ++a) {
+                fp.push_back(static_cast<float>(P[3 * (k - 1) + a] + f * (P[3 * k + a] - P[3 * (k - 1) + a])));
+            }
+        }
+    }
+    const int nc = (int)(fp.size() / 3);
+    if (nc == 0) {
+        return cudaSuccess;
+    }
+    // the directions round a candidate: 14 axis / diagonal, 128 on a golden spiral
+    std::vector<float> dirs = { 1, 0, 0, -1, 0, 0, 0, 1, 0, 0, -1, 0, 0, 0, 1, 0, 0, -1,
+                                .577f, .577f, .577f, -.577f, .577f, .577f, .577f, -.577f, .577f, .577f, .577f, -.577f,
+                                -.577f, -.577f, .577f, -.577f, .577f, -.577f, .577f, -.577f, -.577f, -.577f, -.577f, -.577f };
+    for (int i = 0; i < 128; ++i) {
+        const double zc = 1 - (2 * i + 1) / 128.0, rr = std::sqrt(std::max(0.0, 1 - zc * zc)), ph = 2.39996322972865 * i;
+        dirs.push_back(static_cast<float>(rr * std::cos(ph)));
+        dirs.push_back(static_cast<float>(rr * std::sin(ph)));
+        dirs.push_back(static_cast<float>(zc));
+    }
+    const int ndir = (int)(dirs.size() / 3);
+    float* dD = (float*)alloc(sizeof(float) * dirs.size());
+    float* dF = (float*)alloc(sizeof(float) * fp.size());
+    int4* dL = (int4*)alloc(sizeof(int4) * (size_t)nc);
+    int* dN = (int*)alloc(sizeof(int) * (size_t)nc);
+    float* dHx = (float*)alloc(sizeof(float) * (size_t)nc);
+    if (!dD || !dF || !dL || !dN || !dHx) {
+        return cudaErrorMemoryAllocation;
+    }
+    cudaMemcpyAsync(dD, dirs.data(), sizeof(float) * dirs.size(), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dF, fp.data(), sizeof(float) * fp.size(), cudaMemcpyHostToDevice, s);
+    k_feat_classify<kShape><<<(unsigned)std::min<int64_t>((nc + kFeatWarps - 1) / kFeatWarps, (int64_t)A.sms * 16),
+                              32 * kFeatWarps, 0, s>>>(g, nc, dF, dD, ndir, dL, dN, dHx);
+    std::vector<int4> ls((size_t)nc);
+    std::vector<int> nls((size_t)nc);
+    std::vector<float> hx((size_t)nc);
+    cudaMemcpyAsync(ls.data(), dL, sizeof(int4) * (size_t)nc, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(nls.data(), dN, sizeof(int) * (size_t)nc, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(hx.data(), dHx, sizeof(float) * (size_t)nc, cudaMemcpyDeviceToHost, s);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) {
+        return e;
+    }
+    // one kept per 0.3 h, in candidate order (corners first)
+    std::vector<float> keepP;
+    std::vector<int4> keepL;
+    std::vector<int> keepN;
+    for (int c = 0; c < nc; ++c) {
+        if (nls[c] < 2) {
+            continue;
+        }
+        const float* x = &fp[3 * (size_t)c];
+        const float r = 0.3f * hx[c];
+        bool near = false;
+        for (size_t k = 0; k < keepP.size() / 3 && !near; ++k) {
+            const float dx = keepP[3 * k] - x[0], dy = keepP[3 * k + 1] - x[1], dz = keepP[3 * k + 2] - x[2];
+            near = dx * dx + dy * dy + dz * dz < r * r;
+        }
+        if (!near) {
+            keepP.insert(keepP.end(), x, x + 3);
+            keepL.push_back(ls[c]);
+            keepN.push_back(nls[c]);
+        }
+    }
+    const int nk = (int)keepN.size();
+    if (nk == 0) {
+        return cudaSuccess;
+    }
+    // the kept nodes' cells (the reference's hash cells: side 0.4 hmax), sorted
+    const float cell = 0.4f * A.hmax > 0 ? 0.4f * A.hmax : 1.0f;
+    std::vector<std::pair<unsigned long long, int>> kc((size_t)nk);
+    for (int k = 0; k < nk; ++k) {
+        unsigned long long key = 0;
+        if (!feat_cell_key(static_cast<long long>(std::floor(keepP[3 * (size_t)k] / cell)),
+                           static_cast<long long>(std::floor(keepP[3 * (size_t)k + 1] / cell)),
+                           static_cast<long long>(std::floor(keepP[3 * (size_t)k + 2] / cell)), &key)) {
+            err = "a feature node lies beyond the drop hash's range";
+            return cudaErrorInvalidValue;
+        }
+        kc[(size_t)k] = { key, k };
+    }
+    std::stable_sort(kc.begin(), kc.end(), [](const std::pair<unsigned long long, int>& a,
+                                              const std::pair<unsigned long long, int>& b) { return a.first < b.first; });
+    std::vector<unsigned long long> keys((size_t)nk);
+    std::vector<int> kidx((size_t)nk);
+    for (int k = 0; k < nk; ++k) {
+        keys[(size_t)k] = kc[(size_t)k].first;
+        kidx[(size_t)k] = kc[(size_t)k].second;
+    }
+    auto* dK = (unsigned long long*)alloc(8 * (size_t)nk);
+    int* dKi = (int*)alloc(sizeof(int) * (size_t)nk);
+    float* dKp = (float*)alloc(sizeof(float) * 3 * (size_t)nk);
+    int4* dKl = (int4*)alloc(sizeof(int4) * (size_t)nk);
+    int* dKn = (int*)alloc(sizeof(int) * (size_t)nk);
+    const int n0 = B.n;
+    int* keep = (int*)alloc(sizeof(int) * (size_t)(n0 + 1));
+    if (!dK || !dKi || !dKp || !dKl || !dKn || !keep) {
+        return cudaErrorMemoryAllocation;
+    }
+    cudaMemcpyAsync(dK, keys.data(), 8 * (size_t)nk, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dKi, kidx.data(), sizeof(int) * (size_t)nk, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dKp, keepP.data(), sizeof(float) * 3 * (size_t)nk, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dKl, keepL.data(), sizeof(int4) * (size_t)nk, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dKn, keepN.data(), sizeof(int) * (size_t)nk, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(keep, 0, sizeof(int), s);
+    if (n0 > 0) {
+        k_feat_drop<<<gs_blocks(n0, A.sms), kSeedThreads, 0, s>>>(g, n0, B.P, cell, nk, dK, dKi, dKp, keep);
+        if ((e = scan_counts(sc, keep, n0)) != cudaSuccess) {
+            return e;
+        }
+    }
+    int nkeep = 0;
+    cudaMemcpyAsync(&nkeep, keep + n0, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) {
+        return e;
+    }
+    const int n2 = nkeep + nk;
+    float* P2 = (float*)alloc(sizeof(float) * 3 * (size_t)n2);
+    uint16_t* lab2 = (uint16_t*)alloc(sizeof(uint16_t) * (size_t)n2);
+    uint8_t* typ2 = (uint8_t*)alloc((size_t)n2);
+    uint16_t* part2 = (uint16_t*)alloc(sizeof(uint16_t) * 2 * (size_t)n2);
+    uint16_t* part32 = (uint16_t*)alloc(sizeof(uint16_t) * (size_t)n2);
+    if (!P2 || !lab2 || !typ2 || !part2 || !part32) {
+        return cudaErrorMemoryAllocation;
+    }
+    k_feat_compact<<<gs_blocks(n0 + nk, A.sms), kSeedThreads, 0, s>>>(n0, keep, B.P, B.lab, B.typ, B.part, B.part3, nk,
+                                                                     dKp, dKl, dKn, P2, lab2, typ2, part2, part32);
+    B.P = P2;
+    B.lab = lab2;
+    B.typ = typ2;
+    B.part = part2;
+    B.part3 = part32;
+    B.n = n2;
+    return cudaGetLastError();
+}
 
 // ---- host side: the stages in order ----------------------------------------------------
 template <bool kShape>
@@ -840,6 +1432,12 @@ cudaError_t seed_stages(const SeedArgs& A, SeedBuffers& B, std::string& err) {
     B.n = nt;
     if ((e = cudaGetLastError()) != cudaSuccess) {
         return e;
+    }
+    // 5. shape input: nodes pinned on the sharp features
+    if (A.feat && A.nfeat > 0) {
+        if ((e = feature_pass<kShape>(A, B, sc, alloc, err)) != cudaSuccess) {
+            return e;
+        }
     }
     return cudaStreamSynchronize(s);
 }

@@ -34,7 +34,7 @@ class GridView(C.Structure):
                 ("phi", C.c_void_p), ("nslots", C.c_int64), ("h", C.c_void_p),
                 ("hmin", C.c_float), ("hmax", C.c_float),
                 ("gI", C.c_void_p), ("gTW", C.c_void_p), ("gm", C.c_int32), ("ngTW", C.c_int64),
-                ("grade", C.c_void_p)]
+                ("grade", C.c_void_p), ("feat", C.c_void_p), ("nfeat", C.c_int64)]
 
 
 class RelaxParamsC(C.Structure):
@@ -160,6 +160,7 @@ class Grid:
     gm: int = 0                     # gray thresholds; 0: label volume; < 0: analytic shape fields
     R: int = 6
     grade: np.ndarray | None = None  # uint8 [nz, ny, nx] size grades (seeding only)
+    feat: np.ndarray | None = None   # float32: shape input's sharp features (tn::Grid::feat; seeding only)
 
     @property
     def nbx(self):
@@ -200,6 +201,10 @@ class Grid:
             assert self.grade.dtype == np.uint8 and self.grade.flags.c_contiguous
             assert self.grade.size == self.nx * self.ny * self.nz
         v.grade = self.grade.ctypes.data if self.grade is not None else None
+        if self.feat is not None and self.feat.size:
+            assert self.feat.dtype == np.float32 and self.feat.flags.c_contiguous
+            v.feat = self.feat.ctypes.data
+            v.nfeat = int(self.feat.size)
         return v
 
     @classmethod
@@ -231,6 +236,8 @@ class Grid:
             g.gTW = arr(v.gTW, np.float32, v.ngTW)
         if v.grade:
             g.grade = arr(v.grade, np.uint8, nv).reshape(v.nz, v.ny, v.nx)
+        if v.feat and v.nfeat > 0:
+            g.feat = arr(v.feat, np.float32, v.nfeat)
         return g
 
     def nbytes(self) -> int:
