@@ -679,7 +679,8 @@ __global__ void __launch_bounds__(kNbrMaxThreads, 4) k_neighbors(const DVol* __r
 }
 
 // The self-refresh of the nodes past a full skin (list filled by k_move), one
-// warp per entry; the last block to finish empties the list.
+// warp per entry, except in a volume that rebuilds this iteration; the last
+// block to finish empties the list.
 __global__ void __launch_bounds__(kNbrMaxThreads, 4) k_refresh(const DVol* __restrict__ vols, const VolCtl* __restrict__ ctl,
                                                          const uint16_t* __restrict__ nodevol, const float4* __restrict__ Pq,
                                                          const uint8_t* __restrict__ typ, const uint16_t* __restrict__ lab,
@@ -695,7 +696,10 @@ __global__ void __launch_bounds__(kNbrMaxThreads, 4) k_refresh(const DVol* __res
     for (int e = blockIdx.x * wpb + w; e < cnt; e += nw) {
         const int64_t i = rlist[e];
         const int v = nodevol[i];
-        if (ctl[v].done) {
+        // a volume that rebuilds this iteration rebuilds every list and sets every
+        // build position next (src/v2m_particles.cpp:771-820): its refreshes would
+        // be overwritten unread
+        if (ctl[v].done || ctl[v].rebuild) {
             continue;
         }
         warp_neighbors<false>(vols[v], i, lane, sm[w], Pq, typ, lab, cstart, sorted, Ps, nullptr, nbr, nnb, N);
