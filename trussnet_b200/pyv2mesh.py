@@ -7,7 +7,9 @@ the seeding and the relaxation all run on the device in one call
 (points_cl: one upload of the labels, one copy back of the nodes), bit for bit
 the reference's CPU stages. `optimize_sizing` is the sizing-by-gradient step
 the reference does not have: descent on a sizing grid through the
-differentiable relaxation unroll (trussnet_b200.adjoint).
+differentiable relaxation unroll (trussnet_b200.adjoint). `dump_nodes` /
+`load_nodes` write and read the relaxed nodes in the reference's node-dump
+format (its --dump-nodes), the on-disk hand-off to its tessellation tools.
 """
 from __future__ import annotations
 
@@ -106,3 +108,49 @@ def optimize_sizing(nbr, nnb, typ, x0, G0, cs, *, K=50, ckpt=10, steps=20, step=
         return Gout.cpu().numpy(), losses
     finally:
         u.close()
+
+
+# ---- the node dump: the relaxation's on-disk hand-off --------------------------------
+_DUMP_FIELDS = (("P", "float32", 3), ("Label", "uint16", 1), ("Type", "uint8", 1), ("Partner", "uint16", 2))
+
+
+def dump_nodes(path, nodes) -> None:
+    """Write nodes as v2mesh's node dump (``--dump-nodes``,
+    src/v2m_pipeline.cpp:58-73 of fangq/trussnet; read by its
+    tools/v2mview.py): one JSON header line {name: [dtype, shape, byte
+    offset]} -- compact, keys in sorted order as the reference's JSON library
+    writes them -- then the raw little-endian arrays in the order P float32
+    [n, 3], Label uint16 [n], Type uint8 [n], Partner uint16 [n, 2], the
+    offsets counted from the end of the header line. (The reference's dump has
+    no part3: a CORNER node's fourth label stays in memory.)"""
+    import json
+    n = int(nodes.size())
+    arrays = (np.ascontiguousarray(nodes.P, np.float32).reshape(n, 3), np.ascontiguousarray(nodes.lab, np.uint16),
+              np.ascontiguousarray(nodes.typ, np.uint8), np.ascontiguousarray(nodes.part, np.uint16).reshape(n, 2))
+    head, off = {}, 0
+    for (name, dt, w), a in zip(_DUMP_FIELDS, arrays):
+        head[name] = [dt, [n, w] if w > 1 else [n], off]
+        off += a.nbytes
+    with open(path, "wb") as f:
+        f.write(json.dumps(head, separators=(",", ":"), sort_keys=True).encode())
+        f.write(b"\n")
+        for a in arrays:
+            f.write(a.astype(a.dtype.newbyteorder("<"), copy=False).tobytes())
+
+
+def load_nodes(path):
+    """Nodes from a v2mesh node dump (the reference's or dump_nodes'): P, lab,
+    typ, part as tn::Nodes holds them."""
+    import json
+    from .types import Nodes
+    with open(path, "rb") as f:
+        head = json.loads(f.readline())
+        buf = f.read()
+    out = {}
+    for name, dt, w in _DUMP_FIELDS:
+        dtype, shape, off = head[name]
+        cnt = int(np.prod(shape))
+        out[name] = np.frombuffer(buf, dtype=np.dtype(dtype).newbyteorder("<"), count=cnt, offset=int(off)).reshape(shape)
+    n = int(head["Label"][1][0])
+    return Nodes(P=out["P"].astype(np.float32).reshape(n, 3).copy(), lab=out["Label"].astype(np.uint16).copy(),
+                 typ=out["Type"].astype(np.uint8).copy(), part=out["Partner"].astype(np.uint16).reshape(n, 2).copy())
