@@ -32,6 +32,7 @@
 // point (2^-32) with integer atomics, exact and associative. The gradients are
 // bit-identical run to run.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -44,6 +45,19 @@
 #include "../../include/v2m_cuda.h"
 
 namespace v2m_adj {
+
+// an NVTX range over a call of the unroll's C ABI (header-only NVTX: a branch
+// when no profiler is attached)
+struct Trace {
+    explicit Trace(const char* name) {
+        nvtxRangePushA(name);
+    }
+    ~Trace() {
+        nvtxRangePop();
+    }
+    Trace(const Trace&) = delete;
+    Trace& operator=(const Trace&) = delete;
+};
 
 constexpr double kFix = 4294967296.0;   // 2^32
 constexpr int kT = 256;
@@ -709,6 +723,7 @@ const char* v2m_unroll_last_error(void) {
 int v2m_unroll_create(int64_t n, const int32_t* nbr, const int32_t* nnb, const uint8_t* typ, const int32_t* m,
                       const float* cs, float fscale, float fsurf, float dt, int K, int ckpt, int device,
                       v2m_unroll** out) {
+    v2m_adj::Trace trace("v2m_unroll_create");
     return uguard([&] {
         if (!out || n < 1 || n > (1 << 29) || !nbr || !nnb || !typ || !m || !cs || K < 1 || ckpt < 1) {
             throw std::invalid_argument("bad argument");
@@ -824,6 +839,7 @@ int v2m_unroll_destroy(v2m_unroll* u) {
 }
 
 int v2m_unroll_forward(v2m_unroll* u, const float* x0, const float* G, float* xK, int replay) {
+    v2m_adj::Trace trace("v2m_unroll_forward");
     return uguard([&] {
         if (!u || !x0 || !G || !xK) {
             throw std::invalid_argument("bad argument");
@@ -876,6 +892,7 @@ int v2m_unroll_loss(v2m_unroll* u, const float* x, const float* G, double* loss)
 // gx = gscale * dLoss/dx at x; gG += gscale * dLoss/dG (gG overwritten when accumulate == 0)
 int v2m_unroll_loss_backward(v2m_unroll* u, const float* x, const float* G, float gscale, float* gx, float* gG,
                              int accumulate) {
+    v2m_adj::Trace trace("v2m_unroll_loss_backward");
     return uguard([&] {
         if (!u || !x || !G || !gx || !gG) {
             throw std::invalid_argument("bad argument");
@@ -899,6 +916,7 @@ int v2m_unroll_loss_backward(v2m_unroll* u, const float* x, const float* G, floa
 // reverse of the last forward pass: gxK = dL/dxK in, gx0 = dL/dx0 out,
 // gG (overwritten) = dL/dG through the steps, plus gG_in (may be null) from other terms
 int v2m_unroll_backward(v2m_unroll* u, const float* G, const float* gxK, float* gx0, float* gG, const float* gG_in) {
+    v2m_adj::Trace trace("v2m_unroll_backward");
     return uguard([&] {
         if (!u || !G || !gxK || !gx0 || !gG) {
             throw std::invalid_argument("bad argument");

@@ -8,6 +8,7 @@
 // round trip and a run of iterations replays as one graph. The host reads the
 // per-volume control blocks only between graph replays, to stop early.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <sys/mman.h>
 
 #include <algorithm>
@@ -108,7 +109,23 @@ struct StageClock {
 };
 thread_local StageClock* g_clock = nullptr;
 
+// Tracing: an NVTX range over every call of the C ABI, and an NVTX mark at each
+// stage a call passes (lap), so a profiler's timeline (Nsight Systems, ncu's
+// NVTX filters) shows the library's calls and their stages beside the kernels.
+// NVTX is header-only here: without a tool attached each call costs a branch.
+struct Trace {
+    explicit Trace(const char* name) {
+        nvtxRangePushA(name);
+    }
+    ~Trace() {
+        nvtxRangePop();
+    }
+    Trace(const Trace&) = delete;
+    Trace& operator=(const Trace&) = delete;
+};
+
 void lap(const char* stage) {
+    nvtxMarkA(stage);
     if (g_clock) {
         g_clock->lap(stage);
     }
@@ -1340,6 +1357,7 @@ int v2m_cuda_device_count(void) {
 
 int v2m_session_create(int nvol, const v2m_grid_view* g, const v2m_relax_params* prm, const v2m_nodes_view* nd,
                        int device, v2m_session** out) {
+    Trace trace("v2m_session_create");
     return guard([&] {
         if (!out) {
             throw ArgError("null output");
@@ -1366,6 +1384,7 @@ int v2m_session_reset(v2m_session* s) {
 }
 
 int v2m_session_rebuild(v2m_session* s) {
+    Trace trace("v2m_session_rebuild");
     return guard([&] {
         ck(cudaSetDevice(s->device), "cudaSetDevice");
         do_rebuild(s);
@@ -1373,6 +1392,7 @@ int v2m_session_rebuild(v2m_session* s) {
 }
 
 int v2m_session_force(v2m_session* s) {
+    Trace trace("v2m_session_force");
     return guard([&] {
         ck(cudaSetDevice(s->device), "cudaSetDevice");
         enqueue_force(s, nullptr, nullptr);
@@ -1382,6 +1402,7 @@ int v2m_session_force(v2m_session* s) {
 }
 
 int v2m_session_step_tail(v2m_session* s) {
+    Trace trace("v2m_session_step_tail");
     return guard([&] {
         ck(cudaSetDevice(s->device), "cudaSetDevice");
         enqueue_tail(s);
@@ -1391,6 +1412,7 @@ int v2m_session_step_tail(v2m_session* s) {
 }
 
 int v2m_session_iterate(v2m_session* s, int iters, int graph) {
+    Trace trace("v2m_session_iterate");
     return guard([&] {
         ck(cudaSetDevice(s->device), "cudaSetDevice");
         do_iterate(s, iters, graph);
@@ -1398,6 +1420,7 @@ int v2m_session_iterate(v2m_session* s, int iters, int graph) {
 }
 
 int v2m_session_run(v2m_session* s, int graph) {
+    Trace trace("v2m_session_run");
     return guard([&] {
         ck(cudaSetDevice(s->device), "cudaSetDevice");
         do_rebuild(s);
@@ -1927,6 +1950,7 @@ int v2m_session_clear_counters(v2m_session* s) {
 
 int v2m_seed_cuda(const v2m_grid_view* g, const v2m_relax_params* prm, int device, v2m_seed_result** out,
                   int64_t* n) {
+    Trace trace("v2m_seed_cuda");
     return guard([&] {
         if (!out || !n) {
             throw ArgError("null argument");
@@ -2000,6 +2024,7 @@ void v2m_grid_params_default(v2m_grid_params* p) {
 
 int v2m_grid_build_cuda(const uint16_t* L, int32_t nx, int32_t ny, int32_t nz, const float* vs,
                         const v2m_grid_params* p, int device, v2m_grid_result** out) {
+    Trace trace("v2m_grid_build_cuda");
     return guard([&] {
         if (!out) {
             throw ArgError("null argument");
@@ -2078,6 +2103,7 @@ int v2m_grid_build_cuda(const uint16_t* L, int32_t nx, int32_t ny, int32_t nz, c
 
 int v2m_points_cuda(const uint16_t* L, int32_t nx, int32_t ny, int32_t nz, const float* vs, const v2m_grid_params* gp,
                     const v2m_relax_params* prm, int device, v2m_seed_result** out, int64_t* n, v2m_relax_stats* st) {
+    Trace trace("v2m_points_cuda");
     v2m_session* s = nullptr;
     v2m_session tmp;   // (the allocation context of the grid build and the seeding)
     GridBuildOut O;
@@ -2257,6 +2283,7 @@ int v2m_relax_cuda(const v2m_grid_view* g, const v2m_relax_params* prm, v2m_node
 
 int v2m_relax_cuda_batch(int nvol, const v2m_grid_view* g, const v2m_relax_params* prm, v2m_nodes_view* nd,
                          v2m_relax_stats* st, int device) {
+    Trace trace("v2m_relax_cuda_batch");
     v2m_session* s = nullptr;
     StageClock clock("relax_cl:");
     g_clock = &clock;
