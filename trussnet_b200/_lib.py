@@ -12,7 +12,9 @@ import threading
 from .types import GridView, NodesView, RelaxParamsC, RelaxStatsC
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libv2m_cuda.so")
+# V2M_CUDA_LIBRARY selects another build of the library: libv2m_cuda_check.so,
+# the one with device bounds checks, for checked runs
+LIB_PATH = os.environ.get("V2M_CUDA_LIBRARY") or os.path.join(HERE, "libv2m_cuda.so")
 
 V2M_OK, V2M_ERR_ARG, V2M_ERR_CUDA, V2M_ERR_KERNEL, V2M_ERR_STATE = 0, -1, -2, -3, -4
 

@@ -2,6 +2,7 @@
 
   trussnet_b200/libv2m_cuda.so     the CUDA relaxation (csrc/*.cu), sm_100a, C ABI of
                                    include/v2m_cuda.h
+  trussnet_b200/libv2m_cuda_check.so  the same with device bounds checks (V2M_CHECK)
   trussnet_b200/libv2m_relax_cl.so the C++ shim tn::relax_cl (csrc/relax_cl_shim.cpp),
                                    built only where the reference headers are present
 
@@ -20,6 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libv2m_cuda.so")
+LIB_CHECK = os.path.join(HERE, "libv2m_cuda_check.so")   # the bounds-checked build (V2M_CHECK)
 SHIM = os.path.join(HERE, "libv2m_relax_cl.so")
 
 
@@ -56,33 +58,45 @@ def _stale(out: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build_cuda(force: bool = False, verbose: bool = False) -> str:
+def build_cuda(force: bool = False, verbose: bool = False, check: bool = False) -> str:
+    """libv2m_cuda.so; check=True: libv2m_cuda_check.so, the same sources with
+    V2M_CHECK (device bounds checks on the lookups whose ranges hold by
+    construction; a failed check makes the call return V2M_ERR_KERNEL). The
+    sources compile in parallel."""
+    out = LIB_CHECK if check else LIB
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "v2m_cuda.h"), __file__]
-    if not force and not _stale(LIB, deps):
-        return LIB
-    objs = []
-    logs = []
+    if not force and not _stale(out, deps):
+        return out
+    flags = NVCC_FLAGS + (["-DV2M_CHECK"] if check else [])
+    tag = ".check" if check else ""
+    jobs = []
     for src in SOURCES:
-        obj = os.path.join(CSRC, src.replace(".cu", ".o"))
-        cmd = [nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        logs.append(r.stdout + r.stderr)
-        if r.returncode != 0:
-            raise RuntimeError(f"nvcc failed on {src}:\n{r.stderr[-6000:]}")
+        obj = os.path.join(CSRC, src.replace(".cu", tag + ".o"))
+        cmd = [nvcc(), *flags, "-c", os.path.join(CSRC, src), "-o", obj]
+        jobs.append((src, obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+    objs, logs, failed = [], [], None
+    for src, obj, pr in jobs:
+        o, e = pr.communicate()
+        logs.append(o + e)
+        if pr.returncode != 0 and failed is None:
+            failed = f"nvcc failed on {src}:\n{e[-6000:]}"
         objs.append(obj)
-    tmp = LIB + ".tmp"
+    if failed:
+        raise RuntimeError(failed)
+    tmp = out + ".tmp"
     cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp, *objs, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")
-    os.replace(tmp, LIB)
+    os.replace(tmp, out)
     for o in objs:
         os.remove(o)
-    with open(os.path.join(CSRC, "ptxas_info.txt"), "w") as f:
-        f.write("\n".join(line for log in logs for line in log.splitlines() if "ptxas" in line))
+    if not check:
+        with open(os.path.join(CSRC, "ptxas_info.txt"), "w") as f:
+            f.write("\n".join(line for log in logs for line in log.splitlines() if "ptxas" in line))
     if verbose:
         print("\n".join(logs))
-    return LIB
+    return out
 
 
 def build_shim(force: bool = False) -> str | None:
@@ -135,6 +149,7 @@ def build_oracle() -> None:
 
 def build_all(force: bool = False) -> None:
     build_cuda(force=force)
+    build_cuda(force=force, check=True)
     build_shim(force=force)
     build_oracle()
     build_dropin(force=force)

@@ -75,6 +75,10 @@ __device__ __forceinline__ int slot_lookup(const DGrid& g, int b, int l, int* ha
     *has = 1;
     const int idx = __ffs(bits) - 1;
     const int first = __ldg(g.bl_slot + b);
+    if (kChecked && first >= 0 && (int64_t)first + idx >= g.nslots) {
+        check_fail(g.chk, 20, b);   // a brick's slot beyond the phi array
+        return -1;
+    }
     return first < 0 ? -1 : first + idx;
 }
 
@@ -158,6 +162,14 @@ __device__ __forceinline__ int lab_index(const LabList& ll, int n, int l) {
 __device__ __forceinline__ void cell_corners(const DGrid& g, const Cell& c, int l, float* out) {
     if (c.fast) {
         const int idx = lab_index(c.ll, c.n, l);
+        if (kChecked && idx >= 0 && c.first >= 0 && (int64_t)c.first + idx >= g.ntab) {
+            check_fail(g.chk, 21, c.first);   // a brick's corner table beyond the tables
+#pragma unroll
+            for (int n = 0; n < 8; ++n) {
+                out[n] = 0.0f;
+            }
+            return;
+        }
         if (idx >= 0 && c.first >= 0) {
             const float* base = g.xphi + (size_t)(c.first + idx) * 729 + (c.i0 & 7) + 9 * ((c.j0 & 7) + 9 * (c.k0 & 7));
 #pragma unroll

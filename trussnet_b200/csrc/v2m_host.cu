@@ -320,6 +320,7 @@ cudaError_t staged_d2h(void* dst, const void* src, size_t bytes, cudaStream_t s)
 
 struct v2m_session {
     int device = 0;
+    int* chk = nullptr;   // the checked build's bounds-check word (device, 2 ints)
     cudaStream_t stream = nullptr;
     int nvol = 0;
     std::vector<DVol> hvols;
@@ -376,6 +377,19 @@ bool tune_lookup(v2m_session* s);
 void tune_store(v2m_session* s);
 std::string do_autotune(v2m_session* s, int reps);
 
+// The checked build's bounds-check word of the session's grids (code, index).
+void check_bounds_word(v2m_session* s) {
+    if (!s->chk) {
+        return;
+    }
+    int w[2] = { 0, 0 };
+    ck(cudaMemcpyAsync(w, s->chk, sizeof(w), cudaMemcpyDeviceToHost, s->stream), "read bounds checks");
+    ck(cudaStreamSynchronize(s->stream), "synchronize");
+    if (w[0]) {
+        throw KernelError("bounds check " + std::to_string(w[0]) + " failed at index " + std::to_string(w[1]));
+    }
+}
+
 void check_kernel_error(v2m_session* s) {
     Global g;
     ck(cudaMemcpyAsync(&g, s->d.G, sizeof(Global), cudaMemcpyDeviceToHost, s->stream), "read error flag");
@@ -383,6 +397,7 @@ void check_kernel_error(v2m_session* s) {
     if (g.err) {
         throw KernelError("kernel error " + std::to_string(g.err) + " at index " + std::to_string(g.err_info));
     }
+    check_bounds_word(s);
 }
 
 // True when p is device memory (not readable by the host): views may carry
@@ -556,6 +571,7 @@ void build_corner_tables(v2m_session* s, DGrid& g, size_t nb) {
     ck(cudaStreamSynchronize(s->stream), "synchronize");   // (tabs and rec are host vectors)
     g.xbrick = xbrick;
     g.xphi = xphi;
+    g.ntab = (int64_t)tabs.size();
 }
 
 // One volume's fields on the device: the caller's arrays uploaded, and the
@@ -579,7 +595,15 @@ DGrid upload_grid(v2m_session* s, const v2m_grid_view* g) {
     G.bl_lab = upload(s, g->bl_lab, nb * V2M_BL);
     G.bl_slot = upload(s, g->bl_slot, nb);
     G.phi = upload(s, g->phi, (size_t)g->nslots * V2M_SLOT);
+    G.nslots = g->nslots;
     G.hvox = upload(s, g->h, nvox);
+    if (kChecked) {   // one bounds-check word per session, shared by its grids
+        if (!s->chk) {
+            s->chk = s->alloc<int>(2);
+            ck(cudaMemsetAsync(s->chk, 0, 2 * sizeof(int), s->stream), "memset");
+        }
+        G.chk = s->chk;
+    }
     G.gm = g->gm;
     if (g->gm > 0) {
         G.gI = upload(s, g->gI, nvox);
@@ -1219,7 +1243,15 @@ void seed_on(v2m_session& tmp, const v2m_grid_view* g, const v2m_relax_params* p
     cudaDeviceGetAttribute(&A.sms, cudaDevAttrMultiProcessorCount, dev);
     A.stream = tmp.stream;
     std::string err;
-    const cudaError_t e = seed_run(A, B, err);
+    cudaError_t e = seed_run(A, B, err);
+    if (e == cudaSuccess) {
+        try {
+            check_bounds_word(&tmp);
+        } catch (...) {
+            release_seeds(B, tmp.stream);
+            throw;
+        }
+    }
     if (e != cudaSuccess) {
         release_seeds(B, tmp.stream);
         cudaGetLastError();

@@ -560,8 +560,17 @@ __device__ void warp_neighbors(const DVol& V, int64_t i, int lane, NbrWarpSmem& 
             }
             if (!skip) {
                 const int key0 = qkey + (xa - qx0) + H.dim[L][0] * (cy + H.dim[L][1] * cz);
-                s0 = cs[key0];
-                c = cs[key0 + (xb - xa) + 1] - s0;
+                if (kChecked && (key0 < 0 || key0 + (xb - xa) + 1 > V.nkeys)) {
+                    check_fail(V.g.chk, 22, i);   // a search row beyond the volume's bins
+                    skip = true;
+                } else {
+                    s0 = cs[key0];
+                    c = cs[key0 + (xb - xa) + 1] - s0;
+                    if (kChecked && (c < 0 || s0 < V.nofs || s0 + c > V.nofs + V.n)) {
+                        check_fail(V.g.chk, 23, i);   // bin starts outside the volume's nodes
+                        c = 0;
+                    }
+                }
             }
         }
         // compact the non-empty rows to the first lanes (so that row ends are
@@ -695,6 +704,12 @@ __global__ void __launch_bounds__(kNbrMaxThreads, 4) k_refresh(const DVol* __res
     const int nw = gridDim.x * wpb;
     for (int e = blockIdx.x * wpb + w; e < cnt; e += nw) {
         const int64_t i = rlist[e];
+        if (kChecked && (i < 0 || i >= N || cnt > N)) {
+            if (lane == 0) {
+                raise_error(G, 25, e);   // a refresh entry beyond the nodes
+            }
+            continue;
+        }
         const int v = nodevol[i];
         // a volume that rebuilds this iteration rebuilds every list and sets every
         // build position next (src/v2m_particles.cpp:771-820): its refreshes would
@@ -1111,6 +1126,10 @@ __global__ void __launch_bounds__(kMainThreads, V2M_MOVE_MIN_BLOCKS) k_move_main
         i = queue[N + (q - qa)];
     } else if (q < tot) {
         i = queue[N - 1 - (q - qa - qj)];
+    }
+    if (kChecked && (i < -1 || i >= N || tot > N)) {
+        raise_error(G, 24, (int)q);   // a move queue entry (or length) beyond the nodes
+        i = -1;
     }
     int v = i >= 0 ? nodevol[i] : -1;
     if (shape_any && v >= 0 && (vols[v].g.gm < 0) != kShape) {

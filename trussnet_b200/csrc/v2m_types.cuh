@@ -47,7 +47,28 @@ struct DGrid {
     // 8 bytes of padding.
     const uint4* xbrick;    // 3 per brick
     const float* xphi;      // 729 floats per table, x fastest
+    int64_t nslots;         // phi slots (512 floats each)
+    int64_t ntab;           // corner tables (729 floats each)
+    // The checked build (V2M_CHECK) records its first failed bounds check here
+    // (code, index) and skips the access; the host reads it after each run.
+    int* chk;
 };
+
+// V2M_CHECK: the build with device bounds checks on the lookups whose ranges
+// hold by construction (the sanitizer substitute: a failed check records an
+// error code and its index, skips the access, and the call returns
+// V2M_ERR_KERNEL; nothing traps). Without it the checks compile away.
+#ifdef V2M_CHECK
+constexpr bool kChecked = true;
+#else
+constexpr bool kChecked = false;
+#endif
+
+__device__ __forceinline__ void check_fail(int* chk, int code, long long info) {
+    if (chk && atomicCAS(chk, 0, code) == 0) {
+        chk[1] = (int)info;
+    }
+}
 
 // Multi-level hash geometry (V2mHash, src/opencl/v2m_particle_body.cl:21-27).
 struct DHash {
