@@ -929,7 +929,7 @@ __device__ __forceinline__ void tail_flush(TailAcc& a, VolCtl* cv) {
 // front of the queue, INTERIOR ones at the back, so that a warp of k_move_main
 // holds nodes of one kind. The FIRE power of the block is summed here, in node
 // order (a fixed-shape double tree: deterministic whatever the queue order).
-__global__ void __launch_bounds__(kMoveThreads) k_move_pre(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl,
+__global__ void __launch_bounds__(kMoveThreads, 5) k_move_pre(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl,
                                                           const uint16_t* __restrict__ nodevol,
                                                           const float4* __restrict__ Pq, const float4* __restrict__ F,
                                                           float4* __restrict__ Vel, const uint8_t* __restrict__ typ,
@@ -966,19 +966,24 @@ __global__ void __launch_bounds__(kMoveThreads) k_move_pre(const DVol* __restric
             const float fdt = c.fdt, falpha = c.falpha;
             const float4 pq = Pq[i];
             const int ty0 = typ[i];
+            // the node's force and velocity read with its record, ahead of the
+            // branches that use them (one round of loads; a CORNER node's or a
+            // zeroed velocity's values go unused)
+            const float4 f4pre = F[i];
+            const float4 v4pre = Vel[i];
             // h at the node's position (v2m_move's v2m_h_at), which the stored size is unless a caller
             // overwrote positions or sizes
             const float h = Vd.hn_exact ? fabsf(pq.w) : size_at(Vd.g, Vd.hmode, pq.x, pq.y, pq.z);
             bool finished = true;
             if (ty0 != V2M_CORNER) {
-                const float4 f4 = F[i];
+                const float4 f4 = f4pre;
                 const float stiff = f4.w > 1.0f ? f4.w : 1.0f;
                 const float ac[3] = { f4.x / stiff, f4.y / stiff, f4.z / stiff };
                 float s[3];
                 if (fire) {
                     float vv[3] = { 0.0f, 0.0f, 0.0f };
                     if (!c.vzero) {
-                        const float4 v4 = Vel[i];
+                        const float4 v4 = v4pre;
                         vv[0] = v4.x;
                         vv[1] = v4.y;
                         vv[2] = v4.z;
