@@ -194,7 +194,7 @@ def optimize_sizing(unroll, x0, G0, steps=20, step=0.05, hmin=None, hmax=None):
         Gv = G.clone().requires_grad_(True)
         L = unrolled_loss(x0, Gv, unroll)
         L.backward()
-        losses.append(float(L))
+        losses.append(float(L.detach()))
         g = Gv.grad
         with torch.no_grad():
             G = (G - scale * g / g.abs().max().clamp_min(1e-30)).clamp_(lo, hi).contiguous()
@@ -216,7 +216,7 @@ def optimize_positions(unroll, x0, G, steps=20, step=0.05):
         xv = x.clone().requires_grad_(True)
         L = unrolled_loss(xv, G, unroll)
         L.backward()
-        losses.append(float(L))
+        losses.append(float(L.detach()))
         g = xv.grad
         with torch.no_grad():
             x = (x - step * cell * g / g.norm(dim=1).max().clamp_min(1e-30)).contiguous()
