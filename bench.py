@@ -684,11 +684,13 @@ def run_cuda(args):
     move_ms = stages["move"] / nprof if nprof else 0.0
     move_bytes = 91 * n + 112 * trapped
     move_achieved = move_bytes / (move_ms / 1e3) / 1e9 if move_ms > 0 else None
-    move_roofline = {"kernel": "k_move_pre + k_move_main", "bound": "hbm", "achieved": move_achieved, "peak": peak,
-                     "unit": "GB/s", "frac": move_achieved / peak if move_achieved else None,
+    # (traffic: the ncu dram bytes of one iteration's k_move_int + k_move_main)
+    mtr = [profiled_traffic(k, args.workload) for k in ("k_move_int", "k_move_main")]
+    move_roofline = {"kernel": "k_move_pre + k_move_int + k_move_main", "bound": "hbm", "achieved": move_achieved,
+                     "peak": peak, "unit": "GB/s", "frac": move_achieved / peak if move_achieved else None,
                      "peak_source": peak_kind, "bytes_per_iteration": move_bytes, "ms_per_iteration": move_ms,
                      "queued_trapped": trapped, "queued_interior": interior,
-                     "traffic": profiled_traffic("k_move_main", args.workload)}
+                     "traffic": sum(mtr) if all(t is not None for t in mtr) else None}
     # end to end through the public call (tn::relax_cl's C ABI) with pinned host buffers
     e2e = None
     if args.e2e_steps > 0:

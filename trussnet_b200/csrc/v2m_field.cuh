@@ -158,31 +158,37 @@ __device__ __forceinline__ int lab_index(const LabList& ll, int n, int l) {
     return bits ? __ffs(bits) - 1 : -1;
 }
 
+// the 8 corners of phi_l in a cell whose base voxel lies inside the grid
+// (c.fast): from its brick's corner table, or the uniform value
+__device__ __forceinline__ void table_corners(const DGrid& g, const Cell& c, int l, float* out) {
+    const int idx = lab_index(c.ll, c.n, l);
+    if (kChecked && idx >= 0 && c.first >= 0 && (int64_t)c.first + idx >= g.ntab) {
+        check_fail(g.chk, 21, c.first);   // a brick's corner table beyond the tables
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+            out[n] = 0.0f;
+        }
+        return;
+    }
+    if (idx >= 0 && c.first >= 0) {
+        const float* base = g.xphi + (size_t)(c.first + idx) * 729 + (c.i0 & 7) + 9 * ((c.j0 & 7) + 9 * (c.k0 & 7));
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+            out[n] = __ldg(base + (n & 1) + 9 * ((n >> 1) & 1) + 81 * (n >> 2));
+        }
+    } else {
+        const float f = idx >= 0 ? 1.0f : 0.0f;   // uniform table: its label everywhere; absent label: 0
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+            out[n] = f;
+        }
+    }
+}
+
 // the 8 corners of phi_l in the cell
 __device__ __forceinline__ void cell_corners(const DGrid& g, const Cell& c, int l, float* out) {
     if (c.fast) {
-        const int idx = lab_index(c.ll, c.n, l);
-        if (kChecked && idx >= 0 && c.first >= 0 && (int64_t)c.first + idx >= g.ntab) {
-            check_fail(g.chk, 21, c.first);   // a brick's corner table beyond the tables
-#pragma unroll
-            for (int n = 0; n < 8; ++n) {
-                out[n] = 0.0f;
-            }
-            return;
-        }
-        if (idx >= 0 && c.first >= 0) {
-            const float* base = g.xphi + (size_t)(c.first + idx) * 729 + (c.i0 & 7) + 9 * ((c.j0 & 7) + 9 * (c.k0 & 7));
-#pragma unroll
-            for (int n = 0; n < 8; ++n) {
-                out[n] = __ldg(base + (n & 1) + 9 * ((n >> 1) & 1) + 81 * (n >> 2));
-            }
-        } else {
-            const float f = idx >= 0 ? 1.0f : 0.0f;   // uniform table: its label everywhere; absent label: 0
-#pragma unroll
-            for (int n = 0; n < 8; ++n) {
-                out[n] = f;
-            }
-        }
+        table_corners(g, c, l, out);
         return;
     }
 #pragma unroll

@@ -890,7 +890,8 @@ void enqueue_tail(v2m_session* s) {
     launch_move(s->stream, d);
     launch_control(s->stream, d, s->serial_power);
     launch_refresh(s->stream, d, s->refresh_blocks);
-    s->launches += 4 + (s->serial_power ? 1 : 0);
+    // k_move_pre, k_move_int, k_move_main (and its shape instance), control, refresh
+    s->launches += 5 + (d.shape_any ? 1 : 0) + (s->serial_power ? 1 : 0);
     enqueue_rebuild(s);
 }
 

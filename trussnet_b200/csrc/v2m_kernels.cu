@@ -734,6 +734,7 @@ __global__ void __launch_bounds__(kNbrMaxThreads, 4) k_refresh(const DVol* __res
             G->qtrap = 0;
             G->qint = 0;
             G->qjun = 0;
+            G->qdef = 0;
             G->blocks_done = 0;
             __threadfence();
         }
@@ -1094,11 +1095,215 @@ __global__ void __launch_bounds__(kMoveThreads, 5) k_move_pre(const DVol* __rest
     tail_flush(acc, ctl + bv);
 }
 
+// The iteration's reductions of the nodes a warp finished (the lanes of `act`,
+// this lane among them), combined with warp votes: log2 histogram, max |dp|/h,
+// half-skin count, max displacement (one lane per volume and bin), and the
+// refresh list with one atomic per warp (src/v2m_particles.cpp:874-937).
+__device__ __forceinline__ void warp_tail(const DVol& Vd, VolCtl* cv, int v, int64_t i, unsigned act, unsigned lane,
+                                          float m, float px, float py, float pz, float hh,
+                                          const float4* __restrict__ P0, int* __restrict__ rlist, Global* G) {
+    const float4 q0 = P0[i];
+    const float ex = px - q0.x, ey = py - q0.y, ez = pz - q0.z;
+    const float m2 = ex * ex + ey * ey + ez * ez, s2 = Vd.skin * Vd.skin * hh * hh;
+    const int b = hist_bin(m);
+    const unsigned gb = __match_any_sync(act, (unsigned)(v << 5) | (unsigned)b);
+    if (lane == (unsigned)(__ffs(gb) - 1)) {
+        atomicAdd(&cv->hist[b], __popc(gb));
+    }
+    const unsigned gvol = __match_any_sync(act, (unsigned)v);
+    const unsigned leader = (unsigned)(__ffs(gvol) - 1);
+    const unsigned mx = __reduce_max_sync(gvol, __float_as_uint(m));
+    const bool refresh = m2 > s2 && Vd.policy != 2;   // (policy 2: the first build's lists for the whole run)
+    const bool half = !refresh && m2 > 0.25f * s2;
+    const unsigned nh = __popc(__ballot_sync(act, half) & gvol);
+    unsigned md = 0u;
+    if (Vd.policy == 1) {
+        md = __reduce_max_sync(gvol, __float_as_uint(sqrtf(m2) / hh));
+    }
+    const int slot = blockIdx.x & (kCtlSlots - 1);
+    if (lane == leader) {
+        if (mx) {
+            atomicMax(&cv->maxbits_p[slot], mx);
+        }
+        if (nh) {
+            atomicAdd(&cv->nhalf_p[slot], (int)nh);
+        }
+        if (md) {
+            atomicMax(&cv->maxd_p[slot], md);
+        }
+    }
+    const unsigned rm = __ballot_sync(act, refresh);
+    if (rm) {
+        const unsigned first = (unsigned)(__ffs(rm) - 1);
+        int base = 0;
+        if (lane == first) {
+            base = atomicAdd(&G->nrefresh, __popc(rm));
+        }
+        base = __shfl_sync(act, base, first);
+        if (refresh) {
+            rlist[base + __popc(rm & ((1u << lane) - 1u))] = (int)i;
+        }
+        const unsigned rv = rm & gvol;
+        if (lane == leader && rv) {
+            atomicAdd(&cv->nrefresh, __popc(rv));
+        }
+    }
+}
+
+// Second half of v2m_move for the queued INTERIOR nodes whose move stays
+// INTERIOR (label fields, smooth mode): v2m_move_step's owner ranking at
+// q = p + s and its snap test (src/opencl/v2m_particle_body.cl:659-700), then
+// the node's velocity, |dp|/h, size and the iteration's reductions. This is
+// the common case of the move (most queued nodes) and needs none of the
+// trapped move's projections, so it runs as its own kernel with no
+// out-of-line calls: the ranking reads the bricks' corner tables only, and
+// its warps do not share blocks with the long trapped moves. A node whose
+// move may leave INTERIOR -- its owner label changes, or the snap test's
+// distance estimate is within reach -- or whose step trips the safety net,
+// or whose cell needs the per-corner path, and every node of a volume with
+// analytic shape fields, gray fields or voxel mode, is handed to k_move_main
+// unchanged (appended behind the JUNCTION queue): nothing of it is written
+// here, and k_move_main's move_step takes it from the start, so every node's
+// result is move_step's.
+#ifndef V2M_INT_MIN_BLOCKS
+#define V2M_INT_MIN_BLOCKS 8   // resident blocks of k_move_int per multiprocessor (8 x 128 threads: 64 registers)
+#endif
+__global__ void __launch_bounds__(kMainThreads, V2M_INT_MIN_BLOCKS) k_move_int(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl,
+                                                         const uint16_t* __restrict__ nodevol, float4* __restrict__ Pq,
+                                                         float4* __restrict__ Vel, const uint16_t* __restrict__ lab,
+                                                         float* __restrict__ mvout, const float4* __restrict__ P0,
+                                                         const float4* __restrict__ S, int* __restrict__ queue,
+                                                         int* __restrict__ rlist, Global* G, int64_t N) {
+    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int qb = *((volatile int*)&G->qint), qj = *((volatile int*)&G->qjun);
+    if (blockIdx.x * (int64_t)blockDim.x >= qb) {
+        return;
+    }
+    const unsigned lane = threadIdx.x & 31u;
+    int64_t i = q < qb ? queue[N - 1 - q] : -1;
+    if (kChecked && (i < -1 || i >= N)) {
+        raise_error(G, 24, (int)q);   // a move queue entry beyond the nodes
+        i = -1;
+    }
+    const int v = i >= 0 ? nodevol[i] : -1;
+    bool fin = false, defer = false;
+    float m = 0.0f, qx = 0.0f, qy = 0.0f, qz = 0.0f, hn = 0.0f;
+    if (v >= 0) {
+        const DVol& Vd = vols[v];
+        const DGrid& g = Vd.g;
+        if (g.gm != 0 || Vd.voxmode) {
+            defer = true;
+        } else {
+            const float4 pq = Pq[i];
+            const float4 s4 = S[i];
+            const int a = lab[i];
+            const float h = s4.w;
+            qx = pq.x + s4.x;
+            qy = pq.y + s4.y;
+            qz = pq.z + s4.z;
+            // owner_on_cell's ranking at q, on the brick's corner tables only
+            LabList ll;
+            const int n = labels_near(g, qx, qy, qz, ll);
+            if (n == 1) {
+                defer = ll.get(0) != a;
+            } else {
+                Cell cl;
+                cell_at(g, qx, qy, qz, cl);
+                defer = !cl.fast;   // the per-corner path (a cell based outside the grid, or among > 16 labels)
+                if (!defer) {
+                    int best = ll.get(0), sec = V2M_NOLAB;
+                    float pb = -1.0f, ps = pb;
+#pragma unroll 1
+                    for (int t = 0; t < n; t += 2) {
+                        const int l0 = ll.get(t);
+                        const bool two = t + 1 < n;
+                        const int l1 = two ? ll.get(t + 1) : l0;
+                        float c0[8], c1[8];
+                        table_corners(g, cl, l0, c0);
+                        table_corners(g, cl, l1, c1);
+                        const float v0 = trilerp8(c0, cl.fx, cl.fy, cl.fz), v1 = trilerp8(c1, cl.fx, cl.fy, cl.fz);
+                        if (v0 > pb) {
+                            ps = pb;
+                            sec = best;
+                            pb = v0;
+                            best = l0;
+                        } else if (v0 > ps) {
+                            ps = v0;
+                            sec = l0;
+                        }
+                        if (two) {
+                            if (v1 > pb) {
+                                ps = pb;
+                                sec = best;
+                                pb = v1;
+                                best = l1;
+                            } else if (v1 > ps) {
+                                ps = v1;
+                                sec = l1;
+                            }
+                        }
+                    }
+                    defer = best != a;
+                    if (!defer && sec != V2M_NOLAB && Vd.snap > 0.0f) {
+                        // psi_grad_on(a, sec) on the ranked cell, as move_step
+                        float c[8], e[8];
+                        table_corners(g, cl, a, c);
+                        table_corners(g, cl, sec, e);
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) {
+                            c[k] -= e[k];
+                        }
+                        const float4 r = psi_grad_diff(g, c, cl.fx, cl.fy, cl.fz);
+                        const float gn = sqrtf(r.x * r.x + r.y * r.y + r.z * r.z);
+                        defer = gn > 1e-9f && r.w / gn < Vd.snap * h;
+                    }
+                }
+            }
+            if (!defer) {
+                const float lim = (Vd.maxstep + fmaxf(Vd.snap, 0.5f)) * h;
+                const float m2 = (qx - pq.x) * (qx - pq.x) + (qy - pq.y) * (qy - pq.y) + (qz - pq.z) * (qz - pq.z);
+                if (!(m2 <= lim * lim)) {
+                    defer = true;
+                } else {
+                    m = sqrtf(m2) / h;
+                    hn = size_at(g, Vd.hmode, qx, qy, qz);
+                    fin = true;
+                    if (Vd.fire) {
+                        const float fdt = ctl[v].fdt;
+                        Vel[i] = m > 0.0f ? make_float4((qx - pq.x) / fdt, (qy - pq.y) / fdt, (qz - pq.z) / fdt, 0.0f)
+                                          : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    }
+                    mvout[i] = m;
+                    Pq[i] = make_float4(qx, qy, qz, pack_h(hn, V2M_INTERIOR));
+                    // (typ and part stay as they are: an INTERIOR node keeps both)
+                }
+            }
+        }
+    }
+    const unsigned fm = __ballot_sync(0xffffffffu, fin);
+    if (fin) {
+        warp_tail(vols[v], ctl + v, v, i, fm, lane, m, qx, qy, qz, hn, P0, rlist, G);
+    }
+    const unsigned dm = __ballot_sync(0xffffffffu, defer);
+    if (dm) {
+        const unsigned first = (unsigned)(__ffs(dm) - 1);
+        int base = 0;
+        if (lane == first) {
+            base = atomicAdd(&G->qdef, __popc(dm));
+        }
+        base = __shfl_sync(0xffffffffu, base, first);
+        if (defer) {
+            queue[N + qj + base + __popc(dm & ((1u << lane) - 1u))] = (int)i;
+        }
+    }
+}
+
 // Second half of v2m_move: the trapped move (v2m_move_step) of every queued
-// node, then its velocity, |dp|/h and the iteration's reductions. Blocks of
-// kMainThreads with no block-wide barrier: a warp's statistics are combined
-// with warp votes and flushed by one lane per (volume, bin), so a finished warp
-// never waits for a slower one.
+// trapped node and of the INTERIOR nodes k_move_int handed over, then its
+// velocity, |dp|/h and the iteration's reductions. Blocks of kMainThreads with
+// no block-wide barrier: a warp's statistics are combined with warp votes and
+// flushed by one lane per (volume, bin), so a finished warp never waits for a
+// slower one.
 // Two instances: kShape = false moves the nodes of volumes with sampled fields,
 // kShape = true (launched only when some volume has them) those with analytic
 // shape fields; with both present each skips the other's nodes.
@@ -1114,23 +1319,22 @@ __global__ void __launch_bounds__(kMainThreads, V2M_MOVE_MIN_BLOCKS) k_move_main
                                                            const float4* __restrict__ S, const int* __restrict__ queue,
                                                            int* __restrict__ rlist, Global* G, int64_t N,
                                                            int shape_any) {
-    // the three queues laid end to end -- trapped [0, qa), junction [qa, qa+qj),
-    // interior [qa+qj, qa+qj+qb) -- over at most N threads: a warp holds nodes of
-    // one kind (a junction move costs several interface moves), save the two warps
-    // at the seams
+    // the queues laid end to end -- junction and handed-over INTERIOR moves
+    // [0, qj+qd) (queue[N, N+qj+qd)), then the other trapped ones [qj+qd, tot)
+    // -- over at most N threads: a warp holds nodes of one kind, save the warps
+    // at the seams, and the longest moves (junctions) start first
     const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int qa = *((volatile int*)&G->qtrap), qb = *((volatile int*)&G->qint), qj = *((volatile int*)&G->qjun);
-    const int64_t tot = (int64_t)qa + qj + qb;
+    const int qa = *((volatile int*)&G->qtrap), qj = *((volatile int*)&G->qjun), qd = *((volatile int*)&G->qdef);
+    const int64_t qjd = (int64_t)qj + qd;
+    const int64_t tot = qjd + qa;
     if (blockIdx.x * (int64_t)blockDim.x >= tot) {
         return;
     }
     int64_t i = -1;
-    if (q < qa) {
-        i = queue[q];
-    } else if (q < (int64_t)qa + qj) {
-        i = queue[N + (q - qa)];
+    if (q < qjd) {
+        i = queue[N + q];
     } else if (q < tot) {
-        i = queue[N - 1 - (q - qa - qj)];
+        i = queue[q - qjd];
     }
     if (kChecked && (i < -1 || i >= N || tot > N)) {
         raise_error(G, 24, (int)q);   // a move queue entry (or length) beyond the nodes
@@ -1173,56 +1377,7 @@ __global__ void __launch_bounds__(kMainThreads, V2M_MOVE_MIN_BLOCKS) k_move_main
     Pq[i] = make_float4(st.p[0], st.p[1], st.p[2], pack_h(st.hn, st.ty));
     typ[i] = (uint8_t)st.ty;
     part[i] = (uint32_t)(st.pb & 0xFFFF) | ((uint32_t)(st.pc & 0xFFFF) << 16);
-    // the iteration's reductions, combined per warp
-    const float4 q0 = P0[i];
-    const float ex = st.p[0] - q0.x, ey = st.p[1] - q0.y, ez = st.p[2] - q0.z;
-    const float hh = st.hn;
-    const float m2 = ex * ex + ey * ey + ez * ez, s2 = Vd.skin * Vd.skin * hh * hh;
-    const int b = hist_bin(m);
-    VolCtl* cv = ctl + v;
-    const unsigned gb = __match_any_sync(act, (unsigned)(v << 5) | (unsigned)b);
-    if (lane == (unsigned)(__ffs(gb) - 1)) {
-        atomicAdd(&cv->hist[b], __popc(gb));
-    }
-    const unsigned gvol = __match_any_sync(act, (unsigned)v);
-    const unsigned leader = (unsigned)(__ffs(gvol) - 1);
-    const unsigned mx = __reduce_max_sync(gvol, __float_as_uint(m));
-    const bool refresh = m2 > s2 && Vd.policy != 2;   // (policy 2: the first build's lists for the whole run)
-    const bool half = !refresh && m2 > 0.25f * s2;
-    const unsigned nh = __popc(__ballot_sync(act, half) & gvol);
-    unsigned md = 0u;
-    if (Vd.policy == 1) {
-        md = __reduce_max_sync(gvol, __float_as_uint(sqrtf(m2) / hh));
-    }
-    const int slot = blockIdx.x & (kCtlSlots - 1);
-    if (lane == leader) {
-        if (mx) {
-            atomicMax(&cv->maxbits_p[slot], mx);
-        }
-        if (nh) {
-            atomicAdd(&cv->nhalf_p[slot], (int)nh);
-        }
-        if (md) {
-            atomicMax(&cv->maxd_p[slot], md);
-        }
-    }
-    // the refresh list: one atomic per warp
-    const unsigned rm = __ballot_sync(act, refresh);
-    if (rm) {
-        const unsigned first = (unsigned)(__ffs(rm) - 1);
-        int base = 0;
-        if (lane == first) {
-            base = atomicAdd(&G->nrefresh, __popc(rm));
-        }
-        base = __shfl_sync(act, base, first);
-        if (refresh) {
-            rlist[base + __popc(rm & ((1u << lane) - 1u))] = (int)i;
-        }
-        const unsigned rv = rm & gvol;
-        if (lane == leader && rv) {
-            atomicAdd(&cv->nrefresh, __popc(rv));
-        }
-    }
+    warp_tail(Vd, ctl + v, v, i, act, lane, m, st.p[0], st.p[1], st.p[2], st.hn, P0, rlist, G);
 }
 
 // ---- corner tables (once per session) ----------------------------------------------
@@ -1716,6 +1871,8 @@ void launch_move(cudaStream_t s, const Dev& d) {
     k_move_pre<<<nblk(d.N, kMoveThreads), kMoveThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.F, d.Vel, d.typ,
                                                                 d.mv, d.pw, d.P0, d.S, d.queue, d.psum, d.rlist, d.G,
                                                                 d.N);
+    k_move_int<<<nblk(d.N, kMainThreads), kMainThreads, 0, s>>>(d.vols, d.ctl, d.nodevol, d.Pq, d.Vel, d.lab, d.mv,
+                                                                d.P0, d.S, d.queue, d.rlist, d.G, d.N);
     k_move_main<false><<<nblk(d.N, kMainThreads), kMainThreads, 0, s>>>(
         d.vols, d.ctl, d.nodevol, d.Pq, d.Vel, d.typ, d.lab, d.part, d.mv, d.P0, d.S, d.queue, d.rlist, d.G, d.N,
         d.shape_any);

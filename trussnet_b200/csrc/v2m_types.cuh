@@ -139,6 +139,7 @@ struct Global {
     int qtrap_last, qint_last;   // the last iteration's queue lengths (trapped: junctions included)
     int rebuild_any;     // some volume rebuilds this iteration (the rebuild stages return at once otherwise)
     int qjun;            // junction moves (queue[N, N + qjun))
+    int qdef;            // INTERIOR moves k_move_int hands to k_move_main (queue[N + qjun, N + qjun + qdef))
 };
 
 constexpr int kMaxVol = 1024;
