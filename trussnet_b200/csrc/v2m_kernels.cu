@@ -926,10 +926,10 @@ __device__ __forceinline__ void tail_flush(TailAcc& a, VolCtl* cv) {
 // First half of v2m_move (src/opencl/v2m_particle_body.cl:844-921), every node in
 // node order: FIRE velocity update and power, the step, the settle test and the
 // step cap. Corners and settled nodes finish here; the others are queued with
-// their step (S = s, h) for k_move_main -- trapped (non-INTERIOR) nodes at the
-// front of the queue, INTERIOR ones at the back, so that a warp of k_move_main
-// holds nodes of one kind. The FIRE power of the block is summed here, in node
-// order (a fixed-shape double tree: deterministic whatever the queue order).
+// their step (S = s, h): other trapped nodes at the front of the queue and
+// INTERIOR ones at its back, JUNCTION ones in queue[N, 2N); k_move_int and
+// k_move_main take them by kind. The FIRE power of the block is summed here, in
+// node order (a fixed-shape double tree: deterministic whatever the queue order).
 __global__ void __launch_bounds__(kMoveThreads, 5) k_move_pre(const DVol* __restrict__ vols, VolCtl* __restrict__ ctl,
                                                           const uint16_t* __restrict__ nodevol,
                                                           const float4* __restrict__ Pq, const float4* __restrict__ F,

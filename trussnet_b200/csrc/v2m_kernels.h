@@ -16,7 +16,7 @@ constexpr int kScanTile = 1024;     // bin entries per scan tile (volume bin ran
 constexpr int kScanThreads = 256;
 constexpr int kNbrMaxThreads = 256; // k_neighbors: up to 8 warps per block, one node each
 constexpr int kMoveThreads = 256;   // k_move_pre's block; volume node ranges are aligned to it
-constexpr int kMainThreads = 128;   // k_move_main's block
+constexpr int kMainThreads = 128;   // the block of k_move_int and k_move_main
 constexpr int kCtlThreads = 256;
 constexpr int kNodeAlign = kMoveThreads;
 
